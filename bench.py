@@ -1,0 +1,362 @@
+"""Benchmark: GSHT forward+inverse transforms per second at lmax 1024.
+
+Workload (one "step"): a batch of 64 complex fields at lmax = 1024 on the
+Gauss-Legendre grid (nTheta = 1025, nPhi = 2048), upper index n = 0,
+coefficients complex standard normal with envelope (l+1)^-1.5 from a fixed
+seed; one inverse transform (coefficients -> grid) and one forward transform
+(grid -> coefficients, into a zeroed output) per field. Inputs live in HBM
+when the timed region starts; each step touches ~1.1 GB of coefficients and
+~2.2 GB of grid values, far more than the 126 MB L2, so no flush is needed.
+
+    python bench.py [--gpus N --steps K --warmup W] [--precision fp64|bf16x3|ozaki]
+    python bench.py --impl reference     # the reference's CPU path (oracle/_ref)
+
+Multi-GPU runs (torchrun, one process per GPU) are independent replicas: each
+rank transforms its own 64 fields (weak scaling; the transform has no
+exchange step), timed on the device and reduced with MAX over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GSHT fwd+inv/s, lmax 1024: tensor-core vs FP64 GPU at ≤1e-6 and ≤1e-12 err"
+UNIT = "fwd+inv/s"
+L_MAX = 1024
+N_UPPER = 0
+FIELDS = 64
+ENVELOPE = 1.5
+DTYPE = {"fp64": "f64", "bf16x3": "bf16", "ozaki": "int8"}
+STAGES = ["prep_inverse", "legendre_inverse", "fft_inverse", "fft_forward",
+          "prep_forward", "legendre_forward"]
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default=None, choices=[None, "fp64", "bf16x3", "ozaki"])
+    p.add_argument("--fields", type=int, default=FIELDS)
+    p.add_argument("--lmax", type=int, default=L_MAX)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload(args):
+    return {
+        "workload": (f"{args.fields} complex fields, lmax {args.lmax} (nTheta {args.lmax + 1}, "
+                     f"nPhi {2 * args.lmax}), upper index n={N_UPPER}, envelope (l+1)^-{ENVELOPE}, "
+                     "one inverse + one forward transform per field"),
+        "lmax": args.lmax,
+        "fields_per_gpu": args.fields,
+        "upper_index": N_UPPER,
+        "l2": "inputs larger than L2 (coefficients + grids >> 126 MB); no flush",
+    }
+
+
+def coefficients(lmax, fields, seed=0):
+    import oracle
+
+    rng = np.random.default_rng(seed)
+    return np.stack([oracle.random_coefficients(rng, lmax, lmax, N_UPPER, False, ENVELOPE)
+                     for _ in range(fields)])
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap,power.draw")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                     "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 2 + i and s[2 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# Reference arm: the reference's own CPU implementation (oracle/_ref)
+# ---------------------------------------------------------------------------
+def cpu_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_run(lmax, steps, warmup, log=None):
+    """Times the reference's round trip (InverseTransformation then
+    ForwardTransformation per field, OpenMP over fields) on the host cores.
+    Each step transforms one field per core."""
+    import oracle
+
+    if not oracle.Reference.available():
+        return None, "reference build oracle/_ref/libgsht_ref.so is absent"
+    cores = cpu_cores()
+    ref = oracle.Reference()
+    t0 = time.perf_counter()
+    g = ref.grid(lmax, N_UPPER, 0, 2)  # NRange = Single: one host table
+    build_s = time.perf_counter() - t0
+    coefs = coefficients(lmax, cores, seed=1)
+    for _ in range(warmup):
+        g.roundtrip_batch(lmax, N_UPPER, False, coefs, cores)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        out = g.roundtrip_batch(lmax, N_UPPER, False, coefs, cores)
+    dt = time.perf_counter() - t0
+    err = float(np.linalg.norm(out - coefs) / np.linalg.norm(coefs))
+    g.close()
+    value = steps * cores / dt
+    return {
+        "value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+        "sample": (f"{steps} step(s) x {cores} complex field(s) (one per core), lmax {lmax}, "
+                   f"inverse+forward each, reference GaussLegendreGrid.h compiled in place "
+                   f"(FFTWpp/GaussQuad stand-ins); table build {build_s:.1f} s untimed"),
+        "seconds": dt, "round_trip_rel_err": err,
+    }, None
+
+
+def impl_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    res, why = reference_run(args.lmax, args.steps, args.warmup)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return 0
+    line = {
+        "impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * res["seconds"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload(args) | {"fields_per_step": res["cores"]},
+        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "round_trip_rel_err": res["round_trip_rel_err"],
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------
+def measured_fp64_peak(torch, dev):
+    """cuBLAS DGEMM throughput on this GPU (TFLOP/s), best of 3."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def impl_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import ctypes
+
+    import gshtrans_b200 as gsht
+
+    precision = args.precision or "fp64"
+    forms = () if precision == "fp64" else (precision,)
+    L, B = args.lmax, args.fields
+    grid = gsht.GaussLegendreGrid(L, N_UPPER, nrange=gsht.Single, forms=forms)
+    coef_h = coefficients(L, B, seed=rank)
+    coef = torch.from_numpy(coef_h).to(dev)
+    field = torch.empty((B, grid.FieldSize()), dtype=torch.complex128, device=dev)
+    back = torch.zeros_like(coef)
+
+    def step():
+        back.zero_()
+        grid.inverse_batch(L, N_UPPER, coef, field, precision)
+        grid.forward_batch(L, N_UPPER, field, back, precision)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    rt_err = float(torch.linalg.norm(back - coef) / torch.linalg.norm(coef))
+
+    lib = gsht.library
+    lib.gsht_profile_enable(1)
+    launches0 = gsht.launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    launches = gsht.launch_count() - launches0
+    stage_ms = (ctypes.c_double * 6)()
+    stage_n = (ctypes.c_long * 6)()
+    lib.gsht_profile_read.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    lib.gsht_profile_read(ctypes.cast(stage_ms, ctypes.c_void_p), ctypes.cast(stage_n, ctypes.c_void_p), 6)
+    lib.gsht_profile_enable(0)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * B * args.steps / (ms * 1e-3)
+
+    # Roofline of the dominant kernel: the Legendre contraction (both
+    # directions), 4 flops per (table entry x complex field) per direction.
+    stages = {STAGES[i]: {"ms_total": stage_ms[i], "launches": int(stage_n[i])} for i in range(6)}
+    leg_ms = stage_ms[1] + stage_ms[5]
+    leg_launches = int(stage_n[1] + stage_n[5])
+    flops_per_step = 2 * 4.0 * B * ((L + 1) ** 2 - N_UPPER ** 2) * (L + 1)
+    achieved = flops_per_step * args.steps / (leg_ms * 1e-3) / 1e12 if leg_ms > 0 else None
+    peak = measured_fp64_peak(torch, dev) if precision == "fp64" else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(f"legendre_{precision}")
+    roofline = {
+        "kernel": "k_legendre_fp64 (inverse + forward launches)" if precision == "fp64" else precision,
+        "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        "frac": (achieved / peak) if (achieved and peak) else None,
+        "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in MEASURED_PEAKS.json)",
+        "algorithmic_flops_per_launch": flops_per_step / 2,
+        "avg_launch_ms": leg_ms / max(leg_launches, 1),
+        "traffic": traffic,
+    }
+
+    result = None
+    if rank == 0:
+        e2e = None
+        if not args.no_e2e:
+            e2e = e2e_run(gsht, grid, torch, coef_h, precision, args)
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            res, why = reference_run(L, 1, 0)
+            cpu = ({k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+                   if res else {"value": None, "unavailable": why})
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": DTYPE[precision], "data": "synthetic",
+            "config": workload(args) | {"precision": precision, "parallelism": f"replicas x{world}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clk.summary(), "gpu_launches": launches,
+            "stages_ms": stages, "round_trip_rel_err": rt_err,
+        }
+        print(json.dumps(result))
+    grid.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def e2e_run(gsht, grid, torch, coef_h, precision, args):
+    """The same round trip through the C ABI with HOST coefficient buffers
+    (pinned): every step uploads the coefficients, runs inverse + forward and
+    reads the result back; the grid stays in device memory."""
+    L, B = args.lmax, args.fields
+    cin = torch.from_numpy(coef_h).pin_memory()
+    cout = torch.zeros_like(cin).pin_memory()
+    field = torch.empty((B, grid.FieldSize()), dtype=torch.complex128, device="cuda")
+    steps = max(1, min(args.steps, 3))
+
+    def step():
+        cout.zero_()
+        grid.inverse_batch(L, N_UPPER, cin, field, precision)
+        grid.forward_batch(L, N_UPPER, field, cout, precision)
+
+    step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    nbytes = cin.numel() * 16
+    return {"value": B * steps / dt, "unit": UNIT,
+            "h2d_bytes_per_step": 2 * nbytes, "d2h_bytes_per_step": nbytes,
+            "note": "host coefficients in and out (pinned), grid resident on the GPU; "
+                    "the forward output is uploaded because the forward accumulates into it"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return impl_reference(args)
+    return impl_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,291 @@
+"""gshtrans_b200 — Gauss-Legendre generalized-spherical-harmonic transforms on B200.
+
+Python mirror of the reference's ``GaussLegendreGrid`` interface
+(GaussLegendreGrid.h:24-321, GridBase.h:13-177) over the C ABI of
+``libgsht_cuda.so`` (include/gsht.h). Method names, argument meaning and the
+forward transform's accumulate-into-output semantics follow the reference;
+where the reference asserts, this layer raises :class:`BadArgument`.
+
+Buffers may be NumPy arrays (host) or PyTorch tensors (host or CUDA); CUDA
+tensors are used in place and the call only enqueues work on the current
+stream. The CUDA library is required: there is no CPU fallback, and importing
+this package raises if ``libgsht_cuda.so`` cannot be loaded.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+__all__ = [
+    "All", "NonNegative", "Single", "FP64", "BF16X3", "OZAKI",
+    "GaussLegendreGrid", "GSHTError", "BadArgument", "library", "launch_count",
+    "coefficient_size",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgsht_cuda.so")
+
+# Index ranges (Concepts.h:24-27) and precision forms (include/gsht.h).
+All, NonNegative, Single = 0, 1, 2
+FP64, BF16X3, OZAKI = 0, 1, 2
+_FORM_BIT = {FP64: 1, BF16X3: 2, OZAKI: 4}
+_PRECISION_NAMES = {"fp64": FP64, "bf16x3": BF16X3, "ozaki": OZAKI}
+
+_STATUS = {
+    0: "OK", 1: "BAD_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOUT",
+    5: "UNSUPPORTED", 6: "NO_DEVICE",
+}
+
+
+class GSHTError(RuntimeError):
+    """A non-OK status from libgsht_cuda.so."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class BadArgument(GSHTError, ValueError):
+    """Invalid arguments (the reference asserts on these)."""
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m gshtrans_b200.build`"
+        )
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
+    lib.gsht_grid_create.argtypes = [ip, ip, ip, ip, ctypes.c_uint, ctypes.POINTER(vp)]
+    lib.gsht_grid_destroy.argtypes = [vp]
+    lib.gsht_grid_shape.argtypes = [vp] + [ctypes.POINTER(ip)] * 5
+    lib.gsht_grid_nodes.argtypes = [vp, dp, dp]
+    lib.gsht_wigner_block.argtypes = [vp, ip, ip, dp, ctypes.POINTER(ctypes.c_long)]
+    lib.gsht_coefficient_size.argtypes = [ip, ip, ip]
+    lib.gsht_coefficient_size.restype = ctypes.c_long
+    for f in (lib.gsht_forward, lib.gsht_inverse):
+        f.argtypes = [vp, ip, ip, ip, ip, vp, vp, vp]
+    for f in (lib.gsht_forward_batch, lib.gsht_inverse_batch):
+        f.argtypes = [vp, ip, ip, ip, ip, ip, vp, vp, vp]
+    lib.gsht_last_error.restype = ctypes.c_char_p
+    lib.gsht_launch_count.restype = ctypes.c_ulonglong
+    return lib
+
+
+library = _load()
+
+
+def launch_count() -> int:
+    """Kernels launched by libgsht_cuda.so in this process."""
+    return int(library.gsht_launch_count())
+
+
+def _check(status: int):
+    if status != 0:
+        msg = library.gsht_last_error().decode()
+        if status == 1:
+            raise BadArgument(status, msg)
+        raise GSHTError(status, msg)
+
+
+def coefficient_size(lmax: int, n: int, is_real: bool) -> int:
+    """GridBase::RealCoefficientSize / ComplexCoefficientSize (GridBase.h:79-85)."""
+    s = library.gsht_coefficient_size(lmax, n, int(is_real))
+    if s < 0:
+        raise BadArgument(1, f"no coefficients for lmax={lmax}, n={n}")
+    return int(s)
+
+
+def _precision(p) -> int:
+    if isinstance(p, str):
+        return _PRECISION_NAMES[p.lower()]
+    return int(p)
+
+
+def _buffer(x):
+    """(pointer, is_complex, numel, writable-object) for a NumPy array or torch tensor."""
+    if isinstance(x, np.ndarray):
+        if not x.flags["C_CONTIGUOUS"]:
+            raise BadArgument(1, "arrays must be C-contiguous")
+        if x.dtype == np.complex128:
+            return x.ctypes.data, True, x.size
+        if x.dtype == np.float64:
+            return x.ctypes.data, False, x.size
+        raise BadArgument(1, f"unsupported dtype {x.dtype}")
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        torch = None
+    if torch is not None and isinstance(x, torch.Tensor):
+        if not x.is_contiguous():
+            raise BadArgument(1, "tensors must be contiguous")
+        if x.dtype == torch.complex128:
+            return x.data_ptr(), True, x.numel()
+        if x.dtype == torch.float64:
+            return x.data_ptr(), False, x.numel()
+        raise BadArgument(1, f"unsupported dtype {x.dtype}")
+    raise BadArgument(1, f"unsupported buffer type {type(x)}")
+
+
+def _current_stream(*bufs) -> Optional[int]:
+    for b in bufs:
+        if not isinstance(b, np.ndarray):
+            import torch
+
+            if b.is_cuda:
+                return torch.cuda.current_stream(b.device).cuda_stream
+    return None
+
+
+class GaussLegendreGrid:
+    """GaussLegendreGrid<double, MRange, NRange>(lMax, nMax) on the GPU.
+
+    ``mrange`` is ``All`` or ``NonNegative``; ``nrange`` is ``All``,
+    ``NonNegative`` or ``Single`` (GaussLegendreGrid.h:24-26). ``forms``
+    selects which table forms are built besides FP64: any of ``"bf16x3"``,
+    ``"ozaki"``.
+    """
+
+    def __init__(self, lmax: int, nmax: int, mrange: int = All, nrange: int = All,
+                 forms=()):
+        mask = 1
+        for f in forms:
+            mask |= _FORM_BIT[_precision(f)]
+        h = ctypes.c_void_p()
+        _check(library.gsht_grid_create(int(lmax), int(nmax), int(mrange), int(nrange),
+                                        mask, ctypes.byref(h)))
+        self._h = h
+        self._mrange = mrange
+        self._nrange = nrange
+        vals = [ctypes.c_int() for _ in range(5)]
+        _check(library.gsht_grid_shape(h, *[ctypes.byref(v) for v in vals]))
+        self._lmax, self._nmax, self._min_n, self._nt, self._np = (v.value for v in vals)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library.gsht_grid_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- geometry (GaussLegendreGrid.h:86-103, GridBase.h:17-114) ----
+    def MaxDegree(self) -> int:
+        return self._lmax
+
+    def MaxUpperIndex(self) -> int:
+        return self._nmax
+
+    def MinUpperIndex(self) -> int:
+        return self._min_n
+
+    def UpperIndices(self):
+        return range(self._min_n, self._nmax + 1)
+
+    def NumberOfCoLatitudes(self) -> int:
+        return self._nt
+
+    def NumberOfLongitudes(self) -> int:
+        return self._np
+
+    def FieldSize(self) -> int:
+        return self._nt * self._np
+
+    def CoLatitudes(self) -> np.ndarray:
+        th = np.zeros(self._nt)
+        _check(library.gsht_grid_nodes(self._h, th.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), None))
+        return th
+
+    def CoLatitudeWeights(self) -> np.ndarray:
+        w = np.zeros(self._nt)
+        _check(library.gsht_grid_nodes(self._h, None, w.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return w
+
+    def Longitudes(self) -> np.ndarray:
+        return np.arange(self._np) * (2 * np.pi / self._np)
+
+    def LongitudeWeights(self) -> np.ndarray:
+        return np.full(self._np, 2 * np.pi / self._np)
+
+    def RealCoefficientSize(self, lmax: int, n: int) -> int:
+        return coefficient_size(lmax, n, True)
+
+    def ComplexCoefficientSize(self, lmax: int, n: int) -> int:
+        return coefficient_size(lmax, n, False)
+
+    def CoefficientSize(self, lmax: int, n: int) -> int:
+        return coefficient_size(lmax, n, False)
+
+    def CoefficientSizeNonNegative(self, lmax: int, n: int) -> int:
+        return coefficient_size(lmax, n, True)
+
+    def Wigner(self, n: int, itheta: int) -> np.ndarray:
+        """Table block d^l_{mn}(theta_itheta) in the reference layout (Wigner.h:241-244)."""
+        cnt = ctypes.c_long()
+        _check(library.gsht_wigner_block(self._h, n, itheta, None, ctypes.byref(cnt)))
+        out = np.zeros(cnt.value)
+        _check(library.gsht_wigner_block(self._h, n, itheta,
+                                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                         ctypes.byref(cnt)))
+        return out
+
+    # ---- transforms (GaussLegendreGrid.h:108-321) ----
+    def ForwardTransformation(self, lmax: int, n: int, in_, out, precision="fp64"):
+        """Grid values -> coefficients, ACCUMULATED into ``out``."""
+        self._transform(0, lmax, n, in_, out, precision, 1)
+        return out
+
+    def InverseTransformation(self, lmax: int, n: int, in_, out, precision="fp64"):
+        """Coefficients -> grid values (``out`` overwritten)."""
+        self._transform(1, lmax, n, in_, out, precision, 1)
+        return out
+
+    def forward_batch(self, lmax: int, n: int, in_, out, precision="fp64"):
+        """Batched forward: ``in_`` holds count fields back to back."""
+        return self._transform(0, lmax, n, in_, out, precision, None)
+
+    def inverse_batch(self, lmax: int, n: int, in_, out, precision="fp64"):
+        """Batched inverse: ``in_`` holds count coefficient vectors back to back."""
+        return self._transform(1, lmax, n, in_, out, precision, None)
+
+    def _transform(self, direction, lmax, n, in_, out, precision, count):
+        pin, cin, nin = _buffer(in_)
+        pout, cout, nout = _buffer(out)
+        grid_complex = cin if direction == 0 else cout
+        coef_ok = (cout if direction == 0 else cin)
+        if not coef_ok:
+            raise BadArgument(1, "coefficients must be complex128")
+        is_real = not grid_complex
+        if self._mrange != All and not is_real:
+            raise BadArgument(1, "complex fields need MRange = All")
+        if abs(n) > lmax or lmax < 0 or lmax > self._lmax:
+            raise BadArgument(1, f"bad (lmax={lmax}, n={n}) for grid degree {self._lmax}")
+        cs = coefficient_size(lmax, n, is_real)
+        fs = self.FieldSize()
+        n_grid = nin if direction == 0 else nout
+        n_coef = nout if direction == 0 else nin
+        if count is None:
+            if fs == 0 or n_grid % fs or n_coef % cs or n_grid // fs != n_coef // cs:
+                raise BadArgument(1, "batch buffers do not hold a whole number of fields")
+            count = n_grid // fs
+        elif n_grid != fs or n_coef != cs:
+            raise BadArgument(1, f"sizes: grid {n_grid} (want {fs}), coefficients {n_coef} (want {cs})")
+        stream = _current_stream(in_, out)
+        fn = library.gsht_forward_batch if direction == 0 else library.gsht_inverse_batch
+        _check(fn(self._h, lmax, n, int(is_real), _precision(precision), count,
+                  ctypes.c_void_p(pin), ctypes.c_void_p(pout),
+                  ctypes.c_void_p(stream) if stream else None))
+        return out

@@ -1,0 +1,414 @@
+// C ABI of libgsht_cuda.so (declared in include/gsht.h): grid lifetime,
+// argument validation with the reference's semantics, workspace management
+// and the staging of host buffers.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "gsht_internal.cuh"
+
+namespace gsht {
+
+std::atomic<unsigned long long> g_launches{0};
+static thread_local char t_error[512] = "";
+
+gsht_status fail(gsht_status s, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(t_error, sizeof(t_error), fmt, ap);
+  va_end(ap);
+  return s;
+}
+
+gsht_status cuda_fail(cudaError_t e, const char* what) {
+  return fail(e == cudaErrorMemoryAllocation ? GSHT_ERR_OOM : GSHT_ERR_CUDA,
+              "%s: %s", what, cudaGetErrorString(e));
+}
+
+namespace {
+
+struct ProfRecord {
+  int stage;
+  cudaEvent_t a, b;
+  unsigned long long launches;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRecord> g_prof;
+
+}  // namespace
+
+StageTimer::StageTimer(int stage, cudaStream_t s) : stage_(stage), s_(s) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (!g_prof_on) return;
+  if (cudaEventCreate(&a_) != cudaSuccess || cudaEventCreate(&b_) != cudaSuccess) {
+    cudaGetLastError();
+    a_ = b_ = nullptr;
+    return;
+  }
+  cudaEventRecord(a_, s_);
+  launches0_ = g_launches.load();
+}
+
+StageTimer::~StageTimer() {
+  if (!a_) return;
+  cudaEventRecord(b_, s_);
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof.push_back({stage_, a_, b_, g_launches.load() - launches0_});
+}
+
+namespace {
+
+// lmax == 0 special cases of the reference (GaussLegendreGrid.h:136-140 and
+// :251-260): the forward ASSIGNS out[0] = in[0] / (2 sqrt(pi)); the inverse
+// writes only out[0] = in[0] * 2 sqrt(pi), leaving the other points as they
+// were.
+__global__ void k_lmax0(int dir, int isReal, int count, long fieldSize,
+                        const double* __restrict__ in, double* __restrict__ out) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= count) return;
+  const double twoSqrtPi = 3.5449077018110320546;  // 2 sqrt(pi)
+  if (dir == 0) {  // forward
+    const long inStride = isReal ? fieldSize : 2 * fieldSize;
+    const double re = in[f * inStride];
+    const double im = isReal ? 0.0 : in[f * inStride + 1];
+    out[2 * f] = re / twoSqrtPi;
+    out[2 * f + 1] = im / twoSqrtPi;
+  } else {
+    const long outStride = isReal ? fieldSize : 2 * fieldSize;
+    out[f * outStride] = in[2 * f] * twoSqrtPi;
+    if (!isReal) out[f * outStride + 1] = in[2 * f + 1] * twoSqrtPi;
+  }
+}
+
+bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+gsht_status ensure_workspace(gsht_grid* g, size_t bytes) {
+  if (g->ws_bytes >= bytes) return GSHT_OK;
+  if (g->ws) {
+    GSHT_CUDA(cudaDeviceSynchronize());
+    cudaFree(g->ws);
+    g->ws = nullptr;
+    g->ws_bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&g->ws, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(GSHT_ERR_OOM, "workspace allocation of %zu bytes failed", bytes);
+  }
+  g->ws_bytes = bytes;
+  return GSHT_OK;
+}
+
+gsht_status validate(const gsht_grid* g, int lmax, int n, int is_real,
+                     int precision, int count) {
+  if (!g) return fail(GSHT_ERR_BAD_ARG, "grid is NULL");
+  if (count < 1 || count > 32767) return fail(GSHT_ERR_BAD_ARG, "count %d out of range [1, 32767]", count);
+  if (lmax < 0 || lmax > g->L)
+    return fail(GSHT_ERR_BAD_ARG, "lmax %d outside [0, %d]", lmax, g->L);
+  if (n < g->min_n || n > g->nmax)
+    return fail(GSHT_ERR_BAD_ARG, "upper index %d not in the grid's range [%d, %d]", n, g->min_n, g->nmax);
+  if ((n < 0 ? -n : n) > lmax)
+    return fail(GSHT_ERR_BAD_ARG, "|n| = %d exceeds lmax = %d", n < 0 ? -n : n, lmax);
+  if (!is_real && g->mrange != GSHT_RANGE_ALL)
+    return fail(GSHT_ERR_BAD_ARG, "complex fields need MRange = All");
+  if (precision != GSHT_FP64)
+    return fail(GSHT_ERR_UNSUPPORTED, "precision %d not available", precision);
+  return GSHT_OK;
+}
+
+struct CallScope {
+  gsht_grid* g;
+  cudaStream_t s;
+  std::lock_guard<std::mutex> lock;
+  CallScope(gsht_grid* grid, cudaStream_t stream) : g(grid), s(stream), lock(grid->mu) {}
+};
+
+gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
+                          int precision, int count, const void* in, void* out,
+                          void* stream_ptr) {
+  gsht_status st = validate(g, lmax, n, is_real, precision, count);
+  if (st != GSHT_OK) return st;
+  GSHT_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream_ptr);
+  CallScope scope(g, s);
+  const Table* t = g->table(n);
+  const long cs = coef_size(lmax, n, is_real);
+  const long fs = (long)g->n_theta * g->n_phi;
+  const size_t coefBytes = sizeof(double) * 2 * cs * (size_t)count;
+  const size_t gridBytes = sizeof(double) * (is_real ? 1 : 2) * fs * (size_t)count;
+  const size_t inBytes = dir == 0 ? gridBytes : coefBytes;
+  const size_t outBytes = dir == 0 ? coefBytes : gridBytes;
+  const bool inDev = is_device_ptr(in), outDev = is_device_ptr(out);
+
+  // Workspace: [spec][operand][in staging][out staging], 256-byte aligned.
+  const size_t specBytes = lmax > 0 ? sizeof(double) * 2 * spec_elems(g, lmax, is_real, count) : 0;
+  size_t opBytes = 0;
+  if (dir == 1 && lmax > 0)
+    opBytes = sizeof(double) * 2 * fp64_operand_elems(g, t, lmax, is_real, count);
+  size_t off = 0;
+  auto carve = [&](size_t b) { size_t o = off; off += round_up(b, 256); return o; };
+  const size_t oSpec = carve(specBytes), oOp = carve(opBytes);
+  const size_t oIn = carve(inDev ? 0 : inBytes), oOut = carve(outDev ? 0 : outBytes);
+  st = ensure_workspace(g, off > 0 ? off : 256);
+  if (st != GSHT_OK) return st;
+  char* ws = static_cast<char*>(g->ws);
+  if (g->ws_done) GSHT_CUDA(cudaStreamWaitEvent(s, g->ws_done, 0));
+
+  const double* dIn = inDev ? static_cast<const double*>(in) : reinterpret_cast<double*>(ws + oIn);
+  double* dOut = outDev ? static_cast<double*>(out) : reinterpret_cast<double*>(ws + oOut);
+  if (!inDev) GSHT_CUDA(cudaMemcpyAsync(const_cast<double*>(dIn), in, inBytes, cudaMemcpyHostToDevice, s));
+  // The forward accumulates into its output, so host outputs are uploaded
+  // first; the inverse leaves grid points untouched only for lmax == 0.
+  if (!outDev && (dir == 0 || lmax == 0))
+    GSHT_CUDA(cudaMemcpyAsync(dOut, out, outBytes, cudaMemcpyHostToDevice, s));
+
+  if (lmax == 0) {
+    k_lmax0<<<(count + 127) / 128, 128, 0, s>>>(dir, is_real, count, fs, dIn, dOut);
+    GSHT_LAUNCH_CHECK("k_lmax0");
+  } else {
+    double* spec = reinterpret_cast<double*>(ws + oSpec);
+    if (dir == 0) {
+      {
+        StageTimer tm(GSHT_STAGE_FFT_FORWARD, s);
+        st = fft_forward(g, lmax, is_real, count, dIn, spec, s);
+      }
+      if (st != GSHT_OK) return st;
+      {
+        StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
+        st = legendre_forward_fp64(g, t, lmax, is_real, count, spec, dOut, s);
+      }
+      if (st != GSHT_OK) return st;
+    } else {
+      double* op = reinterpret_cast<double*>(ws + oOp);
+      st = legendre_inverse_fp64(g, t, lmax, is_real, count, dIn, op, spec, s);
+      if (st != GSHT_OK) return st;
+      {
+        StageTimer tm(GSHT_STAGE_FFT_INVERSE, s);
+        st = fft_inverse(g, lmax, is_real, count, spec, dOut, s);
+      }
+      if (st != GSHT_OK) return st;
+    }
+  }
+  if (!outDev) GSHT_CUDA(cudaMemcpyAsync(out, dOut, outBytes, cudaMemcpyDeviceToHost, s));
+  if (!g->ws_done) GSHT_CUDA(cudaEventCreateWithFlags(&g->ws_done, cudaEventDisableTiming));
+  GSHT_CUDA(cudaEventRecord(g->ws_done, s));
+  if (!inDev || !outDev) GSHT_CUDA(cudaStreamSynchronize(s));
+  return GSHT_OK;
+}
+
+}  // namespace
+}  // namespace gsht
+
+using namespace gsht;
+
+extern "C" {
+
+gsht_status gsht_grid_create(int lmax, int nmax, int mrange, int nrange,
+                             unsigned forms, gsht_grid** out) {
+  if (!out) return fail(GSHT_ERR_BAD_ARG, "output handle pointer is NULL");
+  *out = nullptr;
+  if (lmax < 1) return fail(GSHT_ERR_BAD_ARG, "lmax must be >= 1 (got %d)", lmax);
+  if (nmax < 0 || nmax > lmax)
+    return fail(GSHT_ERR_BAD_ARG, "nmax %d outside [0, lmax]", nmax);
+  if (mrange != GSHT_RANGE_ALL && mrange != GSHT_RANGE_NONNEGATIVE)
+    return fail(GSHT_ERR_BAD_ARG, "mrange must be All or NonNegative");
+  if (nrange < GSHT_RANGE_ALL || nrange > GSHT_RANGE_SINGLE)
+    return fail(GSHT_ERR_BAD_ARG, "bad nrange %d", nrange);
+  if (forms & ~7u) return fail(GSHT_ERR_BAD_ARG, "unknown form bits 0x%x", forms);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(GSHT_ERR_NO_DEVICE, "no CUDA device visible");
+  }
+  gsht_grid* g = new (std::nothrow) gsht_grid();
+  if (!g) return fail(GSHT_ERR_OOM, "host allocation failed");
+  GSHT_CUDA(cudaGetDevice(&g->device));
+  g->L = lmax;
+  g->nmax = nmax;
+  g->mrange = mrange;
+  g->nrange = nrange;
+  g->forms = forms | GSHT_FORM_FP64;
+  g->min_n = nrange == GSHT_RANGE_ALL ? -nmax : (nrange == GSHT_RANGE_NONNEGATIVE ? 0 : nmax);
+  g->n_theta = lmax + 1;
+  g->n_phi = 2 * lmax;
+  g->theta_pad = (int)round_up(g->n_theta, kThetaPad);
+  gsht_status st = build_nodes(g);
+  if (st == GSHT_OK) {
+    // Twiddles exp(-2 pi i t / nPhi), t < nPhi, rounded from long double.
+    std::vector<double> tw(2 * (size_t)g->n_phi);
+    const long double twoPi = 6.283185307179586476925286766559005768L;
+    for (int t = 0; t < g->n_phi; t++) {
+      const long double a = twoPi * t / g->n_phi;
+      tw[2 * t] = (double)cosl(a);
+      tw[2 * t + 1] = (double)-sinl(a);
+    }
+    if (cudaMalloc(&g->d_twiddle, sizeof(double) * tw.size()) != cudaSuccess ||
+        cudaMemcpy(g->d_twiddle, tw.data(), sizeof(double) * tw.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaGetLastError();
+      st = fail(GSHT_ERR_OOM, "twiddle table allocation failed");
+    }
+  }
+  if (st == GSHT_OK) {
+    g->tables.resize(g->nmax - g->min_n + 1);
+    cudaStream_t s = nullptr;
+    for (int n = g->min_n; n <= g->nmax && st == GSHT_OK; n++) {
+      Table* t = &g->tables[n - g->min_n];
+      t->n = n;
+      st = build_table(g, t, s);
+      if (st == GSHT_OK) st = build_forms(g, t, s);
+    }
+  }
+  if (st != GSHT_OK) {
+    gsht_grid_destroy(g);
+    return st;
+  }
+  *out = g;
+  return GSHT_OK;
+}
+
+gsht_status gsht_grid_destroy(gsht_grid* g) {
+  if (!g) return GSHT_OK;
+  cudaSetDevice(g->device);
+  cudaDeviceSynchronize();
+  for (auto& t : g->tables) free_table(&t);
+  free_layouts(g);
+  cudaFree(g->d_theta);
+  cudaFree(g->d_weight);
+  cudaFree(g->d_twiddle);
+  cudaFree(g->d_twiddle_half);
+  cudaFree(g->ws);
+  if (g->ws_done) cudaEventDestroy(g->ws_done);
+  delete g;
+  return GSHT_OK;
+}
+
+gsht_status gsht_grid_shape(const gsht_grid* g, int* lmax, int* nmax,
+                            int* min_n, int* n_theta, int* n_phi) {
+  if (!g) return fail(GSHT_ERR_BAD_ARG, "grid is NULL");
+  if (lmax) *lmax = g->L;
+  if (nmax) *nmax = g->nmax;
+  if (min_n) *min_n = g->min_n;
+  if (n_theta) *n_theta = g->n_theta;
+  if (n_phi) *n_phi = g->n_phi;
+  return GSHT_OK;
+}
+
+gsht_status gsht_grid_nodes(const gsht_grid* g, double* colatitudes,
+                            double* weights) {
+  if (!g) return fail(GSHT_ERR_BAD_ARG, "grid is NULL");
+  if (colatitudes) memcpy(colatitudes, g->h_theta.data(), sizeof(double) * g->n_theta);
+  if (weights) memcpy(weights, g->h_weight.data(), sizeof(double) * g->n_theta);
+  return GSHT_OK;
+}
+
+gsht_status gsht_wigner_block(const gsht_grid* g, int n, int itheta,
+                              double* out, long* count) {
+  if (!g) return fail(GSHT_ERR_BAD_ARG, "grid is NULL");
+  if (n < g->min_n || n > g->nmax) return fail(GSHT_ERR_BAD_ARG, "upper index %d not in the grid", n);
+  if (itheta < 0 || itheta >= g->n_theta) return fail(GSHT_ERR_BAD_ARG, "colatitude index %d out of range", itheta);
+  const int L = g->L, na = n < 0 ? -n : n;
+  const bool all = g->mrange == GSHT_RANGE_ALL;
+  const long total = all ? (long)(L + 1) * (L + 1) - (long)n * n
+                         : (long)(L + 1) * (L + 2) / 2 - (long)na * (na + 1) / 2;
+  if (count) *count = total;
+  if (!out) return GSHT_OK;
+  const Table* t = g->table(n);
+  GSHT_CUDA(cudaSetDevice(g->device));
+  std::vector<double> col(t->rows), mir(t->rows);
+  const size_t pitch = sizeof(double) * g->theta_pad;
+  GSHT_CUDA(cudaMemcpy2D(col.data(), sizeof(double), t->t64 + itheta, pitch,
+                         sizeof(double), t->rows, cudaMemcpyDeviceToHost));
+  GSHT_CUDA(cudaMemcpy2D(mir.data(), sizeof(double), t->t64 + (g->n_theta - 1 - itheta),
+                         pitch, sizeof(double), t->rows, cudaMemcpyDeviceToHost));
+  long i = 0;
+  for (int l = na; l <= L; l++) {
+    for (int m = all ? -l : 0; m <= l; m++) {
+      const int am = m < 0 ? -m : m;
+      const int l0 = am > na ? am : na;
+      const long long row = t->row_off[am] + (l - l0);
+      // d^l_{-m,n}(theta_j) = (-1)^{l+n} d^l_{mn}(theta_{nTheta-1-j})
+      out[i++] = m >= 0 ? col[row] : (((l + n) & 1) ? -mir[row] : mir[row]);
+    }
+  }
+  return GSHT_OK;
+}
+
+long gsht_coefficient_size(int lmax, int n, int is_real) {
+  if (lmax < 0 || (n < 0 ? -n : n) > lmax) return -1;
+  return coef_size(lmax, n, is_real);
+}
+
+gsht_status gsht_forward(const gsht_grid* g, int lmax, int n, int is_real,
+                         int precision, const void* in, void* out,
+                         void* stream) {
+  return run_transform(const_cast<gsht_grid*>(g), 0, lmax, n, is_real,
+                       precision, 1, in, out, stream);
+}
+
+gsht_status gsht_inverse(const gsht_grid* g, int lmax, int n, int is_real,
+                         int precision, const void* in, void* out,
+                         void* stream) {
+  return run_transform(const_cast<gsht_grid*>(g), 1, lmax, n, is_real,
+                       precision, 1, in, out, stream);
+}
+
+gsht_status gsht_forward_batch(const gsht_grid* g, int lmax, int n,
+                               int is_real, int precision, int count,
+                               const void* in, void* out, void* stream) {
+  return run_transform(const_cast<gsht_grid*>(g), 0, lmax, n, is_real,
+                       precision, count, in, out, stream);
+}
+
+gsht_status gsht_inverse_batch(const gsht_grid* g, int lmax, int n,
+                               int is_real, int precision, int count,
+                               const void* in, void* out, void* stream) {
+  return run_transform(const_cast<gsht_grid*>(g), 1, lmax, n, is_real,
+                       precision, count, in, out, stream);
+}
+
+gsht_status gsht_profile_enable(int on) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (auto& r : g_prof) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  g_prof.clear();
+  g_prof_on = on != 0;
+  return GSHT_OK;
+}
+
+gsht_status gsht_profile_read(double* ms, long* launches, int nstages) {
+  if (nstages < 0) return fail(GSHT_ERR_BAD_ARG, "negative stage count");
+  for (int i = 0; i < nstages; i++) {
+    if (ms) ms[i] = 0.0;
+    if (launches) launches[i] = 0;
+  }
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (auto& r : g_prof) {
+    GSHT_CUDA(cudaEventSynchronize(r.b));
+    float t = 0.f;
+    GSHT_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+    if (r.stage < nstages) {
+      if (ms) ms[r.stage] += t;
+      if (launches) launches[r.stage] += (long)r.launches;
+    }
+  }
+  return GSHT_OK;
+}
+
+const char* gsht_last_error(void) { return t_error; }
+
+unsigned long long gsht_launch_count(void) { return g_launches.load(); }
+
+}  // extern "C"

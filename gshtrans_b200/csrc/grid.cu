@@ -1,0 +1,414 @@
+// Grid construction on the GPU: Gauss-Legendre nodes (FP64, double-double
+// residuals), the Wigner d^l_{mn}(theta_j) recurrence (one thread per
+// (m, theta_j) chain, exponent-scaled start values), and the compact table
+// forms (BF16 hi/mid/lo planes, Ozaki INT8 slices with per-column
+// power-of-two scales).
+//
+// Replaces GaussLegendreGrid's constructor (GaussLegendreGrid.h:38-73), the
+// GaussQuad node computation it calls (:47-49) and Wigner::ComputeAll /
+// Compute (Wigner.h:24-95, 289-486).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "gsht_internal.cuh"
+
+namespace gsht {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Double-double helpers (Dekker/Knuth error-free transformations).
+// ---------------------------------------------------------------------------
+struct dd {
+  double hi, lo;
+};
+
+__device__ __forceinline__ dd two_sum(double a, double b) {
+  double s = a + b;
+  double bb = s - a;
+  double e = (a - (s - bb)) + (b - bb);
+  return {s, e};
+}
+__device__ __forceinline__ dd quick_two_sum(double a, double b) {
+  double s = a + b;
+  return {s, b - (s - a)};
+}
+__device__ __forceinline__ dd two_prod(double a, double b) {
+  double p = a * b;
+  return {p, fma(a, b, -p)};
+}
+__device__ __forceinline__ dd dd_add(dd a, dd b) {
+  dd s = two_sum(a.hi, b.hi);
+  s.lo += a.lo + b.lo;
+  return quick_two_sum(s.hi, s.lo);
+}
+__device__ __forceinline__ dd dd_neg(dd a) { return {-a.hi, -a.lo}; }
+__device__ __forceinline__ dd dd_mul(dd a, dd b) {
+  dd p = two_prod(a.hi, b.hi);
+  p.lo += a.hi * b.lo + a.lo * b.hi;
+  return quick_two_sum(p.hi, p.lo);
+}
+__device__ __forceinline__ dd dd_mul_d(dd a, double b) {
+  dd p = two_prod(a.hi, b);
+  p.lo += a.lo * b;
+  return quick_two_sum(p.hi, p.lo);
+}
+__device__ __forceinline__ dd dd_div_d(dd a, double b) {
+  double q1 = a.hi / b;
+  dd p = two_prod(q1, b);
+  double r = ((a.hi - p.hi) - p.lo + a.lo) / b;
+  return quick_two_sum(q1, r);
+}
+
+// P_n(x) and P_{n-1}(x) by the three-term recurrence
+// (k+1) P_{k+1} = (2k+1) x P_k - k P_{k-1}, in double-double.
+__device__ void legendre_dd(int n, double x, dd* pn, dd* pnm1) {
+  dd p0 = {1.0, 0.0}, p1 = {x, 0.0};
+  for (int k = 1; k < n; k++) {
+    dd t = dd_mul(two_prod(x, (double)(2 * k + 1)), p1);
+    dd u = dd_mul_d(p0, (double)k);
+    dd p2 = dd_div_d(dd_add(t, dd_neg(u)), (double)(k + 1));
+    p0 = p1;
+    p1 = p2;
+  }
+  *pn = p1;
+  *pnm1 = p0;
+}
+
+// One thread per node pair (x_i, x_{n-1-i} = -x_i): Newton on P_n from the
+// asymptotic guess, residuals in double-double so that the iteration settles
+// on the double nearest the root; theta = acos(-x) (GaussLegendreGrid.h:48).
+__global__ void k_gl_nodes(int n, double* theta, double* weight) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (n + 1) / 2) return;
+  double x = -cospi((i + 0.75) / (n + 0.5));
+  dd pn, pnm1;
+  for (int it = 0; it < 60; it++) {
+    legendre_dd(n, x, &pn, &pnm1);
+    const double dp = n * (x * pn.hi - pnm1.hi) / (x * x - 1.0);
+    const double xn = x - pn.hi / dp;
+    if (xn == x) break;
+    x = xn;
+  }
+  if (2 * i + 1 == n) x = 0.0;
+  legendre_dd(n, x, &pn, &pnm1);
+  // w = 2 (1 - x^2) / (n P_{n-1}(x))^2 at a root of P_n.
+  const double omx2 = (1.0 - x) * (1.0 + x);
+  const double q = n * pnm1.hi;
+  const double w = 2.0 * omx2 / (q * q);
+  // North node: theta = acos(-x) with -x in (0, 1]. South node: theta =
+  // acos(x) = pi - acos(-x), formed with a split pi.
+  const double tn = acos(-x);
+  const double pi_hi = 3.141592653589793116;
+  const double pi_lo = 1.2246467991473532e-16;
+  dd s = two_sum(pi_hi, -tn);
+  const double ts = s.hi + (s.lo + pi_lo);
+  theta[i] = tn;
+  theta[n - 1 - i] = ts;
+  weight[i] = w;
+  weight[n - 1 - i] = w;
+}
+
+// ---------------------------------------------------------------------------
+// Exponent-extended numbers f * 2^e (Fukushima-style X-numbers) for the
+// start values, which underflow double near the poles at high degree.
+// ---------------------------------------------------------------------------
+struct xnum {
+  double f;
+  int e;
+};
+__device__ __forceinline__ void xnorm(xnum& a) {
+  if (a.f != 0.0 && (fabs(a.f) < 0x1p-400 || fabs(a.f) > 0x1p400)) {
+    int k;
+    a.f = frexp(a.f, &k);
+    a.e += k;
+  }
+}
+__device__ __forceinline__ void xmul(xnum& a, double b) {
+  a.f *= b;
+  xnorm(a);
+}
+
+// Start values of the l-recurrence for every order m >= 0 at colatitude
+// theta_j: d^{l0}_{mn}(theta_j), l0 = max(m, |n|). For m >= |n| these are the
+// boundary values d^m_{mn} (WignerMaxOrder, Wigner.h:82-85), generated by the
+// exact ratio d^{m+1}_{m+1,n} / d^m_{mn} = -sqrt((2m+2)(2m+1)/((m+1+n)(m+1-n)))
+// sin(theta/2) cos(theta/2) from d^{|n|}_{|n|,n}; for m < |n| they are the
+// row l = |n| (WignerMax/MinUpperIndex, Wigner.h:87-95), generated downward in
+// m. Products of exact ratios replace the reference's exp(lgamma ...) form,
+// which loses ~|argument| ulps and underflows for L >~ 1930.
+__global__ void k_wigner_start(int L, int n, int nTheta, int thetaPad,
+                               const double* __restrict__ theta,
+                               double* __restrict__ start_f,
+                               int* __restrict__ start_e) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nTheta) return;
+  const int na = n < 0 ? -n : n;
+  double s, c;
+  sincos(0.5 * theta[j], &s, &c);
+  // d^{|n|}_{|n|,n} = c^{2n} (n >= 0) or s^{2|n|} (n < 0).
+  xnum v = {1.0, 0};
+  const double base = n >= 0 ? c : s;
+  for (int k = 0; k < 2 * na; k++) xmul(v, base);
+  auto store = [&](int m, const xnum& x) {
+    const size_t o = (size_t)m * thetaPad + j;
+    start_f[o] = x.f;
+    start_e[o] = x.e;
+  };
+  store(na, v);
+  xnum u = v;
+  for (int m = na; m < L; m++) {
+    const double r = sqrt((double)(2 * m + 2) * (double)(2 * m + 1) /
+                          ((double)(m + 1 + n) * (double)(m + 1 - n)));
+    xmul(u, -r * s * c);
+    store(m + 1, u);
+  }
+  // Orders m < |n| at degree |n|, downward from m = |n|.
+  u = v;
+  for (int m = na; m > 0; m--) {
+    const double r = sqrt((double)(na + m) / (double)(na - m + 1));
+    if (n >= 0) {
+      xmul(u, r * (s / c));
+    } else {
+      xmul(u, -r * (c / s));
+    }
+    store(m - 1, u);
+  }
+}
+
+// The l-recurrence (Wigner.h:347-472) for one order m per block (blockIdx.y)
+// and one colatitude per thread. Per-degree coefficients are computed once per
+// block into shared memory; the chain runs in exponent-extended form until its
+// values enter the normal double range. Values are written Ortho-normalised
+// (factor sqrt(2l+1)/(2 sqrt(pi)), Wigner.h:475-485).
+__global__ void __launch_bounds__(128) k_wigner_chain(
+    int L, int n, int nTheta, int thetaPad, const double* __restrict__ theta,
+    const double* __restrict__ start_f, const int* __restrict__ start_e,
+    const long long* __restrict__ row_off, double* __restrict__ table) {
+  extern __shared__ double sh[];
+  const int m = (int)blockIdx.y;
+  const int na = n < 0 ? -n : n;
+  const int l0 = m > na ? m : na;
+  const int K = L - l0 + 1;
+  double* a = sh;          // f1 = a_l cos(theta) - b_l
+  double* b = sh + K;
+  double* g = sh + 2 * K;  // f2
+  double* nrm = sh + 3 * K;
+  for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    const int l = l0 + k;
+    nrm[k] = sqrt((double)(2 * l + 1)) * 0.28209479177387814347;  // 1/(2 sqrt(pi))
+    a[k] = 0.0;
+    b[k] = 0.0;
+    g[k] = 0.0;
+    if (k == 1) {
+      if (m <= na) {
+        // Row |n|+1, interior orders (Wigner.h:365-373).
+        const double sg = n < 0 ? -1.0 : 1.0;
+        const double c0 = (2.0 * l - 1.0) * rsqrt((double)(l + na)) *
+                          rsqrt((double)(l - m)) * rsqrt((double)(l + m));
+        a[k] = c0 * l;
+        b[k] = c0 * sg * m;
+      } else {
+        // One-term recursion at m = l - 1 (Wigner.h:406-413, 448-457).
+        const double c0 = (2.0 * l - 1.0) * rsqrt((double)(l - n)) *
+                          rsqrt((double)(l + n)) * rsqrt((double)(l - m)) *
+                          rsqrt((double)(l + m)) / (double)(l - 1);
+        a[k] = c0 * l * (l - 1.0);
+        b[k] = c0 * (double)m * (double)n;
+      }
+    } else if (k >= 2) {
+      // Two-term recursion (Wigner.h:428-445).
+      const double inl = rsqrt((double)(l - n)) * rsqrt((double)(l + n));
+      const double dn = rsqrt((double)(l - m)) * rsqrt((double)(l + m));
+      a[k] = (2.0 * l - 1.0) * l * inl * dn;
+      b[k] = (2.0 * l - 1.0) * n * inl / (l - 1.0) * m * dn;
+      g[k] = l * sqrt((double)(l - 1 - n)) * sqrt((double)(l - 1 + n)) * inl /
+             (l - 1.0) * sqrt((double)(l - 1 - m)) * sqrt((double)(l - 1 + m)) *
+             dn;
+    }
+  }
+  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= thetaPad) return;
+  double* out = table + (size_t)row_off[m] * thetaPad + j;
+  if (j >= nTheta) {
+    for (int k = 0; k < K; k++) out[(size_t)k * thetaPad] = 0.0;
+    return;
+  }
+  const double cs = cos(theta[j]);
+  // Exponent-extended chain: value = p * 2^E with E a multiple of 512.
+  int ef = 0;
+  const double f0 = frexp(start_f[(size_t)m * thetaPad + j], &ef);  // [0.5, 1)
+  const int e0 = start_e[(size_t)m * thetaPad + j] + ef;  // value = f0 2^e0
+  int E = 0;
+  if (f0 != 0.0 && e0 < -900) E = -512 * ((-900 - e0 + 511) / 512);
+  double p1 = ldexp(f0, e0 - E), p2 = 0.0;
+  auto emit = [&](int k, double p) {
+    const double v = (E == 0) ? p : ldexp(p, E);
+    out[(size_t)k * thetaPad] = v * nrm[k];
+  };
+  emit(0, p1);
+  for (int k = 1; k < K; k++) {
+    const double p = (a[k] * cs - b[k]) * p1 - g[k] * p2;
+    p2 = p1;
+    p1 = p;
+    if (E < 0 && fabs(p1) >= 0x1p-100) {
+      p1 = ldexp(p1, -512);
+      p2 = ldexp(p2, -512);
+      E += 512;
+    }
+    emit(k, p1);
+  }
+}
+
+// BF16 hi/mid/lo planes: x = hi + mid + lo + O(2^-24 |x|).
+__global__ void k_split_bf16(size_t count, const double* __restrict__ t64,
+                             __nv_bfloat16* __restrict__ tbf,
+                             size_t plane) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double x = t64[i];
+    const __nv_bfloat16 h = __double2bfloat16(x);
+    const double r1 = x - (double)__bfloat162float(h);
+    const __nv_bfloat16 md = __double2bfloat16(r1);
+    const double r2 = r1 - (double)__bfloat162float(md);
+    tbf[i] = h;
+    tbf[plane + i] = md;
+    tbf[2 * plane + i] = __double2bfloat16(r2);
+  }
+}
+
+// Ozaki slices per (m, theta_j) column: sigma = 2^e with max_l |d| < sigma,
+// d / sigma = sum_s S_s 2^{-7 s}, S_s in [-127, 127] by truncation (each
+// residual keeps the sign of the value, so no slice overflows).
+__global__ void k_slice_i8(int L, int n, int thetaPad,
+                           const long long* __restrict__ row_off,
+                           const double* __restrict__ t64,
+                           int8_t* __restrict__ ti8, size_t plane,
+                           int* __restrict__ col_exp) {
+  const int m = blockIdx.y;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= thetaPad) return;
+  const int na = n < 0 ? -n : n;
+  const int l0 = m > na ? m : na;
+  const int K = L - l0 + 1;
+  const size_t base = (size_t)row_off[m] * thetaPad + j;
+  double mx = 0.0;
+  for (int k = 0; k < K; k++) mx = fmax(mx, fabs(t64[base + (size_t)k * thetaPad]));
+  int e = 0;
+  if (mx > 0.0) {
+    frexp(mx, &e);  // mx = f 2^e, f in [0.5, 1) => mx < 2^e
+  }
+  col_exp[(size_t)m * thetaPad + j] = e;
+  for (int k = 0; k < K; k++) {
+    double y = ldexp(t64[base + (size_t)k * thetaPad], -e);  // |y| < 1
+    for (int s = 0; s < kTableSlices; s++) {
+      y *= 128.0;
+      const double q = trunc(y);
+      y -= q;
+      ti8[s * plane + base + (size_t)k * thetaPad] = (int8_t)q;
+    }
+  }
+}
+
+}  // namespace
+
+gsht_status build_nodes(gsht_grid* g) {
+  const int nt = g->n_theta;
+  GSHT_CUDA(cudaMalloc(&g->d_theta, sizeof(double) * g->theta_pad));
+  GSHT_CUDA(cudaMalloc(&g->d_weight, sizeof(double) * g->theta_pad));
+  GSHT_CUDA(cudaMemset(g->d_theta, 0, sizeof(double) * g->theta_pad));
+  GSHT_CUDA(cudaMemset(g->d_weight, 0, sizeof(double) * g->theta_pad));
+  const int pairs = (nt + 1) / 2;
+  k_gl_nodes<<<(pairs + 127) / 128, 128>>>(nt, g->d_theta, g->d_weight);
+  GSHT_LAUNCH_CHECK("k_gl_nodes");
+  g->h_theta.resize(nt);
+  g->h_weight.resize(nt);
+  GSHT_CUDA(cudaMemcpy(g->h_theta.data(), g->d_theta, sizeof(double) * nt,
+                       cudaMemcpyDeviceToHost));
+  GSHT_CUDA(cudaMemcpy(g->h_weight.data(), g->d_weight, sizeof(double) * nt,
+                       cudaMemcpyDeviceToHost));
+  return GSHT_OK;
+}
+
+gsht_status build_table(gsht_grid* g, Table* t, cudaStream_t s) {
+  const int L = g->L, tp = g->theta_pad, na = t->n < 0 ? -t->n : t->n;
+  t->row_off.assign(L + 2, 0);
+  for (int m = 0; m <= L; m++) {
+    const int l0 = m > na ? m : na;
+    t->row_off[m + 1] = t->row_off[m] + (L - l0 + 1);
+  }
+  t->rows = t->row_off[L + 1];
+  GSHT_CUDA(cudaMalloc(&t->d_row_off, sizeof(long long) * (L + 2)));
+  GSHT_CUDA(cudaMemcpy(t->d_row_off, t->row_off.data(),
+                       sizeof(long long) * (L + 2), cudaMemcpyHostToDevice));
+  const size_t elems = (size_t)(t->rows + kTablePadRows) * tp;
+  if (cudaMalloc(&t->t64, sizeof(double) * elems) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(GSHT_ERR_OOM, "table allocation of %zu bytes failed",
+                sizeof(double) * elems);
+  }
+  GSHT_CUDA(cudaMemsetAsync(t->t64, 0, sizeof(double) * elems, s));
+  double* start_f = nullptr;
+  int* start_e = nullptr;
+  GSHT_CUDA(cudaMalloc(&start_f, sizeof(double) * (size_t)(L + 1) * tp));
+  GSHT_CUDA(cudaMalloc(&start_e, sizeof(int) * (size_t)(L + 1) * tp));
+  k_wigner_start<<<(g->n_theta + 127) / 128, 128, 0, s>>>(
+      L, t->n, g->n_theta, tp, g->d_theta, start_f, start_e);
+  GSHT_LAUNCH_CHECK("k_wigner_start");
+  const size_t shmem = sizeof(double) * 4 * (L + 1);
+  if (shmem > 48 * 1024) {
+    GSHT_CUDA(cudaFuncSetAttribute(k_wigner_chain,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)shmem));
+  }
+  dim3 grid((tp + 127) / 128, L + 1);
+  k_wigner_chain<<<grid, 128, shmem, s>>>(L, t->n, g->n_theta, tp, g->d_theta,
+                                          start_f, start_e, t->d_row_off,
+                                          t->t64);
+  GSHT_LAUNCH_CHECK("k_wigner_chain");
+  GSHT_CUDA(cudaStreamSynchronize(s));
+  cudaFree(start_f);
+  cudaFree(start_e);
+  return GSHT_OK;
+}
+
+gsht_status build_forms(gsht_grid* g, Table* t, cudaStream_t s) {
+  const int L = g->L, tp = g->theta_pad;
+  const size_t plane = (size_t)(t->rows + kTablePadRows) * tp;
+  if (g->forms & GSHT_FORM_BF16X3) {
+    if (cudaMalloc(&t->tbf, sizeof(__nv_bfloat16) * 3 * plane) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(GSHT_ERR_OOM, "BF16 table allocation failed");
+    }
+    GSHT_CUDA(cudaMemsetAsync(t->tbf, 0, sizeof(__nv_bfloat16) * 3 * plane, s));
+    k_split_bf16<<<148 * 8, 256, 0, s>>>((size_t)t->rows * tp, t->t64, t->tbf,
+                                         plane);
+    GSHT_LAUNCH_CHECK("k_split_bf16");
+  }
+  if (g->forms & GSHT_FORM_OZAKI) {
+    if (cudaMalloc(&t->ti8, (size_t)kTableSlices * plane) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(GSHT_ERR_OOM, "INT8 slice allocation failed");
+    }
+    GSHT_CUDA(cudaMemsetAsync(t->ti8, 0, (size_t)kTableSlices * plane, s));
+    GSHT_CUDA(cudaMalloc(&t->i8_exp, sizeof(int) * (size_t)(L + 1) * tp));
+    dim3 grid((tp + 127) / 128, L + 1);
+    k_slice_i8<<<grid, 128, 0, s>>>(L, t->n, tp, t->d_row_off, t->t64, t->ti8,
+                                    plane, t->i8_exp);
+    GSHT_LAUNCH_CHECK("k_slice_i8");
+  }
+  GSHT_CUDA(cudaStreamSynchronize(s));
+  return GSHT_OK;
+}
+
+void free_table(Table* t) {
+  cudaFree(t->d_row_off);
+  cudaFree(t->t64);
+  cudaFree(t->tbf);
+  cudaFree(t->ti8);
+  cudaFree(t->i8_exp);
+  *t = Table{};
+}
+
+}  // namespace gsht

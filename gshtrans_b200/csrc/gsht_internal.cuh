@@ -1,0 +1,179 @@
+// Internal declarations shared by the CUDA translation units of
+// libgsht_cuda.so. Nothing here is part of the C ABI (include/gsht.h).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gsht.h"
+
+namespace gsht {
+
+// ---------------------------------------------------------------------------
+// Errors and launch accounting
+// ---------------------------------------------------------------------------
+gsht_status fail(gsht_status s, const char* fmt, ...);
+gsht_status cuda_fail(cudaError_t e, const char* what);
+extern std::atomic<unsigned long long> g_launches;
+
+#define GSHT_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return gsht::cuda_fail(e_, #call); \
+  } while (0)
+
+// Marks one kernel launch and checks the launch status.
+#define GSHT_LAUNCH_CHECK(name)                                    \
+  do {                                                             \
+    gsht::g_launches.fetch_add(1, std::memory_order_relaxed);      \
+    cudaError_t e_ = cudaGetLastError();                           \
+    if (e_ != cudaSuccess) return gsht::cuda_fail(e_, name);       \
+  } while (0)
+
+inline long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
+
+// Brackets one stage of a transform call with CUDA events while stage
+// profiling is enabled (gsht_profile_enable); otherwise does nothing.
+class StageTimer {
+ public:
+  StageTimer(int stage, cudaStream_t s);
+  ~StageTimer();
+  StageTimer(const StageTimer&) = delete;
+  StageTimer& operator=(const StageTimer&) = delete;
+
+ private:
+  int stage_;
+  cudaStream_t s_;
+  cudaEvent_t a_ = nullptr, b_ = nullptr;
+  unsigned long long launches0_ = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Layout constants
+// ---------------------------------------------------------------------------
+// Row pitch (in elements) of every table and spectral buffer along the
+// colatitude axis: nTheta rounded up to kThetaPad.
+constexpr int kThetaPad = 16;
+// Padding of the degree axis of field-side operands (K of the inverse GEMM).
+constexpr int kDegreePadFp64 = 16;
+constexpr int kDegreePadTc = 128;
+// Ozaki slice count of the table (7 bits per slice).
+constexpr int kTableSlices = 7;
+// Extra zero rows allocated after every table so that tile over-reads stay
+// inside the allocation.
+constexpr int kTablePadRows = 256;
+
+// Per upper index n: Wigner table for orders m = 0..L, degrees
+// l = l0(m)..L with l0(m) = max(m, |n|), colatitudes j = 0..nThetaPad-1.
+// Row (m, l) lives at row_off[m] + (l - l0(m)); element (row, j) at
+// row * thetaPad + j. Negative orders follow from
+// d^l_{-m,n}(pi - theta) = (-1)^{l+n} d^l_{mn}(theta) on the symmetric
+// Gauss-Legendre colatitudes.
+struct Table {
+  int n = 0;
+  long long rows = 0;                 // sum over m of K_m = L - l0(m) + 1
+  std::vector<long long> row_off;     // host, size L+2
+  long long* d_row_off = nullptr;     // device copy
+  double* t64 = nullptr;              // FP64 values
+  __nv_bfloat16* tbf = nullptr;       // 3 planes (hi, mid, lo), same layout
+  int8_t* ti8 = nullptr;              // kTableSlices planes, same layout
+  int* i8_exp = nullptr;              // (L+1) x thetaPad column exponents
+};
+
+// Per-order layout of field-side operand rows for one (lmax, |n|, rows,
+// padding): order m owns `rows` rows of pitch[m] = round_up(lmax - l0(m) + 1,
+// pad) elements starting at off[m]. Built once per key and cached on the grid.
+struct OperandLayout {
+  int lmax = 0, na = 0, rows = 0, pad = 0;
+  std::vector<long long> off;  // host, size lmax + 2 (off[lmax+1] = total)
+  std::vector<int> pitch;      // host, size lmax + 1
+  long long* d_off = nullptr;
+  int* d_pitch = nullptr;
+  long long total = 0;
+  int pitch_max = 0;
+};
+
+}  // namespace gsht
+
+// The opaque handle of the C ABI.
+struct gsht_grid {
+  int L = 0;           // grid degree (MaxDegree)
+  int nmax = 0;        // MaxUpperIndex
+  int min_n = 0;       // MinUpperIndex
+  int mrange = 0;      // GSHT_RANGE_ALL / NONNEGATIVE
+  int nrange = 0;
+  unsigned forms = 0;  // GSHT_FORM_* built
+  int device = 0;
+  int n_theta = 0, n_phi = 0, theta_pad = 0;
+
+  std::vector<double> h_theta, h_weight;  // host copies of the nodes
+  double* d_theta = nullptr;              // device nodes
+  double* d_weight = nullptr;
+  double* d_twiddle = nullptr;            // FFT twiddles exp(-2 pi i t / nPhi), t < nPhi
+  double* d_twiddle_half = nullptr;       // twiddles of length nPhi/2 (real-field FFTs)
+
+  std::vector<gsht::Table> tables;        // index n - min_n
+
+  // Workspace shared by the transform calls on this grid.
+  std::mutex mu;
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  cudaEvent_t ws_done = nullptr;  // recorded after the last call's kernels
+  // Cached operand layouts (guarded by mu).
+  mutable std::vector<gsht::OperandLayout*> layouts;
+
+  const gsht::Table* table(int n) const {
+    if (n < min_n || n > nmax) return nullptr;
+    return &tables[n - min_n];
+  }
+};
+
+namespace gsht {
+
+// Table build (grid.cu).
+gsht_status build_nodes(gsht_grid* g);
+gsht_status build_table(gsht_grid* g, Table* t, cudaStream_t s);
+gsht_status build_forms(gsht_grid* g, Table* t, cudaStream_t s);
+void free_table(Table* t);
+
+// FFT stage (fft.cu). spec: spectral buffer [m][sgn][f][j] complex.
+gsht_status fft_inverse(const gsht_grid* g, int lmax, int is_real, int count,
+                        const double* spec, double* out, cudaStream_t s);
+gsht_status fft_forward(const gsht_grid* g, int lmax, int is_real, int count,
+                        const double* in, double* spec, cudaStream_t s);
+
+// Legendre stage, FP64 (legendre_fp64.cu).
+size_t fp64_operand_elems(const gsht_grid* g, const Table* t, int lmax,
+                          int is_real, int count);
+gsht_status legendre_inverse_fp64(const gsht_grid* g, const Table* t, int lmax,
+                                  int is_real, int count, const double* coef,
+                                  double* operand, double* spec,
+                                  cudaStream_t s);
+gsht_status legendre_forward_fp64(const gsht_grid* g, const Table* t, int lmax,
+                                  int is_real, int count, const double* spec,
+                                  double* coef, cudaStream_t s);
+
+// Cached operand layout (legendre_fp64.cu); the caller holds g->mu.
+const OperandLayout* operand_layout(const gsht_grid* g, int lmax, int na,
+                                    int rows, int pad, gsht_status* st);
+void free_layouts(gsht_grid* g);
+
+// Spectral buffer element count: (lmax+1) x sgn x count x thetaPad complex.
+inline size_t spec_elems(const gsht_grid* g, int lmax, int is_real, int count) {
+  const int sgn = is_real ? 1 : 2;
+  return (size_t)(lmax + 1) * sgn * count * g->theta_pad;
+}
+
+inline long coef_size(int lmax, int n, int is_real) {
+  const long na = n < 0 ? -n : n;
+  if (is_real) return (long)(lmax + 1) * (lmax + 2) / 2 - na * (na + 1) / 2;
+  return (long)(lmax + 1) * (lmax + 1) - (long)n * n;
+}
+
+}  // namespace gsht

@@ -1,0 +1,149 @@
+/*
+ * gsht.h — C ABI of libgsht_cuda.so, the B200 (sm_100a) implementation of the
+ * Gauss-Legendre generalized-spherical-harmonic transforms of GSHTrans.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, status codes. Each entry
+ * point names the reference interface it replaces (paths relative to the
+ * GSHTrans source tree). The C++ drop-in headers (GSHTrans/Core in this
+ * repository) and any FFI binding call only these functions.
+ *
+ * Conventions shared with the reference:
+ *   - grid: nTheta = L+1 Gauss-Legendre colatitudes theta_j = acos(-x_j)
+ *     ascending from the north pole, nPhi = 2L longitudes phi_k = k*pi/L;
+ *     field values are ring-major (theta outer, phi inner), real or complex
+ *     (interleaved re/im doubles) — CanonicalComponentField.h:122-124.
+ *   - coefficients: complex (interleaved re/im doubles) in GSHIndices<All>
+ *     order for complex fields (index l^2 - n^2 + l + m) and
+ *     GSHIndices<NonNegative> order for real fields (index
+ *     l(l+1)/2 - |n|(|n|+1)/2 + m) — Indexing.h:104-131,143-146.
+ *   - forward ACCUMULATES into its output (c += ...), and for complex fields
+ *     with lmax == L sets c_{L,L} = 0 — GaussLegendreGrid.h:186-215.
+ *   - FFTs are unnormalised with FFTW's sign conventions.
+ *
+ * Pointers may be host or device memory (detected per call). With device
+ * pointers a call only enqueues work on `stream` (NULL = legacy default
+ * stream); with any host pointer the call copies through the grid's
+ * workspace and returns after the results are in host memory.
+ * Calls that share one grid handle share its workspace: they are ordered on
+ * the GPU (each call waits for the previous one), whichever streams they use.
+ */
+#ifndef GSHT_H
+#define GSHT_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gsht_status {
+  GSHT_OK = 0,
+  GSHT_ERR_BAD_ARG = 1,     /* the reference asserts instead: GaussLegendreGrid.h:41-44,126-134,240-248 */
+  GSHT_ERR_OOM = 2,         /* device or host allocation failed */
+  GSHT_ERR_CUDA = 3,        /* a CUDA runtime/driver call failed */
+  GSHT_ERR_TIMEOUT = 4,     /* a bounded device-side wait expired */
+  GSHT_ERR_UNSUPPORTED = 5, /* form not built for this grid, or unsupported shape */
+  GSHT_ERR_NO_DEVICE = 6    /* no CUDA device visible */
+} gsht_status;
+
+/* Index ranges — Concepts.h:24-27 (All, NonNegative, Single). */
+enum { GSHT_RANGE_ALL = 0, GSHT_RANGE_NONNEGATIVE = 1, GSHT_RANGE_SINGLE = 2 };
+
+/* Legendre-stage precision of a transform call. */
+enum {
+  GSHT_FP64 = 0,   /* FP64 tensor-core (DMMA) contraction: the drop-in path   */
+  GSHT_BF16X3 = 1, /* hi/mid/lo BF16 split products, FP32 accumulation       */
+  GSHT_OZAKI = 2   /* Ozaki INT8 slices, exact INT32 accumulation, FP64 sum   */
+};
+
+/* Table forms built by gsht_grid_create (bit mask). */
+enum { GSHT_FORM_FP64 = 1, GSHT_FORM_BF16X3 = 2, GSHT_FORM_OZAKI = 4 };
+
+typedef struct gsht_grid gsht_grid;
+
+/* Replaces GaussLegendreGrid<double, MRange, NRange>(lMax, nMax, flag)
+ * (GaussLegendreGrid.h:38-73) and the Wigner table it builds
+ * (Wigner<double, Ortho, MRange, NRange, Multiple, ColumnMajor>,
+ * Wigner.h:116-137): computes the Gauss-Legendre nodes and the Wigner tables
+ * for every upper index in the NRange (GridBase.h:17-33) on the GPU.
+ * mrange: GSHT_RANGE_ALL or GSHT_RANGE_NONNEGATIVE; nrange: any range;
+ * forms: GSHT_FORM_* mask (FP64 is always built). */
+gsht_status gsht_grid_create(int lmax, int nmax, int mrange, int nrange,
+                             unsigned forms, gsht_grid** grid);
+
+/* Releases the grid, its tables and its workspace. */
+gsht_status gsht_grid_destroy(gsht_grid* grid);
+
+/* MaxDegree / MaxUpperIndex / MinUpperIndex / NumberOfCoLatitudes /
+ * NumberOfLongitudes (GaussLegendreGrid.h:86-87, GridBase.h:17-45). Any
+ * output pointer may be NULL. */
+gsht_status gsht_grid_shape(const gsht_grid* grid, int* lmax, int* nmax,
+                            int* min_n, int* n_theta, int* n_phi);
+
+/* CoLatitudes() and CoLatitudeWeights() (GaussLegendreGrid.h:89-92) into
+ * host arrays of n_theta doubles (either may be NULL). */
+gsht_status gsht_grid_nodes(const gsht_grid* grid, double* colatitudes,
+                            double* weights);
+
+/* Wigner::operator[](n, iTheta) (Wigner.h:241-244): copies the table block
+ * d^l_{mn}(theta_iTheta), l = |n|..L, in the reference's block layout
+ * (GSHIndices<MRange>(L, L, n), Indexing.h:104-131) into host memory. If
+ * out is NULL only *count is set. */
+gsht_status gsht_wigner_block(const gsht_grid* grid, int n, int itheta,
+                              double* out, long* count);
+
+/* Coefficient count for (lmax, n): GridBase.h:79-85 (Real/ComplexCoefficientSize). */
+long gsht_coefficient_size(int lmax, int n, int is_real);
+
+/* ForwardTransformation(lMax, n, in, out) (GaussLegendreGrid.h:108-217):
+ * grid values -> coefficients, accumulated into out. */
+gsht_status gsht_forward(const gsht_grid* grid, int lmax, int n, int is_real,
+                         int precision, const void* in, void* out,
+                         void* stream);
+
+/* InverseTransformation(lMax, n, in, out) (GaussLegendreGrid.h:222-321):
+ * coefficients -> grid values (out overwritten). */
+gsht_status gsht_inverse(const gsht_grid* grid, int lmax, int n, int is_real,
+                         int precision, const void* in, void* out,
+                         void* stream);
+
+/* Batched forms: `count` fields of the same (lmax, n, is_real), stored back
+ * to back (field i at in + i * field_size, out + i * coefficient_size; sizes
+ * in elements of the respective type). One call runs each stage once for the
+ * whole batch, sharing the Wigner table across the fields. */
+gsht_status gsht_forward_batch(const gsht_grid* grid, int lmax, int n,
+                               int is_real, int precision, int count,
+                               const void* in, void* out, void* stream);
+gsht_status gsht_inverse_batch(const gsht_grid* grid, int lmax, int n,
+                               int is_real, int precision, int count,
+                               const void* in, void* out, void* stream);
+
+/* Stage timing. No counterpart in the reference (which has no tracing):
+ * while enabled, every stage of a transform call is bracketed by CUDA events
+ * recorded on the call's stream; gsht_profile_read synchronises those events
+ * and returns, per stage, the summed device milliseconds and the number of
+ * kernel launches. Enabling clears earlier records. */
+enum {
+  GSHT_STAGE_PREP_INVERSE = 0,     /* coefficients -> per-order operand rows   */
+  GSHT_STAGE_LEGENDRE_INVERSE = 1, /* order-wise contraction, inverse          */
+  GSHT_STAGE_FFT_INVERSE = 2,      /* ring FFTs, inverse                       */
+  GSHT_STAGE_FFT_FORWARD = 3,      /* ring FFTs, forward                       */
+  GSHT_STAGE_PREP_FORWARD = 4,     /* spectra -> per-order operand rows        */
+  GSHT_STAGE_LEGENDRE_FORWARD = 5, /* order-wise contraction, forward          */
+  GSHT_STAGE_COUNT = 6
+};
+gsht_status gsht_profile_enable(int on);
+gsht_status gsht_profile_read(double* ms, long* launches, int nstages);
+
+/* Message describing the last non-OK status returned on this thread. */
+const char* gsht_last_error(void);
+
+/* Number of kernels this library has launched in this process (used to
+ * count device work inside timed regions). */
+unsigned long long gsht_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSHT_H */

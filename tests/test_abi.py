@@ -1,0 +1,64 @@
+"""The C-ABI library loads and exports every symbol include/gsht.h declares;
+host-side validation that needs no GPU."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+import oracle
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "gsht.h")).read()
+    return sorted(set(re.findall(r"\b(gsht_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    import gshtrans_b200 as g
+
+    syms = declared_symbols()
+    assert len(syms) >= 12
+    for s in syms:
+        assert hasattr(g.library, s), s
+
+
+def test_coefficient_sizes_match_reference_layout():
+    import gshtrans_b200 as g
+
+    for lmax in (0, 1, 5, 64, 1024):
+        for n in range(-min(lmax, 3), min(lmax, 3) + 1):
+            assert g.coefficient_size(lmax, n, False) == oracle.size_all(lmax, n)
+            assert g.coefficient_size(lmax, n, True) == oracle.size_nonneg(lmax, n)
+    with pytest.raises(g.BadArgument):
+        g.coefficient_size(2, 3, False)
+
+
+def test_grid_create_rejects_bad_arguments_before_touching_a_device():
+    import gshtrans_b200 as g
+
+    lib = g.library
+    h = ctypes.c_void_p()
+    assert lib.gsht_grid_create(0, 0, 0, 0, 1, ctypes.byref(h)) == 1
+    assert b"lmax" in lib.gsht_last_error()
+    assert lib.gsht_grid_create(8, 9, 0, 0, 1, ctypes.byref(h)) == 1
+    assert lib.gsht_grid_create(8, 2, 2, 0, 1, ctypes.byref(h)) == 1
+    assert lib.gsht_grid_create(8, 2, 0, 0, 64, ctypes.byref(h)) == 1
+    assert lib.gsht_grid_create(8, 2, 0, 0, 1, None) == 1
+
+
+def test_no_device_is_reported_not_faked():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    import gshtrans_b200 as g
+
+    with pytest.raises(g.GSHTError) as e:
+        g.GaussLegendreGrid(8, 2)
+    assert e.value.status == 6

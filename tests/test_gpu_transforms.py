@@ -1,0 +1,186 @@
+"""FP64 GPU transforms (the drop-in path) against the reference.
+
+ForwardTransformation / InverseTransformation (GaussLegendreGrid.h:108-321)
+are compared with the golden fixtures the reference produced, with the C
+restatement on fresh seeded inputs (random grid degrees as in
+tests/CheckCoeff2Coeff.h), and with the reference build where present. The
+bar is the FP64 drop-in tolerance: 1e-13 norm-wise relative error.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden_cases, relerr
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-13  # norm-wise relative, FP64 path vs the reference
+
+
+@pytest.fixture(scope="module")
+def gsht():
+    import gshtrans_b200
+
+    return gshtrans_b200
+
+
+def _grid_zero(g, is_real):
+    return np.zeros(g.FieldSize(), np.float64 if is_real else np.complex128)
+
+
+def test_golden_transforms(gsht, golden):
+    tr = golden["transforms"]
+    grids = {}
+    for i, L, lmax, n, is_real in golden_cases(tr):
+        key = (L, max(abs(n), 3))
+        if key not in grids:
+            grids[key] = gsht.GaussLegendreGrid(L, key[1])
+        g = grids[key]
+        c = tr[f"c{i}_coef"]
+        f = _grid_zero(g, is_real)
+        g.InverseTransformation(lmax, n, c, f)
+        if lmax == 0:
+            assert f[0] == pytest.approx(tr[f"c{i}_grid"][0], rel=1e-15)
+            assert np.all(f[1:] == 0)
+        else:
+            assert relerr(f, tr[f"c{i}_grid"]) < TOL, i
+        out = np.zeros_like(c)
+        g.ForwardTransformation(lmax, n, tr[f"c{i}_grid"], out)
+        assert relerr(out, tr[f"c{i}_fwd"]) < TOL, i
+        acc = tr[f"c{i}_acc_init"].copy()
+        g.ForwardTransformation(lmax, n, tr[f"c{i}_grid"], acc)
+        assert relerr(acc, tr[f"c{i}_acc"]) < TOL, i
+        if not is_real and lmax == L:
+            assert acc[-1] == 0  # c_{L,L} zeroed (GaussLegendreGrid.h:209-215)
+    for g in grids.values():
+        g.close()
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_random_sizes_vs_restated(gsht, restated, seed):
+    # tests/CheckCoeff2Coeff.h:40-84 with seeds: lMaxGrid in [4, 256],
+    # lMax in [4, lMaxGrid], nMax = min(lMax, 4), n in [-nMax, nMax];
+    # nPhi = 2 lMaxGrid takes arbitrary even lengths (generic FFT radices).
+    rng = np.random.default_rng(1000 + seed)
+    L = int(rng.integers(4, 257))
+    lmax = int(rng.integers(4, L + 1))
+    nmax = min(lmax, 4)
+    n = int(rng.integers(-nmax, nmax + 1))
+    with gsht.GaussLegendreGrid(L, nmax) as g:
+        for is_real in (False, True):
+            c = oracle.random_coefficients(rng, L, lmax, n, is_real)
+            f = _grid_zero(g, is_real)
+            g.InverseTransformation(lmax, n, c, f)
+            f_orc = restated.inverse(L, lmax, n, is_real, c)
+            assert relerr(f, f_orc) < TOL
+            out = np.zeros_like(c)
+            g.ForwardTransformation(lmax, n, f, out)
+            c_orc = restated.forward(L, lmax, n, is_real, f)
+            assert relerr(out, c_orc) < TOL
+            # the reference round-trip test: 50000 eps absolute
+            assert np.max(np.abs(out - c)) < 50000 * np.finfo(float).eps
+
+
+def test_nrange_single_and_nonnegative(gsht, restated):
+    L = 24
+    rng = np.random.default_rng(7)
+    for nrange, ns in ((gsht.Single, (3,)), (gsht.NonNegative, (0, 2, 3))):
+        with gsht.GaussLegendreGrid(L, 3, nrange=nrange) as g:
+            assert list(g.UpperIndices()) == (list(range(0, 4)) if nrange == gsht.NonNegative else [3])
+            for n in ns:
+                c = oracle.random_coefficients(rng, L, L, n, False)
+                f = _grid_zero(g, False)
+                g.InverseTransformation(L, n, c, f)
+                assert relerr(f, restated.inverse(L, L, n, False, c)) < TOL
+            with pytest.raises(gsht.BadArgument):
+                g.InverseTransformation(L, -1, oracle.random_coefficients(rng, L, L, -1, False), _grid_zero(g, False))
+
+
+def test_mrange_nonnegative_real_fields(gsht, restated):
+    L = 20
+    rng = np.random.default_rng(8)
+    with gsht.GaussLegendreGrid(L, 2, mrange=gsht.NonNegative) as g:
+        c = oracle.random_coefficients(rng, L, L, -2, True)
+        f = _grid_zero(g, True)
+        g.InverseTransformation(L, -2, c, f)
+        assert relerr(f, restated.inverse(L, L, -2, True, c)) < TOL
+        out = np.zeros_like(c)
+        g.ForwardTransformation(L, -2, f, out)
+        assert relerr(out, restated.forward(L, L, -2, True, f)) < TOL
+        # complex fields need MRange = All (GaussLegendreGrid.h:110-112)
+        with pytest.raises(gsht.BadArgument):
+            g.InverseTransformation(L, 0, oracle.random_coefficients(rng, L, L, 0, False), _grid_zero(g, False))
+
+
+def test_bad_arguments_raise(gsht):
+    with gsht.GaussLegendreGrid(16, 2) as g:
+        c = np.zeros(gsht.coefficient_size(16, 0, False), np.complex128)
+        f = _grid_zero(g, False)
+        with pytest.raises(gsht.BadArgument):
+            g.InverseTransformation(17, 0, c, f)  # lmax above the grid degree
+        with pytest.raises(gsht.BadArgument):
+            g.InverseTransformation(16, 3, c, f)  # n outside the grid range
+        with pytest.raises(gsht.BadArgument):
+            g.InverseTransformation(16, 0, c[:-1], f)  # wrong size
+        with pytest.raises(gsht.BadArgument):
+            g.InverseTransformation(1, -2, np.zeros(4, np.complex128), f)  # |n| > lmax
+
+
+def test_device_tensors_and_batches_match_single_host_calls(gsht):
+    import torch
+
+    L, n, B = 48, -1, 5
+    rng = np.random.default_rng(9)
+    with gsht.GaussLegendreGrid(L, 2) as g:
+        for is_real in (False, True):
+            cs = [oracle.random_coefficients(rng, L, L, n, is_real) for _ in range(B)]
+            singles = []
+            for c in cs:
+                f = _grid_zero(g, is_real)
+                g.InverseTransformation(L, n, c, f)
+                singles.append(f)
+            dc = torch.from_numpy(np.stack(cs)).cuda()
+            df = torch.zeros((B, g.FieldSize()), dtype=torch.float64 if is_real else torch.complex128, device="cuda")
+            g.inverse_batch(L, n, dc, df)
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(df.cpu().numpy(), np.stack(singles))
+            back = torch.zeros_like(dc)
+            g.forward_batch(L, n, df, back)
+            torch.cuda.synchronize()
+            for b in range(B):
+                out = np.zeros_like(cs[b])
+                g.ForwardTransformation(L, n, singles[b], out)
+                np.testing.assert_array_equal(back[b].cpu().numpy(), out)
+
+
+@pytest.mark.parametrize("n,is_real", [(0, False), (2, True), (-2, False)])
+def test_L1024_vs_reference_and_round_trip(gsht, n, is_real):
+    # lmax 1024, n in {0, +2, -2}, real and complex fields,
+    # envelope (l+1)^-1.5. Parity against the reference build where present,
+    # else against the C restatement.
+    import oracle as O
+
+    L = 1024
+    rng = np.random.default_rng(2024 + n)
+    c = O.random_coefficients(rng, L, L, n, is_real, 1.5)
+    with gsht.GaussLegendreGrid(L, abs(n), nrange=gsht.Single if n >= 0 else gsht.All) as g:
+        f = _grid_zero(g, is_real)
+        g.InverseTransformation(L, n, c, f)
+        back = np.zeros_like(c)
+        g.ForwardTransformation(L, n, f, back)
+    assert relerr(back, c) < 1e-12
+    if O.Reference.available() and n >= 0:
+        # NRange = Single keeps the reference's host table at one upper index.
+        r = O.Reference().grid(L, n, 0, 2)
+        f_ref = r.inverse(L, n, is_real, c)
+        c_ref = r.forward(L, n, is_real, f_ref)
+        r.close()
+    else:
+        R = O.Restated()
+        f_ref = R.inverse(L, L, n, is_real, c)
+        c_ref = R.forward(L, L, n, is_real, f_ref)
+    assert relerr(f, f_ref) < TOL
+    assert relerr(back, c_ref) < TOL
