@@ -71,6 +71,9 @@ def _load() -> ctypes.CDLL:
         f.argtypes = [vp, ip, ip, ip, ip, vp, vp, vp]
     for f in (lib.gsht_forward_batch, lib.gsht_inverse_batch):
         f.argtypes = [vp, ip, ip, ip, ip, ip, vp, vp, vp]
+    lib.gsht_device_status.argtypes = [vp]
+    lib.gsht_profile_enable.argtypes = [ip]
+    lib.gsht_profile_read.argtypes = [vp, vp, ip]
     lib.gsht_last_error.restype = ctypes.c_char_p
     lib.gsht_launch_count.restype = ctypes.c_ulonglong
     return lib
@@ -241,6 +244,10 @@ class GaussLegendreGrid:
                                          out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                          ctypes.byref(cnt)))
         return out
+
+    def device_status(self):
+        """Synchronises and raises GSHTError(TIMEOUT) if a kernel gave up a bounded wait."""
+        _check(library.gsht_device_status(self._h))
 
     # ---- transforms (GaussLegendreGrid.h:108-321) ----
     def ForwardTransformation(self, lmax: int, n: int, in_, out, precision="fp64"):

@@ -121,8 +121,12 @@ gsht_status validate(const gsht_grid* g, int lmax, int n, int is_real,
     return fail(GSHT_ERR_BAD_ARG, "|n| = %d exceeds lmax = %d", n < 0 ? -n : n, lmax);
   if (!is_real && g->mrange != GSHT_RANGE_ALL)
     return fail(GSHT_ERR_BAD_ARG, "complex fields need MRange = All");
-  if (precision != GSHT_FP64)
+  if (precision != GSHT_FP64 && precision != GSHT_BF16X3 && precision != GSHT_OZAKI)
     return fail(GSHT_ERR_UNSUPPORTED, "precision %d not available", precision);
+  if (precision == GSHT_BF16X3 && !(g->forms & GSHT_FORM_BF16X3))
+    return fail(GSHT_ERR_UNSUPPORTED, "the BF16x3 table form was not built for this grid");
+  if (precision == GSHT_OZAKI && !(g->forms & GSHT_FORM_OZAKI))
+    return fail(GSHT_ERR_UNSUPPORTED, "the Ozaki table form was not built for this grid");
   return GSHT_OK;
 }
 
@@ -153,8 +157,14 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
   // Workspace: [spec][operand][in staging][out staging], 256-byte aligned.
   const size_t specBytes = lmax > 0 ? sizeof(double) * 2 * spec_elems(g, lmax, is_real, count) : 0;
   size_t opBytes = 0;
-  if (dir == 1 && lmax > 0)
-    opBytes = sizeof(double) * 2 * fp64_operand_elems(g, t, lmax, is_real, count);
+  if (lmax > 0) {
+    if (precision == GSHT_BF16X3)
+      opBytes = bf16_operand_bytes(g, lmax, is_real, count, dir);
+    else if (precision == GSHT_OZAKI)
+      opBytes = oz_operand_bytes(g, lmax, is_real, count, dir);
+    else if (dir == 1)
+      opBytes = sizeof(double) * 2 * fp64_operand_elems(g, t, lmax, is_real, count);
+  }
   size_t off = 0;
   auto carve = [&](size_t b) { size_t o = off; off += round_up(b, 256); return o; };
   const size_t oSpec = carve(specBytes), oOp = carve(opBytes);
@@ -183,14 +193,24 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
         st = fft_forward(g, lmax, is_real, count, dIn, spec, s);
       }
       if (st != GSHT_OK) return st;
-      {
+      if (precision == GSHT_BF16X3) {
+        st = legendre_forward_bf16(g, t, lmax, is_real, count, spec, ws + oOp, dOut, s);
+      } else if (precision == GSHT_OZAKI) {
+        st = legendre_forward_oz(g, t, lmax, is_real, count, spec, ws + oOp, dOut, s);
+      } else {
         StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
         st = legendre_forward_fp64(g, t, lmax, is_real, count, spec, dOut, s);
       }
       if (st != GSHT_OK) return st;
     } else {
-      double* op = reinterpret_cast<double*>(ws + oOp);
-      st = legendre_inverse_fp64(g, t, lmax, is_real, count, dIn, op, spec, s);
+      if (precision == GSHT_BF16X3) {
+        st = legendre_inverse_bf16(g, t, lmax, is_real, count, dIn, ws + oOp, spec, s);
+      } else if (precision == GSHT_OZAKI) {
+        st = legendre_inverse_oz(g, t, lmax, is_real, count, dIn, ws + oOp, spec, s);
+      } else {
+        double* op = reinterpret_cast<double*>(ws + oOp);
+        st = legendre_inverse_fp64(g, t, lmax, is_real, count, dIn, op, spec, s);
+      }
       if (st != GSHT_OK) return st;
       {
         StageTimer tm(GSHT_STAGE_FFT_INVERSE, s);
@@ -202,7 +222,15 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
   if (!outDev) GSHT_CUDA(cudaMemcpyAsync(out, dOut, outBytes, cudaMemcpyDeviceToHost, s));
   if (!g->ws_done) GSHT_CUDA(cudaEventCreateWithFlags(&g->ws_done, cudaEventDisableTiming));
   GSHT_CUDA(cudaEventRecord(g->ws_done, s));
-  if (!inDev || !outDev) GSHT_CUDA(cudaStreamSynchronize(s));
+  if (!inDev || !outDev) {
+    GSHT_CUDA(cudaStreamSynchronize(s));
+    int err = 0;
+    GSHT_CUDA(cudaMemcpy(&err, g->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+      cudaMemset(g->d_err, 0, sizeof(int));
+      return fail(GSHT_ERR_TIMEOUT, "a bounded device wait expired (code %d)", err);
+    }
+  }
   return GSHT_OK;
 }
 
@@ -243,6 +271,11 @@ gsht_status gsht_grid_create(int lmax, int nmax, int mrange, int nrange,
   g->n_phi = 2 * lmax;
   g->theta_pad = (int)round_up(g->n_theta, kThetaPad);
   gsht_status st = build_nodes(g);
+  if (st == GSHT_OK && (cudaMalloc(&g->d_err, sizeof(int)) != cudaSuccess ||
+                        cudaMemset(g->d_err, 0, sizeof(int)) != cudaSuccess)) {
+    cudaGetLastError();
+    st = fail(GSHT_ERR_OOM, "error word allocation failed");
+  }
   if (st == GSHT_OK) {
     // Twiddles exp(-2 pi i t / nPhi), t < nPhi, rounded from long double.
     std::vector<double> tw(2 * (size_t)g->n_phi);
@@ -286,7 +319,7 @@ gsht_status gsht_grid_destroy(gsht_grid* g) {
   cudaFree(g->d_theta);
   cudaFree(g->d_weight);
   cudaFree(g->d_twiddle);
-  cudaFree(g->d_twiddle_half);
+  cudaFree(g->d_err);
   cudaFree(g->ws);
   if (g->ws_done) cudaEventDestroy(g->ws_done);
   delete g;
@@ -403,6 +436,19 @@ gsht_status gsht_profile_read(double* ms, long* launches, int nstages) {
       if (ms) ms[r.stage] += t;
       if (launches) launches[r.stage] += (long)r.launches;
     }
+  }
+  return GSHT_OK;
+}
+
+gsht_status gsht_device_status(const gsht_grid* g) {
+  if (!g) return fail(GSHT_ERR_BAD_ARG, "grid is NULL");
+  GSHT_CUDA(cudaSetDevice(g->device));
+  GSHT_CUDA(cudaDeviceSynchronize());
+  int err = 0;
+  GSHT_CUDA(cudaMemcpy(&err, g->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    GSHT_CUDA(cudaMemset(g->d_err, 0, sizeof(int)));
+    return fail(GSHT_ERR_TIMEOUT, "a bounded device wait expired (code %d)", err);
   }
   return GSHT_OK;
 }

@@ -60,42 +60,54 @@ __device__ __forceinline__ dd dd_div_d(dd a, double b) {
   return quick_two_sum(q1, r);
 }
 
-// P_n(x) and P_{n-1}(x) by the three-term recurrence
+// P_n(x), P_{n-1}(x) and P_{n-2}(x) by the three-term recurrence
 // (k+1) P_{k+1} = (2k+1) x P_k - k P_{k-1}, in double-double.
-__device__ void legendre_dd(int n, double x, dd* pn, dd* pnm1) {
-  dd p0 = {1.0, 0.0}, p1 = {x, 0.0};
+__device__ void legendre_dd(int n, double x, dd* pn, dd* pnm1, dd* pnm2) {
+  dd p0 = {1.0, 0.0}, p1 = {x, 0.0}, pm = {0.0, 0.0};
   for (int k = 1; k < n; k++) {
     dd t = dd_mul(two_prod(x, (double)(2 * k + 1)), p1);
     dd u = dd_mul_d(p0, (double)k);
     dd p2 = dd_div_d(dd_add(t, dd_neg(u)), (double)(k + 1));
+    pm = p0;
     p0 = p1;
     p1 = p2;
   }
   *pn = p1;
   *pnm1 = p0;
+  *pnm2 = pm;
 }
 
 // One thread per node pair (x_i, x_{n-1-i} = -x_i): Newton on P_n from the
 // asymptotic guess, residuals in double-double so that the iteration settles
 // on the double nearest the root; theta = acos(-x) (GaussLegendreGrid.h:48).
+// The weight w = 2 (1 - r^2) / (n P_{n-1}(r))^2 is taken at the root r, not
+// at its double rounding x: with delta = r - x = -P_n(x)/P_n'(x) (first order,
+// P_n in double-double), P_{n-1}(r) = P_{n-1}(x) + P_{n-1}'(x) delta and
+// 1 - r^2 = (1 - x)(1 + x) - 2 x delta. Near the poles P_n' ~ n^2, so the
+// uncorrected form would be off by ~1e-8 relative at lmax 1024.
 __global__ void k_gl_nodes(int n, double* theta, double* weight) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (n + 1) / 2) return;
   double x = -cospi((i + 0.75) / (n + 0.5));
-  dd pn, pnm1;
+  dd pn, pnm1, pnm2;
   for (int it = 0; it < 60; it++) {
-    legendre_dd(n, x, &pn, &pnm1);
+    legendre_dd(n, x, &pn, &pnm1, &pnm2);
     const double dp = n * (x * pn.hi - pnm1.hi) / (x * x - 1.0);
     const double xn = x - pn.hi / dp;
     if (xn == x) break;
     x = xn;
   }
   if (2 * i + 1 == n) x = 0.0;
-  legendre_dd(n, x, &pn, &pnm1);
-  // w = 2 (1 - x^2) / (n P_{n-1}(x))^2 at a root of P_n.
-  const double omx2 = (1.0 - x) * (1.0 + x);
-  const double q = n * pnm1.hi;
-  const double w = 2.0 * omx2 / (q * q);
+  legendre_dd(n, x, &pn, &pnm1, &pnm2);
+  double w = 2.0;
+  if (n >= 2) {
+    const double dp = n * (x * pn.hi - pnm1.hi) / (x * x - 1.0);
+    const double delta = -(pn.hi + pn.lo) / dp;
+    const double dq = (n - 1) * (x * pnm1.hi - pnm2.hi) / (x * x - 1.0);
+    const double q = n * (pnm1.hi + (pnm1.lo + dq * delta));
+    const double omr2 = (1.0 - x) * (1.0 + x) - 2.0 * x * delta;
+    w = 2.0 * omr2 / (q * q);
+  }
   // North node: theta = acos(-x) with -x in (0, 1]. South node: theta =
   // acos(x) = pi - acos(-x), formed with a split pi.
   const double tn = acos(-x);

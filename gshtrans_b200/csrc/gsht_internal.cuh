@@ -116,7 +116,7 @@ struct gsht_grid {
   double* d_theta = nullptr;              // device nodes
   double* d_weight = nullptr;
   double* d_twiddle = nullptr;            // FFT twiddles exp(-2 pi i t / nPhi), t < nPhi
-  double* d_twiddle_half = nullptr;       // twiddles of length nPhi/2 (real-field FFTs)
+  int* d_err = nullptr;                   // device error word (bounded-wait timeouts)
 
   std::vector<gsht::Table> tables;        // index n - min_n
 
@@ -158,6 +158,25 @@ gsht_status legendre_inverse_fp64(const gsht_grid* g, const Table* t, int lmax,
 gsht_status legendre_forward_fp64(const gsht_grid* g, const Table* t, int lmax,
                                   int is_real, int count, const double* spec,
                                   double* coef, cudaStream_t s);
+
+// Legendre stage, BF16x3 on tcgen05 (legendre_tc.cu). dir 0 = forward
+// (operand rows over colatitudes), 1 = inverse (rows over degrees).
+size_t bf16_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir);
+gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                                  int count, const double* coef, void* operand, double* spec,
+                                  cudaStream_t s);
+gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                                  int count, const double* spec, void* operand, double* coef,
+                                  cudaStream_t s);
+
+// Legendre stage, Ozaki INT8 slices on tcgen05 (legendre_oz.cu).
+size_t oz_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir);
+gsht_status legendre_inverse_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                                int count, const double* coef, void* operand, double* spec,
+                                cudaStream_t s);
+gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                                int count, const double* spec, void* operand, double* coef,
+                                cudaStream_t s);
 
 // Cached operand layout (legendre_fp64.cu); the caller holds g->mu.
 const OperandLayout* operand_layout(const gsht_grid* g, int lmax, int na,

@@ -135,6 +135,12 @@ enum {
 gsht_status gsht_profile_enable(int on);
 gsht_status gsht_profile_read(double* ms, long* launches, int nstages);
 
+/* Synchronises the grid's device and reports GSHT_ERR_TIMEOUT if a kernel
+ * gave up a bounded wait since the last check (the word is then cleared).
+ * No counterpart in the reference, which has no device code. Calls with
+ * host buffers perform this check themselves. */
+gsht_status gsht_device_status(const gsht_grid* grid);
+
 /* Message describing the last non-OK status returned on this thread. */
 const char* gsht_last_error(void);
 

@@ -1,0 +1,166 @@
+"""Tensor-core forms of the Legendre stage against the FP64 path.
+
+BF16x3 (tcgen05 kind::f16, six hi/mid/lo split products, FP32 accumulation
+in TMEM) must stay within 1e-6 norm-wise relative error of the FP64 drop-in
+path, in both directions, for every field kind the reference supports.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden_cases, relerr
+
+pytestmark = pytest.mark.gpu
+
+TOL_BF16 = 1e-6
+
+
+@pytest.fixture(scope="module")
+def gsht():
+    import gshtrans_b200
+
+    return gshtrans_b200
+
+
+def _zeros_grid(g, is_real, count=None):
+    shape = g.FieldSize() if count is None else (count, g.FieldSize())
+    return np.zeros(shape, np.float64 if is_real else np.complex128)
+
+
+def _both(g, lmax, n, is_real, c, precision):
+    f = _zeros_grid(g, is_real)
+    g.InverseTransformation(lmax, n, c, f, precision)
+    back = np.zeros_like(c)
+    g.ForwardTransformation(lmax, n, f, back, precision)
+    g.device_status()
+    return f, back
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_bf16x3_random_sizes_vs_fp64(gsht, seed):
+    rng = np.random.default_rng(500 + seed)
+    L = int(rng.integers(4, 257))
+    lmax = int(rng.integers(max(4, L // 2), L + 1))
+    nmax = min(lmax, 4)
+    n = int(rng.integers(-nmax, nmax + 1))
+    with gsht.GaussLegendreGrid(L, nmax, forms=("bf16x3",)) as g:
+        for is_real in (False, True):
+            c = oracle.random_coefficients(rng, L, lmax, n, is_real, 1.0)
+            f64, b64 = _both(g, lmax, n, is_real, c, "fp64")
+            f16, b16 = _both(g, lmax, n, is_real, c, "bf16x3")
+            assert relerr(f16, f64) < TOL_BF16
+            # forward alone, on the same (FP64) grid values
+            out = np.zeros_like(c)
+            g.ForwardTransformation(lmax, n, f64, out, "bf16x3")
+            assert relerr(out, b64) < TOL_BF16
+            assert relerr(b16, c) < 3 * TOL_BF16
+
+
+def test_bf16x3_golden(gsht, golden):
+    tr = golden["transforms"]
+    grids = {}
+    for i, L, lmax, n, is_real in golden_cases(tr):
+        if lmax == 0:
+            continue
+        key = (L, max(abs(n), 3))
+        if key not in grids:
+            grids[key] = gsht.GaussLegendreGrid(L, key[1], forms=("bf16x3",))
+        g = grids[key]
+        f = _zeros_grid(g, is_real)
+        g.InverseTransformation(lmax, n, tr[f"c{i}_coef"], f, "bf16x3")
+        assert relerr(f, tr[f"c{i}_grid"]) < TOL_BF16, i
+        acc = tr[f"c{i}_acc_init"].copy()
+        g.ForwardTransformation(lmax, n, tr[f"c{i}_grid"], acc, "bf16x3")
+        assert relerr(acc, tr[f"c{i}_acc"]) < TOL_BF16, i
+    for g in grids.values():
+        g.close()
+
+
+@pytest.mark.parametrize("n,is_real", [(0, False), (0, True), (2, False), (-2, True)])
+def test_bf16x3_L1024_batched(gsht, n, is_real):
+    # configs[1] shapes: lmax 1024, n in {0, +-2}, envelope (l+1)^-1.5.
+    import torch
+
+    L, B = 1024, 4
+    rng = np.random.default_rng(77 + n)
+    c = np.stack([oracle.random_coefficients(rng, L, L, n, is_real, 1.5) for _ in range(B)])
+    with gsht.GaussLegendreGrid(L, abs(n), forms=("bf16x3",)) as g:
+        dc = torch.from_numpy(c).cuda()
+        res = {}
+        for prec in ("fp64", "bf16x3"):
+            f = torch.zeros((B, g.FieldSize()), dtype=torch.float64 if is_real else torch.complex128, device="cuda")
+            g.inverse_batch(L, n, dc, f, prec)
+            back = torch.zeros_like(dc)
+            g.forward_batch(L, n, f, back, prec)
+            g.device_status()
+            res[prec] = (f.cpu().numpy(), back.cpu().numpy())
+    assert relerr(res["bf16x3"][0], res["fp64"][0]) < TOL_BF16
+    assert relerr(res["bf16x3"][1], res["fp64"][1]) < 2 * TOL_BF16
+
+
+# --- Ozaki INT8 slices (tcgen05 kind::i8, exact INT32 accumulation) --------
+
+TOL_OZ = 1e-12
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_ozaki_random_sizes_vs_fp64(gsht, seed):
+    rng = np.random.default_rng(900 + seed)
+    L = int(rng.integers(4, 257))
+    lmax = int(rng.integers(max(4, L // 2), L + 1))
+    nmax = min(lmax, 4)
+    n = int(rng.integers(-nmax, nmax + 1))
+    with gsht.GaussLegendreGrid(L, nmax, forms=("ozaki",)) as g:
+        for is_real in (False, True):
+            c = oracle.random_coefficients(rng, L, lmax, n, is_real, 1.0)
+            f64, b64 = _both(g, lmax, n, is_real, c, "fp64")
+            foz, boz = _both(g, lmax, n, is_real, c, "ozaki")
+            assert relerr(foz, f64) < TOL_OZ
+            out = np.zeros_like(c)
+            g.ForwardTransformation(lmax, n, f64, out, "ozaki")
+            assert relerr(out, b64) < TOL_OZ
+            assert np.max(np.abs(boz - c)) < 50000 * np.finfo(float).eps
+
+
+def test_ozaki_golden(gsht, golden):
+    tr = golden["transforms"]
+    grids = {}
+    for i, L, lmax, n, is_real in golden_cases(tr):
+        if lmax == 0:
+            continue
+        key = (L, max(abs(n), 3))
+        if key not in grids:
+            grids[key] = gsht.GaussLegendreGrid(L, key[1], forms=("ozaki",))
+        g = grids[key]
+        f = _zeros_grid(g, is_real)
+        g.InverseTransformation(lmax, n, tr[f"c{i}_coef"], f, "ozaki")
+        assert relerr(f, tr[f"c{i}_grid"]) < TOL_OZ, i
+        acc = tr[f"c{i}_acc_init"].copy()
+        g.ForwardTransformation(lmax, n, tr[f"c{i}_grid"], acc, "ozaki")
+        assert relerr(acc, tr[f"c{i}_acc"]) < TOL_OZ, i
+    for g in grids.values():
+        g.close()
+
+
+@pytest.mark.parametrize("n,is_real", [(0, False), (0, True), (2, False), (-2, True)])
+def test_ozaki_L1024_batched(gsht, n, is_real):
+    import torch
+
+    L, B = 1024, 4
+    rng = np.random.default_rng(177 + n)
+    c = np.stack([oracle.random_coefficients(rng, L, L, n, is_real, 1.5) for _ in range(B)])
+    with gsht.GaussLegendreGrid(L, abs(n), forms=("ozaki",)) as g:
+        dc = torch.from_numpy(c).cuda()
+        res = {}
+        for prec in ("fp64", "ozaki"):
+            f = torch.zeros((B, g.FieldSize()), dtype=torch.float64 if is_real else torch.complex128, device="cuda")
+            g.inverse_batch(L, n, dc, f, prec)
+            back = torch.zeros_like(dc)
+            g.forward_batch(L, n, f, back, prec)
+            g.device_status()
+            res[prec] = (f.cpu().numpy(), back.cpu().numpy())
+    assert relerr(res["ozaki"][0], res["fp64"][0]) < TOL_OZ
+    assert relerr(res["ozaki"][1], res["fp64"][1]) < TOL_OZ
