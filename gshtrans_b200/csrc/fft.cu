@@ -233,11 +233,303 @@ __global__ void __launch_bounds__(256) k_fft_forward(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Register-staged path: R rings per block, every thread owns kVPT points;
+// each Stockham stage loads its butterflies' inputs into registers, syncs,
+// and writes the outputs back in place (one buffer of R*n points). Radices
+// 8, 4, 2 and 3; lengths whose factorisation has other primes use the
+// generic path above.
+// ---------------------------------------------------------------------------
+template <int P>
+__device__ __forceinline__ void dft_reg(double2 (&c)[P], int sign);
+
+template <>
+__device__ __forceinline__ void dft_reg<2>(double2 (&c)[2], int) {
+  const double2 a = cadd(c[0], c[1]), b = csub(c[0], c[1]);
+  c[0] = a;
+  c[1] = b;
+}
+
+template <>
+__device__ __forceinline__ void dft_reg<4>(double2 (&c)[4], int sign) {
+  const double2 s02 = cadd(c[0], c[2]), d02 = csub(c[0], c[2]);
+  const double2 s13 = cadd(c[1], c[3]), d13 = cmul_si(csub(c[1], c[3]), sign);
+  c[0] = cadd(s02, s13);
+  c[1] = cadd(d02, d13);
+  c[2] = csub(s02, s13);
+  c[3] = csub(d02, d13);
+}
+
+template <>
+__device__ __forceinline__ void dft_reg<8>(double2 (&c)[8], int sign) {
+  double2 e[4] = {c[0], c[2], c[4], c[6]};
+  double2 o[4] = {c[1], c[3], c[5], c[7]};
+  dft_reg<4>(e, sign);
+  dft_reg<4>(o, sign);
+  const double h = 0.70710678118654752440;  // 1/sqrt(2)
+  const double sg = (double)sign;
+  // o[r] *= exp(sign 2 pi i r / 8), r = 1..3
+  o[1] = make_double2(h * (o[1].x - sg * o[1].y), h * (o[1].y + sg * o[1].x));
+  o[2] = cmul_si(o[2], sign);
+  o[3] = make_double2(h * (-o[3].x - sg * o[3].y), h * (-o[3].y + sg * o[3].x));
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    c[r] = cadd(e[r], o[r]);
+    c[r + 4] = csub(e[r], o[r]);
+  }
+}
+
+template <>
+__device__ __forceinline__ void dft_reg<3>(double2 (&c)[3], int sign) {
+  const double s3 = 0.86602540378443864676;  // sqrt(3)/2
+  const double2 t = cadd(c[1], c[2]);
+  const double2 u = cmul_si(csub(c[1], c[2]), sign);
+  const double2 x0 = cadd(c[0], t);
+  const double2 b = make_double2(c[0].x - 0.5 * t.x, c[0].y - 0.5 * t.y);
+  c[0] = x0;
+  c[1] = make_double2(b.x + s3 * u.x, b.y + s3 * u.y);
+  c[2] = make_double2(b.x - s3 * u.x, b.y - s3 * u.y);
+}
+
+template <int P, int NB>
+__device__ __forceinline__ void reg_stage(double2* buf, int n, int l, int m,
+                                          const double2* __restrict__ tw, int twStride,
+                                          int sign) {
+  const int nbr = n / P;
+  double2 v[NB][P];
+#pragma unroll
+  for (int b = 0; b < NB; b++) {
+    const int idx = threadIdx.x + b * 256;
+    const int ring = idx / nbr, bi = idx - ring * nbr;
+    const int j = bi / m, k = bi - j * m;
+    const int src = ring * n + k + j * m;
+#pragma unroll
+    for (int q = 0; q < P; q++) v[b][q] = buf[src + q * l * m];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < NB; b++) {
+    const int idx = threadIdx.x + b * 256;
+    const int ring = idx / nbr, bi = idx - ring * nbr;
+    const int j = bi / m, k = bi - j * m;
+    dft_reg<P>(v[b], sign);
+    const int t = j * m;
+    if (t) {
+#pragma unroll
+      for (int r = 1; r < P; r++) v[b][r] = cmul(v[b][r], twiddle(tw, t * r, twStride, sign));
+    }
+    const int dst = ring * n + k + j * P * m;
+#pragma unroll
+    for (int r = 0; r < P; r++) buf[dst + r * m] = v[b][r];
+  }
+  __syncthreads();
+}
+
+template <int kVPT>
+__device__ void fft_reg(double2* buf, const FftPlan& plan, const double2* __restrict__ tw,
+                        int sign) {
+  const int n = plan.n;
+  int l = n, m = 1;
+  for (int s = 0; s < plan.stages; s++) {
+    const int p = plan.radix[s];
+    l /= p;
+    if (p == 8) {
+      if constexpr (kVPT % 8 == 0) reg_stage<8, kVPT / 8>(buf, n, l, m, tw, plan.tw_stride, sign);
+    } else if (p == 4) {
+      reg_stage<4, kVPT / 4>(buf, n, l, m, tw, plan.tw_stride, sign);
+    } else if (p == 2) {
+      reg_stage<2, kVPT / 2>(buf, n, l, m, tw, plan.tw_stride, sign);
+    } else {
+      if constexpr (kVPT % 3 == 0) reg_stage<3, kVPT / 3>(buf, n, l, m, tw, plan.tw_stride, sign);
+    }
+    m *= p;
+  }
+}
+
+// Inverse, R rings per block: block (ring group, field).
+template <bool kReal, int kVPT>
+__global__ void __launch_bounds__(256) k_fft_inverse_reg(
+    FftPlan plan, int R, int L, int lmax, int nTheta, int thetaPad, int count,
+    const double2* __restrict__ spec, const double2* __restrict__ tw,
+    double* __restrict__ out) {
+  extern __shared__ double2 smem[];
+  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int nPhi = 2 * L, n = plan.n;
+  const int sgnCount = kReal ? 1 : 2;
+  auto S = [&](int m, int sgn, int jj) {
+    return spec[((size_t)(m * sgnCount + sgn) * count + f) * thetaPad + jj];
+  };
+  if (!kReal) {
+    for (int e = threadIdx.x; e < R * nPhi; e += 256) {
+      const int r = e % R, bin = e / R;
+      const int j = j0 + r;
+      double2 x = make_double2(0.0, 0.0);
+      if (j < nTheta) {
+        if (bin <= lmax) x = S(bin, 0, j);
+        if (bin >= nPhi - lmax) x = cadd(x, S(nPhi - bin, 1, nTheta - 1 - j));
+      }
+      smem[r * n + bin] = x;
+    }
+  } else {
+    const int M = L;
+    for (int e = threadIdx.x; e < R * M; e += 256) {
+      const int r = e % R, bin = e / R;
+      const int j = j0 + r;
+      double2 z = make_double2(0.0, 0.0);
+      if (j < nTheta) {
+        const int bc = M - bin;
+        double2 x0 = bin <= lmax ? S(bin, 0, j) : make_double2(0.0, 0.0);
+        double2 x1 = bc <= lmax ? S(bc, 0, j) : make_double2(0.0, 0.0);
+        if (bin == 0) x0.y = 0.0;
+        if (bc == M) x1.y = 0.0;
+        const double2 xc = cconj(x1);
+        const double2 w = twiddle(tw, bin, 1, +1);
+        z = cadd(cadd(x0, xc), cmul_si(cmul(w, csub(x0, xc)), +1));
+      }
+      smem[r * n + bin] = z;
+    }
+  }
+  __syncthreads();
+  fft_reg<kVPT>(smem, plan, tw, +1);
+  for (int e = threadIdx.x; e < R * n; e += 256) {
+    const int r = e / n, k = e - r * n;
+    const int j = j0 + r;
+    if (j >= nTheta) continue;
+    if (!kReal) {
+      reinterpret_cast<double2*>(out)[((size_t)f * nTheta + j) * nPhi + k] = smem[e];
+    } else {
+      reinterpret_cast<double2*>(out + ((size_t)f * nTheta + j) * nPhi)[k] = smem[e];
+    }
+  }
+}
+
+// Forward, R rings per block.
+template <bool kReal, int kVPT>
+__global__ void __launch_bounds__(256) k_fft_forward_reg(
+    FftPlan plan, int R, int L, int lmax, int nTheta, int thetaPad, int count,
+    const double* __restrict__ in, const double* __restrict__ weight,
+    const double2* __restrict__ tw, double2* __restrict__ spec) {
+  extern __shared__ double2 smem[];
+  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int nPhi = 2 * L, n = plan.n;
+  const int sgnCount = kReal ? 1 : 2;
+  auto S = [&](int m, int sgn, int jj) -> double2& {
+    return spec[((size_t)(m * sgnCount + sgn) * count + f) * thetaPad + jj];
+  };
+  if (j0 <= nTheta - 1 && nTheta - 1 < j0 + R) {
+    const int padW = thetaPad - nTheta;
+    for (int i = threadIdx.x; i < (lmax + 1) * sgnCount * padW; i += 256) {
+      const int q = i / padW, jj = nTheta + (i - q * padW);
+      S(q / sgnCount, q % sgnCount, jj) = make_double2(0.0, 0.0);
+    }
+  }
+  for (int e = threadIdx.x; e < R * n; e += 256) {
+    const int r = e / n, k = e - r * n;
+    const int j = j0 + r;
+    double2 x = make_double2(0.0, 0.0);
+    if (j < nTheta) {
+      if (!kReal) {
+        x = reinterpret_cast<const double2*>(in)[((size_t)f * nTheta + j) * nPhi + k];
+      } else {
+        x = reinterpret_cast<const double2*>(in + ((size_t)f * nTheta + j) * nPhi)[k];
+      }
+    }
+    smem[e] = x;
+  }
+  __syncthreads();
+  fft_reg<kVPT>(smem, plan, tw, -1);
+  const double twoPiOverN = 6.283185307179586477 / nPhi;
+  for (int e = threadIdx.x; e < R * (lmax + 1); e += 256) {
+    const int r = e % R, m = e / R;
+    const int j = j0 + r;
+    if (j >= nTheta) continue;
+    const double scale = weight[j] * twoPiOverN;
+    const double2* X = smem + r * n;
+    if (!kReal) {
+      S(m, 0, j) = cscale(X[m], scale);
+      S(m, 1, nTheta - 1 - j) = m ? cscale(X[nPhi - m], scale) : make_double2(0.0, 0.0);
+    } else {
+      const int M = L;
+      const double2 z0 = X[m == M ? 0 : m];
+      const double2 zc = cconj(X[m == 0 ? 0 : M - m]);
+      const double2 w = twiddle(tw, m, 1, -1);
+      const double2 ev = cscale(cadd(z0, zc), 0.5);
+      const double2 od = cscale(cmul_si(csub(z0, zc), -1), 0.5);
+      S(m, 0, j) = cscale(cadd(ev, cmul(w, od)), scale);
+    }
+  }
+}
+
+// Register-path configuration for a transform length: points per thread
+// kVPT in {16, 24, 32} and rings per block R = kVPT * 256 / n, or 0 if the
+// length needs the generic path.
+struct RegConfig {
+  int vpt = 0, rings = 0;
+  FftPlan plan{};
+};
+
+RegConfig reg_config(int n, int tableLen) {
+  RegConfig c;
+  FftPlan p{};
+  p.n = n;
+  p.tw_stride = tableLen / n;
+  int m = n, s = 0;
+  while (m % 8 == 0) { p.radix[s++] = 8; m /= 8; }
+  while (m % 4 == 0) { p.radix[s++] = 4; m /= 4; }
+  while (m % 2 == 0) { p.radix[s++] = 2; m /= 2; }
+  while (m % 3 == 0) { p.radix[s++] = 3; m /= 3; }
+  if (m != 1 || n < 8) return c;
+  p.stages = s;
+  for (int vpt : {16, 24, 32}) {
+    if ((vpt * 256) % n) continue;
+    bool ok = true;
+    for (int i = 0; i < s; i++) ok = ok && (vpt % p.radix[i] == 0);
+    if (!ok) continue;
+    c.vpt = vpt;
+    c.rings = vpt * 256 / n;
+    c.plan = p;
+    return c;
+  }
+  return c;
+}
+
+template <int kVPT>
+gsht_status launch_inverse_reg(const gsht_grid* g, const RegConfig& c, int lmax, int is_real,
+                               int count, const double* spec, double* out, cudaStream_t s) {
+  const size_t shmem = sizeof(double2) * kVPT * 256;
+  dim3 grid((g->n_theta + c.rings - 1) / c.rings, count);
+  auto kr = is_real ? k_fft_inverse_reg<true, kVPT> : k_fft_inverse_reg<false, kVPT>;
+  GSHT_CUDA(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
+  kr<<<grid, 256, shmem, s>>>(c.plan, c.rings, g->L, lmax, g->n_theta, g->theta_pad, count,
+                              reinterpret_cast<const double2*>(spec),
+                              reinterpret_cast<const double2*>(g->d_twiddle), out);
+  GSHT_LAUNCH_CHECK("k_fft_inverse_reg");
+  return GSHT_OK;
+}
+
+template <int kVPT>
+gsht_status launch_forward_reg(const gsht_grid* g, const RegConfig& c, int lmax, int is_real,
+                               int count, const double* in, double* spec, cudaStream_t s) {
+  const size_t shmem = sizeof(double2) * kVPT * 256;
+  dim3 grid((g->n_theta + c.rings - 1) / c.rings, count);
+  auto kf = is_real ? k_fft_forward_reg<true, kVPT> : k_fft_forward_reg<false, kVPT>;
+  GSHT_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
+  kf<<<grid, 256, shmem, s>>>(c.plan, c.rings, g->L, lmax, g->n_theta, g->theta_pad, count,
+                              in, g->d_weight, reinterpret_cast<const double2*>(g->d_twiddle),
+                              reinterpret_cast<double2*>(spec));
+  GSHT_LAUNCH_CHECK("k_fft_forward_reg");
+  return GSHT_OK;
+}
+
 }  // namespace
 
 gsht_status fft_inverse(const gsht_grid* g, int lmax, int is_real, int count,
                         const double* spec, double* out, cudaStream_t s) {
   const int N = g->n_phi;
+  const RegConfig rc = reg_config(is_real ? N / 2 : N, N);
+  if (rc.vpt == 16) return launch_inverse_reg<16>(g, rc, lmax, is_real, count, spec, out, s);
+  if (rc.vpt == 24) return launch_inverse_reg<24>(g, rc, lmax, is_real, count, spec, out, s);
+  if (rc.vpt == 32) return launch_inverse_reg<32>(g, rc, lmax, is_real, count, spec, out, s);
   const FftPlan plan = make_plan(is_real ? N / 2 : N, N);
   const size_t shmem = sizeof(double2) * 2 * plan.n;
   dim3 grid(g->n_theta, count);
@@ -263,6 +555,10 @@ gsht_status fft_inverse(const gsht_grid* g, int lmax, int is_real, int count,
 gsht_status fft_forward(const gsht_grid* g, int lmax, int is_real, int count,
                         const double* in, double* spec, cudaStream_t s) {
   const int N = g->n_phi;
+  const RegConfig rc = reg_config(is_real ? N / 2 : N, N);
+  if (rc.vpt == 16) return launch_forward_reg<16>(g, rc, lmax, is_real, count, in, spec, s);
+  if (rc.vpt == 24) return launch_forward_reg<24>(g, rc, lmax, is_real, count, in, spec, s);
+  if (rc.vpt == 32) return launch_forward_reg<32>(g, rc, lmax, is_real, count, in, spec, s);
   const FftPlan plan = make_plan(is_real ? N / 2 : N, N);
   const size_t shmem = sizeof(double2) * 2 * plan.n;
   dim3 grid(g->n_theta, count);

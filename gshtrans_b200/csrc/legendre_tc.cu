@@ -9,7 +9,7 @@
 // batch's field rows (r = 2 q + re/im, q = sign x field) are operand B
 // (N = 128). In the BF16x3 form both operands are split into hi/mid/lo BF16
 // planes and six split products (hi.hi, hi.mid, mid.hi, hi.lo, lo.hi,
-// mid.mid) accumulate into one FP32 TMEM accumulator.
+// mid.mid) accumulate in FP32 in TMEM.
 //
 // Warp roles (192 threads): warp 0 issues TMA loads, warp 1 owns TMEM and
 // issues MMAs from one lane, warps 2-5 drain TMEM in the epilogue. Every
@@ -36,6 +36,13 @@ struct TcArgs {
   long coefSize;
   int* err;
 };
+
+// TMEM accumulators per tile: products of very different magnitude would
+// otherwise share one FP32 accumulator whose every update truncates; hi.hi
+// goes to up to kBigAcc accumulators by K block and the other five products to
+// a separate one, all summed in FP64 in the epilogue (4 x 128 = 512 columns).
+constexpr int kBigAcc = 3;
+constexpr int kAccumulators = kBigAcc + 1;
 
 // Products of the BF16x3 form: (A split, B split).
 __host__ __device__ constexpr int prodA(int p) { return p == 0 ? 0 : p == 1 ? 0 : p == 2 ? 1 : p == 3 ? 0 : p == 4 ? 2 : 1; }
@@ -85,7 +92,7 @@ __global__ void __launch_bounds__(192, 1)
     prefetch_tmap(&mapA);
     prefetch_tmap(&mapB);
   }
-  if (warp == 1) tmem_alloc(tmemSlot, kN);
+  if (warp == 1) tmem_alloc(tmemSlot, kAccumulators * kN);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -115,6 +122,9 @@ __global__ void __launch_bounds__(192, 1)
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t id = idesc(1, 1, kDir == 0 ? 1 : 0, 0, kN, kBM);
+      // hi.hi products go to one of nbig accumulators by K block; the five
+      // smaller products share accumulator 0 (see kAccumulators).
+      const int nbig = nk < kBigAcc ? nk : kBigAcc;
       bool ok = true;
       for (int kc = 0; kc < nk && ok; kc++) {
         const int s = kc % kStages;
@@ -123,17 +133,22 @@ __global__ void __launch_bounds__(192, 1)
           break;
         }
         tc_fence_after();
+        const int big = 1 + (kc * nbig) / nk;
+        const int bigFirst = ((big - 1) * nk + nbig - 1) / nbig;
         const uint32_t st = smem_u32(smem + s * kStageBytes);
 #pragma unroll
         for (int pr = 0; pr < kNP; pr++) {
           const uint32_t aBase = st + prodA(pr) * kTileA;
           const uint32_t bBase = st + kNA * kTileA + prodB(pr) * kTileB;
+          const uint32_t d = tmem + (uint32_t)((pr == 0 ? big : 0) * kN);
 #pragma unroll
           for (int k16 = 0; k16 < kBK / 16; k16++) {
             const uint64_t ad = kDir == 0 ? sdesc_sw128(aBase + k16 * 2048, kTileA / 2, 1024)
                                           : sdesc_sw128(aBase + k16 * 32, 16, 1024);
             const uint64_t bd = sdesc_sw128(bBase + k16 * 32, 16, 1024);
-            mma_f16(tmem, ad, bd, id, (kc | pr | k16) != 0);
+            const bool first = pr == 0 ? (kc == bigFirst && k16 == 0)
+                                       : (kc == 0 && k16 == 0 && pr == 1);
+            mma_f16(d, ad, bd, id, first ? 0u : 1u);
           }
         }
         mma_commit(&empty[s]);
@@ -148,19 +163,27 @@ __global__ void __launch_bounds__(192, 1)
     tc_fence_after();
     if (ready) {
       const int tileRow = mtile * kBM + row;
+      const int nbig = nk < kBigAcc ? nk : kBigAcc;
 #pragma unroll 1
       for (int c = 0; c < kN / 16; c++) {
-        uint32_t v[16];
-        tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + c * 16, v);
-        tmem_wait_ld();
+        double acc[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) acc[i] = 0.0;
+#pragma unroll 1
+        for (int a = 0; a <= nbig; a++) {
+          uint32_t v[16];
+          tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + a * kN + c * 16, v);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; i++) acc[i] += (double)__uint_as_float(v[i]);
+        }
         const int q0 = (ntile * kN + c * 16) / 2;
         if (tileRow >= rowsM) continue;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
           const int q = q0 + i;
           if (q >= p.Q) break;
-          double2 val = make_double2((double)__uint_as_float(v[2 * i]),
-                                     (double)__uint_as_float(v[2 * i + 1]));
+          double2 val = make_double2(acc[2 * i], acc[2 * i + 1]);
           if (kDir == 0) {
             p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] = val;
           } else {
@@ -190,7 +213,7 @@ __global__ void __launch_bounds__(192, 1)
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem, kN);
+    tmem_dealloc(tmem, kAccumulators * kN);
   }
 }
 
