@@ -211,29 +211,12 @@ def measured_fp64_peak(torch, dev):
     return best
 
 
-def impl_ours(args):
-    import torch
-    import torch.distributed as dist
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
+def measure_mode(gsht, grid, torch, dev, coef, field, back, precision, args, world, dist):
+    """Times args.steps round trips in one precision form (CUDA events on the
+    current stream, barrier + synchronize on both sides, MAX over ranks)."""
     import ctypes
 
-    import gshtrans_b200 as gsht
-
-    precision = args.precision or "fp64"
-    forms = () if precision == "fp64" else (precision,)
-    L, B = args.lmax, args.fields
-    grid = gsht.GaussLegendreGrid(L, N_UPPER, nrange=gsht.Single, forms=forms)
-    coef_h = coefficients(L, B, seed=rank)
-    coef = torch.from_numpy(coef_h).to(dev)
-    field = torch.empty((B, grid.FieldSize()), dtype=torch.complex128, device=dev)
-    back = torch.zeros_like(coef)
+    L = args.lmax
 
     def step():
         back.zero_()
@@ -243,8 +226,8 @@ def impl_ours(args):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    grid.device_status()
     rt_err = float(torch.linalg.norm(back - coef) / torch.linalg.norm(coef))
-
     lib = gsht.library
     lib.gsht_profile_enable(1)
     launches0 = gsht.launch_count()
@@ -252,7 +235,7 @@ def impl_ours(args):
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    with ClockSampler(torch.cuda.current_device()) as clk:
         e0.record()
         for _ in range(args.steps):
             step()
@@ -264,56 +247,144 @@ def impl_ours(args):
     launches = gsht.launch_count() - launches0
     stage_ms = (ctypes.c_double * 6)()
     stage_n = (ctypes.c_long * 6)()
-    lib.gsht_profile_read.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
-    lib.gsht_profile_read(ctypes.cast(stage_ms, ctypes.c_void_p), ctypes.cast(stage_n, ctypes.c_void_p), 6)
+    lib.gsht_profile_read(ctypes.cast(stage_ms, ctypes.c_void_p),
+                          ctypes.cast(stage_n, ctypes.c_void_p), 6)
     lib.gsht_profile_enable(0)
+    grid.device_status()
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    value = world * B * args.steps / (ms * 1e-3)
+    stages = {STAGES[i]: {"ms_per_step": stage_ms[i] / args.steps,
+                          "launches_per_step": stage_n[i] / args.steps} for i in range(6)}
+    return {"ms": ms, "launches": launches, "stages": stages, "clocks": clk.summary(),
+            "round_trip_rel_err": rt_err,
+            "legendre_ms": (stage_ms[1] + stage_ms[5]) / args.steps,
+            "legendre_launches": int(stage_n[1] + stage_n[5])}
 
-    # Roofline of the dominant kernel: the Legendre contraction (both
-    # directions), 4 flops per (table entry x complex field) per direction.
-    stages = {STAGES[i]: {"ms_total": stage_ms[i], "launches": int(stage_n[i])} for i in range(6)}
-    leg_ms = stage_ms[1] + stage_ms[5]
-    leg_launches = int(stage_n[1] + stage_n[5])
-    flops_per_step = 2 * 4.0 * B * ((L + 1) ** 2 - N_UPPER ** 2) * (L + 1)
-    achieved = flops_per_step * args.steps / (leg_ms * 1e-3) / 1e12 if leg_ms > 0 else None
-    peak = measured_fp64_peak(torch, dev) if precision == "fp64" else None
+
+def legendre_roofline(precision, res, args, peaks):
+    """Roofline of the dominant kernel, the per-order Legendre contraction
+    (inverse + forward launches). Algorithmic work: 4 flops per (table entry
+    x complex field) per direction; for the tensor-core forms the tensor-pipe
+    work is that times the split products (6 BF16 MMAs, 28 INT8 MMAs)."""
+    L, B = args.lmax, args.fields
+    entries = ((L + 1) ** 2 - N_UPPER ** 2) * (L + 1)
+    flops_per_dir = 4.0 * B * entries
+    t = res["legendre_ms"] * 1e-3 / 2  # per launch (one direction)
+    pipe = {"fp64": 1, "bf16x3": 6, "ozaki": 28}[precision]
+    achieved = pipe * flops_per_dir / t / 1e12
+    if precision == "fp64":
+        peak, src = peaks.get("fp64"), "cuBLAS DGEMM 8192^3 measured in this run"
+        unit = "TFLOP/s"
+    elif precision == "bf16x3":
+        peak, src = peaks.get("bf16"), "MEASURED_PEAKS.json bf16_tflops (burst, of measured)"
+        unit = "TFLOP/s"
+    else:
+        peak, src = peaks.get("int8"), "2 x MEASURED_PEAKS.json bf16_tflops (dense INT8 = 2x BF16 rate)"
+        unit = "TOP/s"
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get(f"legendre_{precision}")
-    roofline = {
-        "kernel": "k_legendre_fp64 (inverse + forward launches)" if precision == "fp64" else precision,
-        "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-        "frac": (achieved / peak) if (achieved and peak) else None,
-        "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in MEASURED_PEAKS.json)",
-        "algorithmic_flops_per_launch": flops_per_step / 2,
-        "avg_launch_ms": leg_ms / max(leg_launches, 1),
-        "traffic": traffic,
+    return {
+        "kernel": {"fp64": "k_legendre_fp64", "bf16x3": "k_legendre_tc (kind::f16)",
+                   "ozaki": "k_legendre_oz (kind::i8)"}[precision] + " inverse+forward",
+        "bound": "tensor", "achieved": achieved, "peak": peak, "unit": unit,
+        "frac": achieved / peak if peak else None, "peak_source": src,
+        "algorithmic_flops_per_launch": flops_per_dir,
+        "tensor_ops_per_launch": pipe * flops_per_dir,
+        "avg_launch_ms": 1e3 * t, "traffic": traffic,
     }
 
+
+def impl_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import gshtrans_b200 as gsht
+
+    modes = [args.precision] if args.precision else ["ozaki", "bf16x3", "fp64"]
+    headline = modes[0]
+    L, B = args.lmax, args.fields
+    grid = gsht.GaussLegendreGrid(L, N_UPPER, nrange=gsht.Single,
+                                  forms=[m for m in modes if m != "fp64"])
+    coef_h = coefficients(L, B, seed=rank)
+    coef = torch.from_numpy(coef_h).to(dev)
+    field = torch.empty((B, grid.FieldSize()), dtype=torch.complex128, device=dev)
+    back = torch.zeros_like(coef)
+
+    results = {m: measure_mode(gsht, grid, torch, dev, coef, field, back, m, args, world, dist)
+               for m in modes}
+    # accuracy of each form against the FP64 path on the same inputs
+    ref_f = ref_c = None
+    if "fp64" in modes and len(modes) > 1:
+        ref_f = torch.empty_like(field)
+        grid.inverse_batch(L, N_UPPER, coef, ref_f, "fp64")
+        ref_c = torch.zeros_like(coef)
+        grid.forward_batch(L, N_UPPER, ref_f, ref_c, "fp64")
+        for m in modes:
+            f = torch.empty_like(field)
+            grid.inverse_batch(L, N_UPPER, coef, f, m)
+            c = torch.zeros_like(coef)
+            grid.forward_batch(L, N_UPPER, ref_f, c, m)
+            results[m]["inverse_rel_err_vs_fp64"] = float(torch.linalg.norm(f - ref_f) / torch.linalg.norm(ref_f))
+            results[m]["forward_rel_err_vs_fp64"] = float(torch.linalg.norm(c - ref_c) / torch.linalg.norm(ref_c))
+            del f, c
+        del ref_f, ref_c
+    torch.cuda.synchronize()
+    peaks = {}
+    mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(mp):
+        mpj = json.load(open(mp))
+        peaks["bf16"] = mpj.get("bf16_tflops")
+        peaks["int8"] = 2 * mpj["bf16_tflops"] if mpj.get("bf16_tflops") else None
+    if "fp64" in modes:
+        peaks["fp64"] = measured_fp64_peak(torch, dev)
+
+    res = results[headline]
+    value = world * B * args.steps / (res["ms"] * 1e-3)
     result = None
     if rank == 0:
         e2e = None
         if not args.no_e2e:
-            e2e = e2e_run(gsht, grid, torch, coef_h, precision, args)
+            e2e = e2e_run(gsht, grid, torch, coef_h, headline, args)
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            res, why = reference_run(L, 1, 0)
-            cpu = ({k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
-                   if res else {"value": None, "unavailable": why})
+            rr, why = reference_run(L, 1, 0)
+            cpu = ({k: rr[k] for k in ("value", "unit", "cores", "kind", "sample")}
+                   if rr else {"value": None, "unavailable": why})
+        mode_lines = {}
+        for m in modes:
+            r = results[m]
+            mode_lines[m] = {
+                "value": world * B * args.steps / (r["ms"] * 1e-3), "unit": UNIT,
+                "ms_per_step": r["ms"] / args.steps,
+                "round_trip_rel_err": r["round_trip_rel_err"],
+                "inverse_rel_err_vs_fp64": r.get("inverse_rel_err_vs_fp64"),
+                "forward_rel_err_vs_fp64": r.get("forward_rel_err_vs_fp64"),
+                "stages": r["stages"],
+                "roofline": legendre_roofline(m, r, args, peaks),
+            }
+        if "fp64" in modes:
+            for m in modes:
+                mode_lines[m]["speedup_vs_fp64_gpu"] = mode_lines[m]["value"] / mode_lines["fp64"]["value"]
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": DTYPE[precision], "data": "synthetic",
-            "config": workload(args) | {"precision": precision, "parallelism": f"replicas x{world}"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "clocks": clk.summary(), "gpu_launches": launches,
-            "stages_ms": stages, "round_trip_rel_err": rt_err,
+            "dtype": DTYPE[headline], "data": "synthetic",
+            "config": workload(args) | {"precision": headline, "parallelism": f"replicas x{world}"},
+            "roofline": mode_lines[headline]["roofline"], "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": res["clocks"], "gpu_launches": res["launches"],
+            "round_trip_rel_err": res["round_trip_rel_err"], "modes": mode_lines,
         }
         print(json.dumps(result))
     grid.close()
