@@ -193,6 +193,20 @@ def impl_reference(args):
 # ---------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------
+def reduce_max_ms(ms: float, dist, device) -> float:
+    """Slowest rank's device time: the job's time for replicas run in parallel."""
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(rank: int) -> int:
+    """Each rank transforms its own fields (distinct seeded coefficients)."""
+    return 1000 + rank
+
+
 def measured_fp64_peak(torch, dev):
     """cuBLAS DGEMM throughput on this GPU (TFLOP/s), best of 3."""
     n = 8192
@@ -252,9 +266,7 @@ def measure_mode(gsht, grid, torch, dev, coef, field, back, precision, args, wor
     lib.gsht_profile_enable(0)
     grid.device_status()
     if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = reduce_max_ms(ms, dist, dev)
     stages = {STAGES[i]: {"ms_per_step": stage_ms[i] / args.steps,
                           "launches_per_step": stage_n[i] / args.steps} for i in range(6)}
     return {"ms": ms, "launches": launches, "stages": stages, "clocks": clk.summary(),
@@ -316,7 +328,7 @@ def impl_ours(args):
     L, B = args.lmax, args.fields
     grid = gsht.GaussLegendreGrid(L, N_UPPER, nrange=gsht.Single,
                                   forms=[m for m in modes if m != "fp64"])
-    coef_h = coefficients(L, B, seed=rank)
+    coef_h = coefficients(L, B, seed=replica_seed(rank))
     coef = torch.from_numpy(coef_h).to(dev)
     field = torch.empty((B, grid.FieldSize()), dtype=torch.complex128, device=dev)
     back = torch.zeros_like(coef)

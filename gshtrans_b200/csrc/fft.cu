@@ -291,6 +291,11 @@ __device__ __forceinline__ void dft_reg<3>(double2 (&c)[3], int sign) {
   c[2] = make_double2(b.x - s3 * u.x, b.y - s3 * u.y);
 }
 
+// Shared-memory index of point u in the register path: one 16-byte pad per
+// 8 points, so that the strided accesses of early Stockham stages (lane
+// stride 8 points) hit distinct bank groups.
+__device__ __forceinline__ int pad8(int u) { return u + (u >> 3); }
+
 template <int P, int NB>
 __device__ __forceinline__ void reg_stage(double2* buf, int n, int l, int m,
                                           const double2* __restrict__ tw, int twStride,
@@ -304,7 +309,7 @@ __device__ __forceinline__ void reg_stage(double2* buf, int n, int l, int m,
     const int j = bi / m, k = bi - j * m;
     const int src = ring * n + k + j * m;
 #pragma unroll
-    for (int q = 0; q < P; q++) v[b][q] = buf[src + q * l * m];
+    for (int q = 0; q < P; q++) v[b][q] = buf[pad8(src + q * l * m)];
   }
   __syncthreads();
 #pragma unroll
@@ -320,7 +325,7 @@ __device__ __forceinline__ void reg_stage(double2* buf, int n, int l, int m,
     }
     const int dst = ring * n + k + j * P * m;
 #pragma unroll
-    for (int r = 0; r < P; r++) buf[dst + r * m] = v[b][r];
+    for (int r = 0; r < P; r++) buf[pad8(dst + r * m)] = v[b][r];
   }
   __syncthreads();
 }
@@ -368,7 +373,7 @@ __global__ void __launch_bounds__(256) k_fft_inverse_reg(
         if (bin <= lmax) x = S(bin, 0, j);
         if (bin >= nPhi - lmax) x = cadd(x, S(nPhi - bin, 1, nTheta - 1 - j));
       }
-      smem[r * n + bin] = x;
+      smem[pad8(r * n + bin)] = x;
     }
   } else {
     const int M = L;
@@ -386,7 +391,7 @@ __global__ void __launch_bounds__(256) k_fft_inverse_reg(
         const double2 w = twiddle(tw, bin, 1, +1);
         z = cadd(cadd(x0, xc), cmul_si(cmul(w, csub(x0, xc)), +1));
       }
-      smem[r * n + bin] = z;
+      smem[pad8(r * n + bin)] = z;
     }
   }
   __syncthreads();
@@ -396,9 +401,9 @@ __global__ void __launch_bounds__(256) k_fft_inverse_reg(
     const int j = j0 + r;
     if (j >= nTheta) continue;
     if (!kReal) {
-      reinterpret_cast<double2*>(out)[((size_t)f * nTheta + j) * nPhi + k] = smem[e];
+      reinterpret_cast<double2*>(out)[((size_t)f * nTheta + j) * nPhi + k] = smem[pad8(e)];
     } else {
-      reinterpret_cast<double2*>(out + ((size_t)f * nTheta + j) * nPhi)[k] = smem[e];
+      reinterpret_cast<double2*>(out + ((size_t)f * nTheta + j) * nPhi)[k] = smem[pad8(e)];
     }
   }
 }
@@ -434,7 +439,7 @@ __global__ void __launch_bounds__(256) k_fft_forward_reg(
         x = reinterpret_cast<const double2*>(in + ((size_t)f * nTheta + j) * nPhi)[k];
       }
     }
-    smem[e] = x;
+    smem[pad8(e)] = x;
   }
   __syncthreads();
   fft_reg<kVPT>(smem, plan, tw, -1);
@@ -444,14 +449,14 @@ __global__ void __launch_bounds__(256) k_fft_forward_reg(
     const int j = j0 + r;
     if (j >= nTheta) continue;
     const double scale = weight[j] * twoPiOverN;
-    const double2* X = smem + r * n;
+    auto X = [&](int b) { return smem[pad8(r * n + b)]; };
     if (!kReal) {
-      S(m, 0, j) = cscale(X[m], scale);
-      S(m, 1, nTheta - 1 - j) = m ? cscale(X[nPhi - m], scale) : make_double2(0.0, 0.0);
+      S(m, 0, j) = cscale(X(m), scale);
+      S(m, 1, nTheta - 1 - j) = m ? cscale(X(nPhi - m), scale) : make_double2(0.0, 0.0);
     } else {
       const int M = L;
-      const double2 z0 = X[m == M ? 0 : m];
-      const double2 zc = cconj(X[m == 0 ? 0 : M - m]);
+      const double2 z0 = X(m == M ? 0 : m);
+      const double2 zc = cconj(X(m == 0 ? 0 : M - m));
       const double2 w = twiddle(tw, m, 1, -1);
       const double2 ev = cscale(cadd(z0, zc), 0.5);
       const double2 od = cscale(cmul_si(csub(z0, zc), -1), 0.5);
@@ -496,7 +501,7 @@ RegConfig reg_config(int n, int tableLen) {
 template <int kVPT>
 gsht_status launch_inverse_reg(const gsht_grid* g, const RegConfig& c, int lmax, int is_real,
                                int count, const double* spec, double* out, cudaStream_t s) {
-  const size_t shmem = sizeof(double2) * kVPT * 256;
+  const size_t shmem = sizeof(double2) * (kVPT * 256 + kVPT * 32);
   dim3 grid((g->n_theta + c.rings - 1) / c.rings, count);
   auto kr = is_real ? k_fft_inverse_reg<true, kVPT> : k_fft_inverse_reg<false, kVPT>;
   GSHT_CUDA(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
@@ -510,7 +515,7 @@ gsht_status launch_inverse_reg(const gsht_grid* g, const RegConfig& c, int lmax,
 template <int kVPT>
 gsht_status launch_forward_reg(const gsht_grid* g, const RegConfig& c, int lmax, int is_real,
                                int count, const double* in, double* spec, cudaStream_t s) {
-  const size_t shmem = sizeof(double2) * kVPT * 256;
+  const size_t shmem = sizeof(double2) * (kVPT * 256 + kVPT * 32);
   dim3 grid((g->n_theta + c.rings - 1) / c.rings, count);
   auto kf = is_real ? k_fft_forward_reg<true, kVPT> : k_fft_forward_reg<false, kVPT>;
   GSHT_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
