@@ -158,6 +158,10 @@ gsht_status legendre_inverse_fp64(const gsht_grid* g, const Table* t, int lmax,
 gsht_status legendre_forward_fp64(const gsht_grid* g, const Table* t, int lmax,
                                   int is_real, int count, const double* spec,
                                   double* coef, cudaStream_t s);
+gsht_status legendre_inverse_fp64_layout(const gsht_grid* g, const Table* t, int lmax,
+                                         int is_real, int count, const double* coef,
+                                         const long long* dOff, const int* dPitch, int kpMax,
+                                         double* operand, double* spec, cudaStream_t s);
 
 // Legendre stage, BF16x3 on tcgen05 (legendre_tc.cu). dir 0 = forward
 // (operand rows over colatitudes), 1 = inverse (rows over degrees).

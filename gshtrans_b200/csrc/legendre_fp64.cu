@@ -364,3 +364,39 @@ gsht_status legendre_forward_fp64(const gsht_grid* g, const Table* t, int lmax,
 }
 
 }  // namespace gsht
+
+namespace gsht {
+
+// The inverse contraction of legendre_inverse_fp64 with an operand layout the
+// caller already placed in device memory (off/pitch as in OperandLayout) and
+// without stage timers: launches only the two kernels, allocates nothing.
+gsht_status legendre_inverse_fp64_layout(const gsht_grid* g, const Table* t, int lmax,
+                                         int is_real, int count, const double* coef,
+                                         const long long* dOff, const int* dPitch, int kpMax,
+                                         double* operand, double* spec, cudaStream_t s) {
+  const int na = t->n < 0 ? -t->n : t->n;
+  const int sgnCount = is_real ? 1 : 2;
+  const int Q = sgnCount * count;
+  double2* op = reinterpret_cast<double2*>(operand);
+  const long cs = coef_size(lmax, t->n, is_real);
+  dim3 pg((kpMax + 127) / 128, lmax + 1, Q);
+  k_prep_inverse_fp64<<<pg, 128, 0, s>>>(lmax, t->n, na, count, sgnCount, is_real, cs,
+                                         reinterpret_cast<const double2*>(coef), dOff, dPitch,
+                                         op);
+  GSHT_LAUNCH_CHECK("k_prep_inverse_fp64");
+  Fp64Args a{};
+  a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count;
+  a.sgnCount = sgnCount; a.Q = Q; a.nTheta = g->n_theta; a.thetaPad = g->theta_pad;
+  a.isReal = is_real; a.rowOff = t->d_row_off; a.opOff = dOff; a.opPitch = dPitch;
+  a.table = t->t64; a.A = op; a.out = reinterpret_cast<double2*>(spec);
+  a.coefSize = cs;
+  dim3 grid((g->n_theta + BN - 1) / BN, (Q + BMC - 1) / BMC, lmax + 1);
+  GSHT_CUDA(cudaFuncSetAttribute(k_legendre_fp64<0>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)fp64_smem_bytes<0>()));
+  k_legendre_fp64<0><<<grid, 256, fp64_smem_bytes<0>(), s>>>(a);
+  GSHT_LAUNCH_CHECK("k_legendre_fp64<inverse>");
+  return GSHT_OK;
+}
+
+}  // namespace gsht

@@ -118,6 +118,24 @@ gsht_status gsht_inverse_batch(const gsht_grid* grid, int lmax, int n,
                                int is_real, int precision, int count,
                                const void* in, void* out, void* stream);
 
+/* Allocation-free FP64 inverse transform of ONE field. No counterpart in the
+ * reference: it serves callers that must not allocate device memory while
+ * they transform (an owning arena or caching allocator, a latency-critical
+ * loop, or a component that must not meet out-of-memory after start-up).
+ * `in` (coefficients) and `out` (grid values) must be device pointers; the
+ * scratch comes from a fixed 16 MiB array in the library's device memory,
+ * which every GPU that loads the library holds until the process exits.
+ * Sizes whose scratch would exceed it are rejected with GSHT_ERR_UNSUPPORTED
+ * and a message giving the bytes needed (a complex field on a grid of its
+ * own degree fits up to lmax ~ 580, a real one up to ~ 800); lmax >= 1.
+ * The first call on a device looks up the array's device address, so make
+ * that first call before any stream capture. All calls share the one array
+ * and it keeps the last call's contents: calls that overlap on the GPU (on
+ * different streams, or different threads) race and corrupt each other;
+ * order them. Results equal gsht_inverse with GSHT_FP64. */
+gsht_status gsht_inverse_noalloc(const gsht_grid* grid, int lmax, int n, int is_real,
+                                 const void* in, void* out, void* stream);
+
 /* Stage timing. No counterpart in the reference (which has no tracing):
  * while enabled, every stage of a transform call is bracketed by CUDA events
  * recorded on the call's stream; gsht_profile_read synchronises those events
