@@ -22,6 +22,7 @@
 #include <cstring>
 
 #include "gsht_internal.cuh"
+#include "tc_common.cuh"
 
 namespace gsht {
 namespace {
@@ -279,6 +280,40 @@ __device__ __forceinline__ void dft_reg<8>(double2 (&c)[8], int sign) {
   }
 }
 
+// 16 = 4 x 4: DFT4 over n1 of x[4 n1 + n2] for each n2, twiddle
+// W16^(n2 k1), DFT4 over n2; output k = k1 + 4 k2.
+template <>
+__device__ __forceinline__ void dft_reg<16>(double2 (&c)[16], int sign) {
+  const double sg = (double)sign;
+  const double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173;  // cos, sin(pi/8)
+  const double h = 0.70710678118654752440;
+  double2 a[4][4];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; n2++) {
+    double2 t[4] = {c[n2], c[4 + n2], c[8 + n2], c[12 + n2]};
+    dft_reg<4>(t, sign);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) a[n2][k1] = t[k1];
+  }
+  // W16^e = (cos(2 pi e / 16), sign sin(2 pi e / 16)) for e = n2 k1.
+  a[1][1] = cmul(a[1][1], make_double2(c1, sg * s1));
+  a[1][2] = cmul(a[1][2], make_double2(h, sg * h));
+  a[1][3] = cmul(a[1][3], make_double2(s1, sg * c1));
+  a[2][1] = cmul(a[2][1], make_double2(h, sg * h));
+  a[2][2] = cmul_si(a[2][2], sign);
+  a[2][3] = cmul(a[2][3], make_double2(-h, sg * h));
+  a[3][1] = cmul(a[3][1], make_double2(s1, sg * c1));
+  a[3][2] = cmul(a[3][2], make_double2(-h, sg * h));
+  a[3][3] = cmul(a[3][3], make_double2(-c1, -sg * s1));
+#pragma unroll
+  for (int k1 = 0; k1 < 4; k1++) {
+    double2 t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+    dft_reg<4>(t, sign);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; k2++) c[k1 + 4 * k2] = t[k2];
+  }
+}
+
 template <>
 __device__ __forceinline__ void dft_reg<3>(double2 (&c)[3], int sign) {
   const double s3 = 0.86602540378443864676;  // sqrt(3)/2
@@ -465,6 +500,615 @@ __global__ void __launch_bounds__(256) k_fft_forward_reg(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Power-of-two lengths with everything compile-time: N points per ring,
+// R = 4096 / N rings per block (16 points per thread), radix-8 stages then one
+// radix-4 or radix-2 stage; indices by shifts and masks. Used for rings of
+// 32..128 points; longer power-of-two rings take the three-pass path below.
+// Ring r's point u
+// sits at r * RS + u + u / 8, which keeps both the in-ring strided accesses
+// and the ring-interleaved gathers conflict-free. Global loads are issued
+// all at once per thread before any shared-memory store.
+// ---------------------------------------------------------------------------
+template <int N>
+struct P2 {
+  static constexpr int kPoints = N > 4096 ? N : 4096;
+  static constexpr int kVPT = kPoints / 256;
+  static constexpr int R = kPoints / N;
+  // Ring stride: in the ring-interleaved gathers a quarter warp touches
+  // min(R, 8) rings x max(1, 8 / R) consecutive points; RS = 8 / R (mod 8) for
+  // R < 8 and RS odd otherwise puts those eight 16-byte accesses in eight
+  // different bank groups.
+  static constexpr int RS = N + N / 8 + (R < 8 ? 8 / R : 1);
+  static constexpr int kSmem = R * RS;  // double2 units
+  __device__ __forceinline__ static int at(int ring, int u) { return ring * RS + u + (u >> 3); }
+};
+
+__host__ __device__ constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x / 2); }
+
+template <int N, int P, int M>
+__device__ __forceinline__ void p2_stage(double2* buf, const double2* __restrict__ tw,
+                                         int twStride, int sign) {
+  constexpr int L = N / (P * M);
+  constexpr int NBR = N / P;  // butterflies per ring
+  constexpr int NB = P2<N>::kVPT / P;  // butterflies per thread
+  double2 v[NB][P];
+#pragma unroll
+  for (int b = 0; b < NB; b++) {
+    const int idx = threadIdx.x + b * 256;
+    const int ring = idx >> ilog2(NBR), bi = idx & (NBR - 1);
+    const int j = bi >> ilog2(M), k = bi & (M - 1);
+#pragma unroll
+    for (int q = 0; q < P; q++) v[b][q] = buf[P2<N>::at(ring, k + j * M + q * L * M)];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < NB; b++) {
+    const int idx = threadIdx.x + b * 256;
+    const int ring = idx >> ilog2(NBR), bi = idx & (NBR - 1);
+    const int j = bi >> ilog2(M), k = bi & (M - 1);
+    dft_reg<P>(v[b], sign);
+    const int t = j * M;
+    if (L > 1 && t) {
+#pragma unroll
+      for (int r = 1; r < P; r++) v[b][r] = cmul(v[b][r], twiddle(tw, t * r, twStride, sign));
+    }
+#pragma unroll
+    for (int r = 0; r < P; r++) buf[P2<N>::at(ring, k + j * P * M + r * M)] = v[b][r];
+  }
+  __syncthreads();
+}
+
+template <int N, int M>
+__device__ __forceinline__ void p2_fft(double2* buf, const double2* __restrict__ tw, int twStride,
+                                       int sign) {
+  constexpr int rem = N / M;
+  constexpr int P = rem % 8 == 0 ? 8 : (rem % 4 == 0 ? 4 : 2);
+  p2_stage<N, P, M>(buf, tw, twStride, sign);
+  if constexpr (M * P < N) p2_fft<N, M * P>(buf, tw, twStride, sign);
+}
+
+template <bool kReal, int N>
+__global__ void __launch_bounds__(256) k_fft_inverse_p2(
+    int L, int lmax, int nTheta, int thetaPad, int count, const double2* __restrict__ spec,
+    const double2* __restrict__ tw, double* __restrict__ out) {
+  extern __shared__ double2 smem[];
+  constexpr int R = P2<N>::R;
+  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int nPhi = 2 * L;
+  const int sgnCount = kReal ? 1 : 2;
+  const int twStride = nPhi / N;
+  auto S = [&](int m, int sgn, int jj) {
+    return spec[((size_t)(m * sgnCount + sgn) * count + f) * thetaPad + jj];
+  };
+  constexpr int kPer = R * N / 256;  // points per thread (16)
+  double2 xv[kPer];
+#pragma unroll
+  for (int it = 0; it < kPer; it++) {
+    const int e = threadIdx.x + it * 256;
+    const int r = e & (R - 1), bin = e >> ilog2(R);
+    const int j = j0 + r;
+    double2 x = make_double2(0.0, 0.0);
+    if (j < nTheta) {
+      if (!kReal) {
+        if (bin <= lmax) x = S(bin, 0, j);
+        if (bin >= nPhi - lmax) x = cadd(x, S(nPhi - bin, 1, nTheta - 1 - j));
+      } else {
+        const int M = L, bc = M - bin;
+        double2 x0 = bin <= lmax ? S(bin, 0, j) : make_double2(0.0, 0.0);
+        double2 x1 = bc <= lmax ? S(bc, 0, j) : make_double2(0.0, 0.0);
+        if (bin == 0) x0.y = 0.0;
+        if (bc == M) x1.y = 0.0;
+        const double2 xc = cconj(x1);
+        const double2 w = twiddle(tw, bin, 1, +1);
+        x = cadd(cadd(x0, xc), cmul_si(cmul(w, csub(x0, xc)), +1));
+      }
+    }
+    xv[it] = x;
+  }
+#pragma unroll
+  for (int it = 0; it < kPer; it++) {
+    const int e = threadIdx.x + it * 256;
+    smem[P2<N>::at(e & (R - 1), e >> ilog2(R))] = xv[it];
+  }
+  __syncthreads();
+  p2_fft<N, 1>(smem, tw, twStride, +1);
+  for (int e = threadIdx.x; e < R * N; e += 256) {
+    const int r = e >> ilog2(N), k = e & (N - 1);
+    const int j = j0 + r;
+    if (j >= nTheta) continue;
+    if (!kReal) {
+      reinterpret_cast<double2*>(out)[((size_t)f * nTheta + j) * nPhi + k] = smem[P2<N>::at(r, k)];
+    } else {
+      reinterpret_cast<double2*>(out + ((size_t)f * nTheta + j) * nPhi)[k] = smem[P2<N>::at(r, k)];
+    }
+  }
+}
+
+template <bool kReal, int N>
+__global__ void __launch_bounds__(256) k_fft_forward_p2(
+    int L, int lmax, int nTheta, int thetaPad, int count, const double* __restrict__ in,
+    const double* __restrict__ weight, const double2* __restrict__ tw,
+    double2* __restrict__ spec) {
+  extern __shared__ double2 smem[];
+  constexpr int R = P2<N>::R;
+  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int nPhi = 2 * L;
+  const int sgnCount = kReal ? 1 : 2;
+  const int twStride = nPhi / N;
+  auto S = [&](int m, int sgn, int jj) -> double2& {
+    return spec[((size_t)(m * sgnCount + sgn) * count + f) * thetaPad + jj];
+  };
+  if (j0 <= nTheta - 1 && nTheta - 1 < j0 + R) {
+    const int padW = thetaPad - nTheta;
+    for (int i = threadIdx.x; i < (lmax + 1) * sgnCount * padW; i += 256) {
+      const int q = i / padW, jj = nTheta + (i - q * padW);
+      S(q / sgnCount, q % sgnCount, jj) = make_double2(0.0, 0.0);
+    }
+  }
+  constexpr int kPer = R * N / 256;
+  double2 xv[kPer];
+#pragma unroll
+  for (int it = 0; it < kPer; it++) {
+    const int e = threadIdx.x + it * 256;
+    const int r = e >> ilog2(N), k = e & (N - 1);
+    const int j = j0 + r;
+    double2 x = make_double2(0.0, 0.0);
+    if (j < nTheta) {
+      x = kReal ? reinterpret_cast<const double2*>(in + ((size_t)f * nTheta + j) * nPhi)[k]
+                : reinterpret_cast<const double2*>(in)[((size_t)f * nTheta + j) * nPhi + k];
+    }
+    xv[it] = x;
+  }
+#pragma unroll
+  for (int it = 0; it < kPer; it++) {
+    const int e = threadIdx.x + it * 256;
+    smem[P2<N>::at(e >> ilog2(N), e & (N - 1))] = xv[it];
+  }
+  __syncthreads();
+  p2_fft<N, 1>(smem, tw, twStride, -1);
+  const double twoPiOverN = 6.283185307179586477 / nPhi;
+  for (int e = threadIdx.x; e < R * (lmax + 1); e += 256) {
+    const int r = e & (R - 1), m = e >> ilog2(R);
+    const int j = j0 + r;
+    if (j >= nTheta) continue;
+    const double scale = weight[j] * twoPiOverN;
+    auto X = [&](int b) { return smem[P2<N>::at(r, b)]; };
+    if (!kReal) {
+      S(m, 0, j) = cscale(X(m), scale);
+      S(m, 1, nTheta - 1 - j) = m ? cscale(X(nPhi - m), scale) : make_double2(0.0, 0.0);
+    } else {
+      const int M = L;
+      const double2 z0 = X(m == M ? 0 : m);
+      const double2 zc = cconj(X(m == 0 ? 0 : M - m));
+      const double2 w = twiddle(tw, m, 1, -1);
+      const double2 ev = cscale(cadd(z0, zc), 0.5);
+      const double2 od = cscale(cmul_si(csub(z0, zc), -1), 0.5);
+      S(m, 0, j) = cscale(cadd(ev, cmul(w, od)), scale);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Three-pass power-of-two path (rings of 256..4096 points). A block holds
+// 4096 points (R = 4096 / N rings), 16 per thread, and runs the Stockham
+// stages 16 x ... with radix-16/8/4 register butterflies: the first stage
+// works directly on the values loaded from global memory, the last one writes
+// its results straight to global memory, so shared memory is crossed only
+// between stages (two round trips for N = 2048 instead of five). Twiddles of
+// a butterfly are built from at most three table loads (w^t, w^4t, w^8t) by
+// complex products, each power at most four products deep. Ring r's point u
+// sits at r * RS + u + u / 16: with RS = N + N/16 + 8/R every stage's loads
+// and stores, in both the ring-major and the ring-interleaved thread maps,
+// are free of bank conflicts (checked by enumeration of the quarter-warp
+// access sets).
+// ---------------------------------------------------------------------------
+template <int N>
+struct P3 {
+  static constexpr int kPoints = N > 4096 ? N : 4096;
+  static constexpr int R = kPoints / N;
+  static constexpr int RS = N + N / 16 + (R > 8 ? 1 : (R > 1 ? 8 / R : 0));
+  static constexpr int kSmem = R * RS;  // double2 units
+  __device__ __forceinline__ static int at(int ring, int u) { return ring * RS + u + (u >> 4); }
+};
+
+// Radix of the stage that follows M points of already combined length.
+template <int N, int M>
+struct P3Radix {
+  static constexpr int rem = N / M;
+  static constexpr int P = M == 1 ? 16
+                           : ((rem % 16 == 0 && rem / 16 != 2) ? 16
+                              : (rem % 8 == 0 ? 8 : (rem % 4 == 0 ? 4 : 2)));
+};
+
+// v[r] *= w^(t r), w = exp(sign 2 pi i / N) from the table at stride twStride.
+template <int P>
+__device__ __forceinline__ void p3_twiddle(double2 (&v)[P], const double2* __restrict__ tw, int t,
+                                           int twStride, int sign) {
+  if (t == 0) return;
+  const double2 a = twiddle(tw, t, twStride, sign);
+  v[1] = cmul(v[1], a);
+  if constexpr (P > 2) {
+    const double2 a2 = cmul(a, a), a3 = cmul(a2, a);
+    v[2] = cmul(v[2], a2);
+    v[3] = cmul(v[3], a3);
+    if constexpr (P > 4) {
+      const double2 b = twiddle(tw, 4 * t, twStride, sign);
+      const double2 b1 = cmul(b, a), b2 = cmul(b, a2), b3 = cmul(b, a3);
+      v[4] = cmul(v[4], b);
+      v[5] = cmul(v[5], b1);
+      v[6] = cmul(v[6], b2);
+      v[7] = cmul(v[7], b3);
+      if constexpr (P > 8) {
+        const double2 c = twiddle(tw, 8 * t, twStride, sign);
+        v[8] = cmul(v[8], c);
+        v[9] = cmul(v[9], cmul(c, a));
+        v[10] = cmul(v[10], cmul(c, a2));
+        v[11] = cmul(v[11], cmul(c, a3));
+        v[12] = cmul(v[12], cmul(c, b));
+        v[13] = cmul(v[13], cmul(c, b1));
+        v[14] = cmul(v[14], cmul(c, b2));
+        v[15] = cmul(v[15], cmul(c, b3));
+      }
+    }
+  }
+}
+
+// Middle stages (every stage after the first and before the last), in place.
+template <int N, int M>
+__device__ __forceinline__ void p3_middle(double2* buf, const double2* __restrict__ tw,
+                                          int twStride, int sign) {
+  constexpr int P = P3Radix<N, M>::P;
+  if constexpr (M * P < N) {
+    constexpr int L = N / (P * M);
+    constexpr int NBR = N / P;
+    constexpr int NB = 16 / P;
+    double2 v[NB][P];
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      const int g = threadIdx.x + b * 256;
+      const int ring = g >> ilog2(NBR), bi = g & (NBR - 1);
+      const int j = bi >> ilog2(M), k = bi & (M - 1);
+#pragma unroll
+      for (int q = 0; q < P; q++) v[b][q] = buf[P3<N>::at(ring, k + j * M + q * L * M)];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      const int g = threadIdx.x + b * 256;
+      const int ring = g >> ilog2(NBR), bi = g & (NBR - 1);
+      const int j = bi >> ilog2(M), k = bi & (M - 1);
+      dft_reg<P>(v[b], sign);
+      p3_twiddle<P>(v[b], tw, j * M, twStride, sign);
+#pragma unroll
+      for (int r = 0; r < P; r++) buf[P3<N>::at(ring, k + j * P * M + r * M)] = v[b][r];
+    }
+    __syncthreads();
+    p3_middle<N, M * P>(buf, tw, twStride, sign);
+  }
+}
+
+// Combined length before the last stage.
+template <int N, int M = 1>
+__host__ __device__ constexpr int p3_last_m() {
+  constexpr int P = P3Radix<N, M>::P;
+  if constexpr (M * P >= N) return M;
+  else return p3_last_m<N, M * P>();
+}
+
+// Spectral rows per TMA box of the inverse's staged loads.
+constexpr int kSpecBox = 64;
+
+// kTma: the block's spectral rows (orders 0..lmax for each sign, R
+// colatitudes each; the -m rows at the mirrored colatitudes) are brought into
+// shared memory by 4-D TMA boxes of kSpecBox rows before the first stage, so
+// the strided 16R-byte row segments cost no load instructions or registers;
+// the first stage reads them from shared memory. Without kTma the first
+// stage loads them from global memory directly.
+template <bool kReal, int N, bool kTma>
+__global__ void __launch_bounds__(256, 2) k_fft_inverse_p3(
+    const __grid_constant__ CUtensorMap specMap, int L, int lmax, int nTheta, int thetaPad,
+    int count, const double2* __restrict__ spec, const double2* __restrict__ tw,
+    double* __restrict__ out, int* err, int smemElems) {
+  // TMA destinations want 128-byte alignment: round the dynamic base up (the
+  // launch adds 128 bytes of slack plus the barrier word after the buffer).
+  extern __shared__ unsigned char p3_raw[];
+  double2* smem = reinterpret_cast<double2*>(
+      (reinterpret_cast<uintptr_t>(p3_raw) + 127) & ~uintptr_t(127));
+  uint64_t& bar = *reinterpret_cast<uint64_t*>(smem + smemElems);
+  constexpr int R = P3<N>::R;
+  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int nPhi = 2 * L;
+  const int sgnCount = kReal ? 1 : 2;
+  const int twStride = nPhi / N;
+  const int nbox = (lmax + 1 + kSpecBox - 1) / kSpecBox;
+  const int M1 = nbox * kSpecBox;  // staged rows per sign
+  auto S = [&](int m, int sgn, int jj) {
+    return spec[((size_t)(m * sgnCount + sgn) * count + f) * thetaPad + jj];
+  };
+  if constexpr (kTma) {
+    if (threadIdx.x == 0) {
+      tc::mbar_init(&bar, 1);
+      tc::fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc::prefetch_tmap(&specMap);
+      tc::mbar_arrive_expect_tx(&bar, (uint32_t)(sgnCount * M1 * R * sizeof(double2)));
+      for (int sg = 0; sg < sgnCount; sg++) {
+        // Colatitudes j0.. (sign 0) or their mirror images nTheta-j0-R.. (sign 1).
+        const int x = 2 * (sg == 0 ? j0 : nTheta - j0 - R);
+        for (int b = 0; b < nbox; b++)
+          tc::tma_load_4d(smem + (size_t)(sg * M1 + b * kSpecBox) * R, &specMap, &bar, x, f, sg,
+                          b * kSpecBox);
+      }
+    }
+    tc::mbar_wait(&bar, 0, err, 21);
+  }
+  // First stage (radix 16, M = 1), rings interleaved across lanes so that
+  // lanes 0..R-1 read R consecutive colatitudes of one spectral row.
+  {
+    const int r = threadIdx.x & (R - 1), jj = threadIdx.x >> ilog2(R);
+    const int th = j0 + r;
+    double2 v[16];
+    // Row m of sign sg (staged): colatitude j0 + r is element r, its mirror
+    // nTheta-1-(j0+r) element R-1-r.
+    auto T = [&](int m, int sg) {
+      return sg == 0 ? smem[(size_t)m * R + r] : smem[(size_t)(M1 + m) * R + (R - 1 - r)];
+    };
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int bin = jj + q * (N / 16);
+      double2 x = make_double2(0.0, 0.0);
+      if (kTma || th < nTheta) {
+        if (!kReal) {
+          if (bin <= lmax) x = kTma ? T(bin, 0) : S(bin, 0, th);
+          if (bin >= nPhi - lmax)
+            x = cadd(x, kTma ? T(nPhi - bin, 1) : S(nPhi - bin, 1, nTheta - 1 - th));
+        } else {
+          const int M = L, bc = M - bin;
+          double2 x0 = bin <= lmax ? (kTma ? T(bin, 0) : S(bin, 0, th)) : make_double2(0.0, 0.0);
+          double2 x1 = bc <= lmax ? (kTma ? T(bc, 0) : S(bc, 0, th)) : make_double2(0.0, 0.0);
+          if (bin == 0) x0.y = 0.0;
+          if (bc == M) x1.y = 0.0;
+          const double2 xc = cconj(x1);
+          const double2 w = twiddle(tw, bin, 1, +1);
+          x = cadd(cadd(x0, xc), cmul_si(cmul(w, csub(x0, xc)), +1));
+        }
+      }
+      v[q] = x;
+    }
+    if constexpr (kTma) __syncthreads();  // the staged rows share the buffer
+    dft_reg<16>(v, +1);
+    p3_twiddle<16>(v, tw, jj, twStride, +1);
+#pragma unroll
+    for (int q = 0; q < 16; q++) smem[P3<N>::at(r, jj * 16 + q)] = v[q];
+  }
+  __syncthreads();
+  p3_middle<N, 16>(smem, tw, twStride, +1);
+  // Last stage (L = 1, no twiddles), ring-major so that lanes write
+  // consecutive longitudes.
+  constexpr int M = p3_last_m<N>();
+  constexpr int P = N / M;
+  constexpr int NB = 16 / P;
+#pragma unroll
+  for (int b = 0; b < NB; b++) {
+    const int g = threadIdx.x + b * 256;
+    const int ring = g >> ilog2(M), k = g & (M - 1);
+    double2 v[P];
+#pragma unroll
+    for (int q = 0; q < P; q++) v[q] = smem[P3<N>::at(ring, k + q * M)];
+    dft_reg<P>(v, +1);
+    const int th = j0 + ring;
+    if (th < nTheta) {
+      double2* row = kReal ? reinterpret_cast<double2*>(out + ((size_t)f * nTheta + th) * nPhi)
+                           : reinterpret_cast<double2*>(out) + ((size_t)f * nTheta + th) * nPhi;
+#pragma unroll
+      for (int r = 0; r < P; r++) row[k + r * M] = v[r];
+    }
+  }
+}
+
+template <bool kReal, int N>
+__global__ void __launch_bounds__(256, 2) k_fft_forward_p3(
+    int L, int lmax, int nTheta, int thetaPad, int count, const double* __restrict__ in,
+    const double* __restrict__ weight, const double2* __restrict__ tw,
+    double2* __restrict__ spec) {
+  extern __shared__ double2 smem[];
+  constexpr int R = P3<N>::R;
+  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int nPhi = 2 * L;
+  const int sgnCount = kReal ? 1 : 2;
+  const int twStride = nPhi / N;
+  auto S = [&](int m, int sgn, int jj) -> double2& {
+    return spec[((size_t)(m * sgnCount + sgn) * count + f) * thetaPad + jj];
+  };
+  if (j0 <= nTheta - 1 && nTheta - 1 < j0 + R) {
+    const int padW = thetaPad - nTheta;
+    for (int i = threadIdx.x; i < (lmax + 1) * sgnCount * padW; i += 256) {
+      const int q = i / padW, jj = nTheta + (i - q * padW);
+      S(q / sgnCount, q % sgnCount, jj) = make_double2(0.0, 0.0);
+    }
+  }
+  // First stage, ring-major: lanes read consecutive longitudes.
+  {
+    constexpr int NBR = N / 16;
+    const int ring = threadIdx.x >> ilog2(NBR), jj = threadIdx.x & (NBR - 1);
+    const int th = j0 + ring;
+    double2 v[16];
+    const double2* row = kReal ? reinterpret_cast<const double2*>(in + ((size_t)f * nTheta + th) * nPhi)
+                               : reinterpret_cast<const double2*>(in) + ((size_t)f * nTheta + th) * nPhi;
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q] = th < nTheta ? row[jj + q * NBR] : make_double2(0.0, 0.0);
+    dft_reg<16>(v, -1);
+    p3_twiddle<16>(v, tw, jj, twStride, -1);
+#pragma unroll
+    for (int q = 0; q < 16; q++) smem[P3<N>::at(ring, jj * 16 + q)] = v[q];
+  }
+  __syncthreads();
+  p3_middle<N, 16>(smem, tw, twStride, -1);
+  constexpr int M = p3_last_m<N>();
+  constexpr int P = N / M;
+  constexpr int NB = 16 / P;
+  const double twoPiOverN = 6.283185307179586477 / nPhi;
+  if constexpr (!kReal) {
+    // Last stage with rings interleaved across lanes: lanes 0..R-1 write R
+    // consecutive colatitudes of one spectral row.
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      const int g = threadIdx.x + b * 256;
+      const int ring = g & (R - 1), k = g >> ilog2(R);
+      double2 v[P];
+#pragma unroll
+      for (int q = 0; q < P; q++) v[q] = smem[P3<N>::at(ring, k + q * M)];
+      dft_reg<P>(v, -1);
+      const int th = j0 + ring;
+      if (th < nTheta) {
+        const double scale = weight[th] * twoPiOverN;
+#pragma unroll
+        for (int r = 0; r < P; r++) {
+          const int bin = k + r * M;
+          const double2 x = cscale(v[r], scale);
+          if (bin <= lmax) S(bin, 0, th) = x;
+          if (bin == 0) S(0, 1, nTheta - 1 - th) = make_double2(0.0, 0.0);
+          else if (bin >= nPhi - lmax) S(nPhi - bin, 1, nTheta - 1 - th) = x;
+        }
+      }
+    }
+  } else {
+    double2 v[NB][P];
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      const int g = threadIdx.x + b * 256;
+      const int ring = g >> ilog2(M), k = g & (M - 1);
+#pragma unroll
+      for (int q = 0; q < P; q++) v[b][q] = smem[P3<N>::at(ring, k + q * M)];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      const int g = threadIdx.x + b * 256;
+      const int ring = g >> ilog2(M), k = g & (M - 1);
+      dft_reg<P>(v[b], -1);
+#pragma unroll
+      for (int r = 0; r < P; r++) smem[P3<N>::at(ring, k + r * M)] = v[b][r];
+    }
+    __syncthreads();
+    // Real field: unpack the half-length transform, X(m) from z(m) and
+    // conj z(M - m), M = nPhi / 2.
+    for (int e = threadIdx.x; e < R * (lmax + 1); e += 256) {
+      const int r = e & (R - 1), m = e >> ilog2(R);
+      const int th = j0 + r;
+      if (th >= nTheta) continue;
+      const double scale = weight[th] * twoPiOverN;
+      const int Mh = L;
+      const double2 z0 = smem[P3<N>::at(r, m == Mh ? 0 : m)];
+      const double2 zc = cconj(smem[P3<N>::at(r, m == 0 ? 0 : Mh - m)]);
+      const double2 w = twiddle(tw, m, 1, -1);
+      const double2 ev = cscale(cadd(z0, zc), 0.5);
+      const double2 od = cscale(cmul_si(csub(z0, zc), -1), 0.5);
+      S(m, 0, th) = cscale(cadd(ev, cmul(w, od)), scale);
+    }
+  }
+}
+
+// Tensor map of the spectral buffer as FP64 [m][sign][field][2 * thetaPad]
+// with a 2R x 1 x 1 x kSpecBox box (R colatitudes of kSpecBox rows).
+bool spec_map(CUtensorMap* map, double* spec, int thetaPad, int count, int sgnCount, int lmax,
+              int R) {
+  tc::EncodeTiledFn fn = tc::encode_fn();
+  if (!fn) return false;
+  const cuuint64_t tp2 = 2 * (cuuint64_t)thetaPad;
+  cuuint64_t dims[4] = {tp2, (cuuint64_t)count, (cuuint64_t)sgnCount, (cuuint64_t)lmax + 1};
+  cuuint64_t strides[3] = {tp2 * 8, tp2 * 8 * count, tp2 * 8 * count * sgnCount};
+  cuuint32_t box[4] = {(cuuint32_t)(2 * R), 1, 1, kSpecBox};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, spec, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int N>
+gsht_status launch_p3(const gsht_grid* g, int dir, int lmax, int is_real, int count,
+                      const double* src, double* dst, cudaStream_t s) {
+  size_t shmem = sizeof(double2) * P3<N>::kSmem;
+  constexpr int R = P3<N>::R;
+  dim3 grid((g->n_theta + R - 1) / R, count);
+  const double2* tw = reinterpret_cast<const double2*>(g->d_twiddle);
+  if (dir == 1) {
+    // Staged spectral rows: sign x ceil((lmax+1)/kSpecBox) boxes x R colatitudes.
+    const int sgnCount = is_real ? 1 : 2;
+    const size_t staged =
+        sizeof(double2) * sgnCount * (size_t)((lmax + kSpecBox) / kSpecBox) * kSpecBox * R;
+    CUtensorMap map{};
+    const bool tma = staged <= 110 * 1024 &&
+                     spec_map(&map, const_cast<double*>(src), g->theta_pad, count, sgnCount, lmax, R);
+    if (tma) shmem = shmem > staged ? shmem : staged;
+    const int smemElems = (int)(shmem / sizeof(double2));
+    shmem += 128 + 16;
+    if (tma) {
+      auto k = is_real ? k_fft_inverse_p3<true, N, true> : k_fft_inverse_p3<false, N, true>;
+      GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
+      k<<<grid, 256, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count,
+                                 reinterpret_cast<const double2*>(src), tw, dst, g->d_err,
+                                 smemElems);
+    } else {
+      auto k = is_real ? k_fft_inverse_p3<true, N, false> : k_fft_inverse_p3<false, N, false>;
+      GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
+      k<<<grid, 256, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count,
+                                 reinterpret_cast<const double2*>(src), tw, dst, g->d_err,
+                                 smemElems);
+    }
+    GSHT_LAUNCH_CHECK("k_fft_inverse_p3");
+  } else {
+    auto k = is_real ? k_fft_forward_p3<true, N> : k_fft_forward_p3<false, N>;
+    GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
+    k<<<grid, 256, shmem, s>>>(g->L, lmax, g->n_theta, g->theta_pad, count, src, g->d_weight,
+                               tw, reinterpret_cast<double2*>(dst));
+    GSHT_LAUNCH_CHECK("k_fft_forward_p3");
+  }
+  return GSHT_OK;
+}
+
+template <int N>
+gsht_status launch_p2(const gsht_grid* g, int dir, int lmax, int is_real, int count,
+                      const double* src, double* dst, cudaStream_t s) {
+  const size_t shmem = sizeof(double2) * P2<N>::kSmem;
+  dim3 grid((g->n_theta + P2<N>::R - 1) / P2<N>::R, count);
+  const double2* tw = reinterpret_cast<const double2*>(g->d_twiddle);
+  if (dir == 1) {
+    auto k = is_real ? k_fft_inverse_p2<true, N> : k_fft_inverse_p2<false, N>;
+    GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
+    k<<<grid, 256, shmem, s>>>(g->L, lmax, g->n_theta, g->theta_pad, count,
+                               reinterpret_cast<const double2*>(src), tw, dst);
+    GSHT_LAUNCH_CHECK("k_fft_inverse_p2");
+  } else {
+    auto k = is_real ? k_fft_forward_p2<true, N> : k_fft_forward_p2<false, N>;
+    GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
+    k<<<grid, 256, shmem, s>>>(g->L, lmax, g->n_theta, g->theta_pad, count, src, g->d_weight,
+                               tw, reinterpret_cast<double2*>(dst));
+    GSHT_LAUNCH_CHECK("k_fft_forward_p2");
+  }
+  return GSHT_OK;
+}
+
+// Power-of-two paths if n is one of the compiled lengths; *used = false otherwise.
+gsht_status fft_p2(const gsht_grid* g, int n, int dir, int lmax, int is_real, int count,
+                   const double* src, double* dst, cudaStream_t s, bool* used) {
+  *used = true;
+  switch (n) {
+    case 32: return launch_p2<32>(g, dir, lmax, is_real, count, src, dst, s);
+    case 64: return launch_p2<64>(g, dir, lmax, is_real, count, src, dst, s);
+    case 128: return launch_p2<128>(g, dir, lmax, is_real, count, src, dst, s);
+    case 256: return launch_p3<256>(g, dir, lmax, is_real, count, src, dst, s);
+    case 512: return launch_p3<512>(g, dir, lmax, is_real, count, src, dst, s);
+    case 1024: return launch_p3<1024>(g, dir, lmax, is_real, count, src, dst, s);
+    case 2048: return launch_p3<2048>(g, dir, lmax, is_real, count, src, dst, s);
+    case 4096: return launch_p3<4096>(g, dir, lmax, is_real, count, src, dst, s);
+    default: *used = false; return GSHT_OK;
+  }
+}
+
 // Register-path configuration for a transform length: points per thread
 // kVPT in {16, 24, 32} and rings per block R = kVPT * 256 / n, or 0 if the
 // length needs the generic path.
@@ -531,6 +1175,9 @@ gsht_status launch_forward_reg(const gsht_grid* g, const RegConfig& c, int lmax,
 gsht_status fft_inverse(const gsht_grid* g, int lmax, int is_real, int count,
                         const double* spec, double* out, cudaStream_t s) {
   const int N = g->n_phi;
+  bool used = false;
+  gsht_status st = fft_p2(g, is_real ? N / 2 : N, 1, lmax, is_real, count, spec, out, s, &used);
+  if (used) return st;
   const RegConfig rc = reg_config(is_real ? N / 2 : N, N);
   if (rc.vpt == 16) return launch_inverse_reg<16>(g, rc, lmax, is_real, count, spec, out, s);
   if (rc.vpt == 24) return launch_inverse_reg<24>(g, rc, lmax, is_real, count, spec, out, s);
@@ -560,6 +1207,9 @@ gsht_status fft_inverse(const gsht_grid* g, int lmax, int is_real, int count,
 gsht_status fft_forward(const gsht_grid* g, int lmax, int is_real, int count,
                         const double* in, double* spec, cudaStream_t s) {
   const int N = g->n_phi;
+  bool used = false;
+  gsht_status st = fft_p2(g, is_real ? N / 2 : N, 0, lmax, is_real, count, in, spec, s, &used);
+  if (used) return st;
   const RegConfig rc = reg_config(is_real ? N / 2 : N, N);
   if (rc.vpt == 16) return launch_forward_reg<16>(g, rc, lmax, is_real, count, in, spec, s);
   if (rc.vpt == 24) return launch_forward_reg<24>(g, rc, lmax, is_real, count, in, spec, s);

@@ -99,6 +99,14 @@ struct OperandLayout {
   int pitch_max = 0;
 };
 
+// Work list of a persistent tensor-core launch: tiles (m, mtile, ntile, nk)
+// in order of decreasing m-block work, cached on the grid per key.
+struct TileList {
+  int dir = 0, lmax = 0, na = 0, rows = 0, ntile = 0, kstep = 0;
+  int4* d_tiles = nullptr;
+  int count = 0;
+};
+
 }  // namespace gsht
 
 // The opaque handle of the C ABI.
@@ -127,6 +135,7 @@ struct gsht_grid {
   cudaEvent_t ws_done = nullptr;  // recorded after the last call's kernels
   // Cached operand layouts (guarded by mu).
   mutable std::vector<gsht::OperandLayout*> layouts;
+  mutable std::vector<gsht::TileList*> tile_lists;
 
   const gsht::Table* table(int n) const {
     if (n < min_n || n > nmax) return nullptr;
@@ -141,6 +150,9 @@ gsht_status build_nodes(gsht_grid* g);
 gsht_status build_table(gsht_grid* g, Table* t, cudaStream_t s);
 gsht_status build_forms(gsht_grid* g, Table* t, cudaStream_t s);
 void free_table(Table* t);
+gsht_status wigner_compute(int lmax, int mmax, int nmax, int mrange, int nrange, int norm,
+                           int row_major, const double* theta, int ntheta, double* out,
+                           long* count);
 
 // FFT stage (fft.cu). spec: spectral buffer [m][sgn][f][j] complex.
 gsht_status fft_inverse(const gsht_grid* g, int lmax, int is_real, int count,
@@ -186,6 +198,11 @@ gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, in
 const OperandLayout* operand_layout(const gsht_grid* g, int lmax, int na,
                                     int rows, int pad, gsht_status* st);
 void free_layouts(gsht_grid* g);
+// Cached tile list for a persistent tensor-core launch (legendre_tc.cu).
+// dir 0 = inverse (M = colatitudes), 1 = forward (M = degrees); rows = field
+// rows R; ntile = field rows per tile; the caller holds g->mu.
+const TileList* tile_list(const gsht_grid* g, int dir, int lmax, int na, int rows,
+                          int ntile, int kstep, gsht_status* st);
 
 // Spectral buffer element count: (lmax+1) x sgn x count x thetaPad complex.
 inline size_t spec_elems(const gsht_grid* g, int lmax, int is_real, int count) {

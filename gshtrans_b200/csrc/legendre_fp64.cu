@@ -290,6 +290,11 @@ void free_layouts(gsht_grid* g) {
     delete o;
   }
   g->layouts.clear();
+  for (auto* t : g->tile_lists) {
+    cudaFree(t->d_tiles);
+    delete t;
+  }
+  g->tile_lists.clear();
 }
 
 size_t fp64_operand_elems(const gsht_grid* g, const Table* t, int lmax,

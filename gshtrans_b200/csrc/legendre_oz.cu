@@ -36,6 +36,7 @@ constexpr int kStageBytes = kS * (kTileA + kTileB);  // 84 KB
 constexpr int kStages = 2;
 constexpr int kTmemCols = 512;
 constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + 1024 + 256;
+static_assert(kNDiag * kN <= kTmemCols, "diagonal accumulators exceed the TMEM allocation");
 
 struct OzArgs {
   int L, lmax, n, na, count, Q, R, nTheta, thetaPad, isReal;
@@ -47,38 +48,40 @@ struct OzArgs {
   int* err;
 };
 
+constexpr int kEpiWarps = 8;  // two warps per TMEM lane quarter
+constexpr int kThreads = 32 * (2 + kEpiWarps);
+
+// Persistent kernel over the tile list (see legendre_tc.cu for the protocol):
+// the epilogue sums the 7 diagonal accumulators of its 32 columns in FP64,
+// releases TMEM, then writes.
 template <int kDir>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(kThreads, 1)
     k_legendre_oz(const __grid_constant__ CUtensorMap mapA,
-                  const __grid_constant__ CUtensorMap mapB, OzArgs p) {
+                  const __grid_constant__ CUtensorMap mapB, OzArgs p,
+                  const int4* __restrict__ tiles, int numTiles) {
   extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
+  constexpr int kCols = kN / 2;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* accBar = empty + kStages;
-  uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(accBar + 1);
+  uint64_t* accFull = empty + kStages;
+  uint64_t* accEmpty = accFull + 1;
+  uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(accEmpty + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int mtile = blockIdx.x, ntile = blockIdx.y, m = blockIdx.z;
-  const int l0 = m > p.na ? m : p.na;
-  const int Keff = p.lmax - l0 + 1;
-  const int rowsM = kDir == 0 ? p.nTheta : Keff;
-  if (mtile * kBM >= rowsM) return;
   __shared__ int skip;
   if (threadIdx.x == 0) skip = *reinterpret_cast<volatile int*>(p.err);
   __syncthreads();
-  if (skip) return;
-  const int nk = kDir == 0 ? (Keff + kBK - 1) / kBK : (p.thetaPad + kBK - 1) / kBK;
-  const long long tRow = p.rowOff[m];
-  const int bRow = m * p.R + ntile * kN;
+  if (skip || blockIdx.x >= numTiles) return;
 
   if (warp == 0 && lane == 0) {
     for (int s = 0; s < kStages; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accBar, 1);
+    mbar_init(accFull, 1);
+    mbar_init(accEmpty, kEpiWarps);
     fence_barrier_init();
     prefetch_tmap(&mapA);
     prefetch_tmap(&mapB);
@@ -91,102 +94,154 @@ __global__ void __launch_bounds__(192, 1)
 
   if (warp == 0) {
     if (lane == 0) {
-      for (int kc = 0; kc < nk; kc++) {
-        const int s = kc % kStages;
-        if (kc >= kStages && !mbar_wait(&empty[s], ((kc / kStages) - 1) & 1, p.err, 11)) break;
-        unsigned char* st = smem + s * kStageBytes;
-        mbar_arrive_expect_tx(&full[s], kStageBytes);
-        for (int a = 0; a < kS; a++) {
-          if (kDir == 0) {
-            // MN-major: 128 colatitudes (one 128 B row) x 64 degree rows.
-            tma_load_3d(st + a * kTileA, &mapA, &full[s], mtile * kBM, (int)(tRow + kc * kBK), a);
-          } else {
-            tma_load_3d(st + a * kTileA, &mapA, &full[s], kc * kBK, (int)(tRow + mtile * kBM), a);
+      int it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < numTiles && ok; t += gridDim.x) {
+        const int4 tl = tiles[t];
+        const long long tRow = p.rowOff[tl.x];
+        const int bRow = tl.x * p.R + tl.z * kN;
+        for (int kc = 0; kc < tl.w; kc++, it++) {
+          const int s = it % kStages;
+          if (it >= kStages && !mbar_wait(&empty[s], ((it / kStages) - 1) & 1, p.err, 11)) {
+            ok = false;
+            break;
           }
+          unsigned char* st = smem + s * kStageBytes;
+          mbar_arrive_expect_tx(&full[s], kStageBytes);
+          for (int a = 0; a < kS; a++) {
+            if (kDir == 0) {
+              // MN-major: 128 colatitudes (one 128 B row) x 64 degree rows.
+              tma_load_3d(st + a * kTileA, &mapA, &full[s], tl.y * kBM, (int)(tRow + kc * kBK), a);
+            } else {
+              tma_load_3d(st + a * kTileA, &mapA, &full[s], kc * kBK, (int)(tRow + tl.y * kBM), a);
+            }
+          }
+          for (int b = 0; b < kS; b++)
+            tma_load_3d(st + kS * kTileA + b * kTileB, &mapB, &full[s], kc * kBK, bRow, b);
         }
-        for (int b = 0; b < kS; b++)
-          tma_load_3d(st + kS * kTileA + b * kTileB, &mapB, &full[s], kc * kBK, bRow, b);
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t id = idesc(2, 1, kDir == 0 ? 1 : 0, 0, kN, kBM);
-      for (int kc = 0; kc < nk; kc++) {
-        const int s = kc % kStages;
-        if (!mbar_wait(&full[s], (kc / kStages) & 1, p.err, 12)) break;
+      int it = 0, tc = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < numTiles && ok; t += gridDim.x, tc++) {
+        const int nk = tiles[t].w;
+        if (tc > 0 && !mbar_wait(accEmpty, (tc - 1) & 1, p.err, 14)) break;
         tc_fence_after();
-        const uint32_t st = smem_u32(smem + s * kStageBytes);
+        for (int kc = 0; kc < nk; kc++, it++) {
+          const int s = it % kStages;
+          if (!mbar_wait(&full[s], (it / kStages) & 1, p.err, 12)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t st = smem_u32(smem + s * kStageBytes);
 #pragma unroll
-        for (int i = 0; i < kS; i++) {
+          for (int i = 0; i < kS; i++) {
 #pragma unroll
-          for (int j = 0; i + j < kS; j++) {
-            const uint32_t aBase = st + i * kTileA;
-            const uint32_t bBase = st + kS * kTileA + j * kTileB;
-            const uint32_t d = tmem + (uint32_t)((i + j) * kN);
+            for (int j = 0; i + j < kS; j++) {
+              const uint32_t aBase = st + i * kTileA;
+              const uint32_t bBase = st + kS * kTileA + j * kTileB;
+              const uint32_t d = tmem + (uint32_t)((i + j) * kN);
 #pragma unroll
-            for (int k32 = 0; k32 < kBK / 32; k32++) {
-              const uint64_t ad = kDir == 0 ? sdesc_sw128(aBase + k32 * 4096, 8192, 1024)
-                                            : sdesc_sw64(aBase + k32 * 32, 16, 512);
-              const uint64_t bd = sdesc_sw64(bBase + k32 * 32, 16, 512);
-              mma_i8(d, ad, bd, id, (kc | i | k32) != 0);
+              for (int k32 = 0; k32 < kBK / 32; k32++) {
+                const uint64_t ad = kDir == 0 ? sdesc_sw128(aBase + k32 * 4096, 8192, 1024)
+                                              : sdesc_sw64(aBase + k32 * 32, 16, 512);
+                const uint64_t bd = sdesc_sw64(bBase + k32 * 32, 16, 512);
+                mma_i8(d, ad, bd, id, (kc | i | k32) != 0);
+              }
             }
           }
+          mma_commit(&empty[s]);
         }
-        mma_commit(&empty[s]);
+        mma_commit(accFull);
       }
-      mma_commit(accBar);
     }
   } else {
     const int quarter = warp & 3;
+    const int half = (warp - 2) >> 2;
     const int row = quarter * 32 + lane;
-    const bool ready = mbar_wait(accBar, 0, p.err, 13);
-    tc_fence_after();
-    if (ready) {
-      const int tileRow = mtile * kBM + row;
-      const bool live = tileRow < rowsM;
-      const int eA = (kDir == 0 && live) ? p.tabExp[(size_t)m * p.thetaPad + tileRow] : 0;
-#pragma unroll 1
-      for (int c = 0; c < kN / 16; c++) {
-        double acc[16];
+    int tc = 0;
+    for (int t = blockIdx.x; t < numTiles; t += gridDim.x, tc++) {
+      const int4 tl = tiles[t];
+      const int m = tl.x;
+      if (!mbar_wait(accFull, tc & 1, p.err, 13)) break;
+      tc_fence_after();
+      double acc[kCols];
 #pragma unroll
-        for (int i = 0; i < 16; i++) acc[i] = 0.0;
-#pragma unroll 1
-        for (int d = 0; d < kNDiag; d++) {
-          uint32_t v[16];
-          tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + d * kN + c * 16, v);
-          tmem_wait_ld();
-          const double w = ldexp(1.0, -7 * (d + 2));
+      for (int i = 0; i < kCols; i++) acc[i] = 0.0;
+      static_assert(kCols == 32, "two 16-column loads per diagonal");
 #pragma unroll
-          for (int i = 0; i < 16; i++) acc[i] = fma((double)(int)v[i], w, acc[i]);
+      for (int d = 0; d < kNDiag; d++) {
+        const double w = ldexp(1.0, -7 * (d + 2));
+        const uint32_t ta = tmem + ((uint32_t)(quarter * 32) << 16) + d * kN + half * kCols;
+        uint32_t v0[16], v1[16];
+        tmem_ld16(ta, v0);
+        tmem_ld16(ta + 16, v1);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          acc[i] = fma((double)(int)v0[i], w, acc[i]);
+          acc[16 + i] = fma((double)(int)v1[i], w, acc[16 + i]);
         }
-        if (!live) continue;
-        const int r0 = ntile * kN + c * 16;
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(accEmpty);
+      const int l0 = m > p.na ? m : p.na;
+      const int keff = p.lmax - l0 + 1;
+      const int tileRow = tl.y * kBM + row;
+      const int rowsM = kDir == 0 ? p.nTheta : keff;
+      if (tileRow >= rowsM) continue;
+      const int eA = kDir == 0 ? p.tabExp[(size_t)m * p.thetaPad + tileRow] : 0;
+      const int q0 = (tl.z * kN + half * kCols) / 2;
+      if (kDir == 0) {
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-          const int q = r0 / 2 + i;
+        for (int i = 0; i < kCols / 2; i++) {
+          const int q = q0 + i;
           if (q >= p.Q) break;
           const int ere = p.rowExp[(size_t)m * p.R + 2 * q];
           const int eim = p.rowExp[(size_t)m * p.R + 2 * q + 1];
-          double2 val = make_double2(ldexp(acc[2 * i], eA + ere), ldexp(acc[2 * i + 1], eA + eim));
-          if (kDir == 0) {
-            p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] = val;
-          } else {
+          p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
+              make_double2(ldexp(acc[2 * i], eA + ere), ldexp(acc[2 * i + 1], eA + eim));
+        }
+      } else {
+        const int l = l0 + tileRow;
+#pragma unroll
+        for (int b0 = 0; b0 < kCols / 2; b0 += 4) {
+          double2* ptr[4];
+          double2 old[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const int q = q0 + b0 + i;
+            ptr[i] = nullptr;
+            if (q >= p.Q) continue;
             const int sgn = q / p.count, f = q - sgn * p.count;
             if (sgn == 1 && m == 0) continue;
-            const int l = l0 + tileRow;
+            const long idx = p.isReal
+                                 ? (long)l * (l + 1) / 2 - (long)p.na * (p.na + 1) / 2 + m
+                                 : (long)l * l - (long)p.n * p.n + l + (sgn ? -m : m);
+            ptr[i] = p.out + (size_t)f * p.coefSize + idx;
+          }
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+            if (ptr[i]) old[i] = *ptr[i];
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            if (!ptr[i]) continue;
+            const int q = q0 + b0 + i;
+            const int sgn = q / p.count;
+            const int ere = p.rowExp[(size_t)m * p.R + 2 * q];
+            const int eim = p.rowExp[(size_t)m * p.R + 2 * q + 1];
+            double2 val = make_double2(ldexp(acc[2 * (b0 + i)], ere),
+                                       ldexp(acc[2 * (b0 + i) + 1], eim));
             if (sgn == 1 && ((l + p.n) & 1)) val = make_double2(-val.x, -val.y);
-            long idx;
-            if (p.isReal) {
-              idx = (long)l * (l + 1) / 2 - (long)p.na * (p.na + 1) / 2 + m;
-            } else {
-              idx = (long)l * l - (long)p.n * p.n + l + (sgn ? -m : m);
-            }
-            double2* o = p.out + (size_t)f * p.coefSize + idx;
             if (!p.isReal && sgn == 0 && m == p.L && l == p.L && p.lmax == p.L) {
-              *o = make_double2(0.0, 0.0);
+              *ptr[i] = make_double2(0.0, 0.0);  // GaussLegendreGrid.h:209-215
             } else {
-              const double2 c0 = *o;
-              *o = make_double2(c0.x + val.x, c0.y + val.y);
+              *ptr[i] = make_double2(old[i].x + val.x, old[i].y + val.y);
             }
           }
         }
@@ -220,7 +275,29 @@ __device__ __forceinline__ void write_slices(double y, int8_t* dst, size_t plane
   }
 }
 
-// Inverse: packed coefficients -> slices over degrees, K pitch `pitch`.
+// Four values -> seven slice quads, s-th quad to dst + s * plane (4-byte
+// aligned): the 4-wide form of write_slices.
+__device__ __forceinline__ void write_slices4(const double (&y0)[4], int8_t* dst, size_t plane) {
+  double y[4] = {y0[0], y0[1], y0[2], y0[3]};
+#pragma unroll
+  for (int s = 0; s < kS; s++) {
+    char4 c;
+    int8_t* cc = reinterpret_cast<int8_t*>(&c);
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      y[t] *= 128.0;
+      const double q = trunc(y[t]);
+      y[t] -= q;
+      cc[t] = (int8_t)q;
+    }
+    *reinterpret_cast<char4*>(dst + s * plane) = c;
+  }
+}
+
+// Inverse: packed coefficients -> slices over degrees, K pitch `pitch` (a
+// multiple of 64). One warp per row (m, q): the row maxima give the two
+// exponents, then each lane writes four consecutive degrees as 4-byte slice
+// quads.
 __global__ void k_prep_inverse_oz(int lmax, int n, int na, int count, int Q, int R, int isReal,
                                   long coefSize, int pitch, size_t plane,
                                   const double2* __restrict__ coef, int8_t* __restrict__ op,
@@ -259,15 +336,23 @@ __global__ void k_prep_inverse_oz(int lmax, int n, int na, int count, int Q, int
     rowExp[(size_t)m * R + 2 * q] = ere;
     rowExp[(size_t)m * R + 2 * q + 1] = eim;
   }
-  for (int k = lane; k < kp; k += 32) {
-    const double2 v = value(k);
-    write_slices(ldexp(v.x, -ere), op + r0 + k, plane);
-    write_slices(ldexp(v.y, -eim), op + r0 + pitch + k, plane);
+  for (int k4 = 4 * lane; k4 < kp; k4 += 128) {
+    double re[4], im[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const double2 v = value(k4 + t);
+      re[t] = ldexp(v.x, -ere);
+      im[t] = ldexp(v.y, -eim);
+    }
+    write_slices4(re, op + r0 + k4, plane);
+    write_slices4(im, op + r0 + pitch + k4, plane);
   }
 }
 
 // Forward: weighted spectra times the table column scales -> slices over
-// colatitudes (pitch thetaPad).
+// colatitudes (pitch thetaPad, a multiple of 16). One warp per row (m, q),
+// four consecutive colatitudes per lane: a first pass finds the row maxima,
+// the second (reading the row again, now from L2) writes 4-byte slice quads.
 __global__ void k_prep_forward_oz(int lmax, int Q, int R, int thetaPad, size_t plane,
                                   const double2* __restrict__ spec,
                                   const int* __restrict__ tabExp, int8_t* __restrict__ op,
@@ -276,12 +361,18 @@ __global__ void k_prep_forward_oz(int lmax, int Q, int R, int thetaPad, size_t p
   if (wid >= (lmax + 1) * Q) return;
   const int m = wid / Q, q = wid - m * Q;
   const double2* row = spec + ((size_t)m * Q + q) * thetaPad;
-  const int* te = tabExp + (size_t)m * thetaPad;
+  const int4* te4 = reinterpret_cast<const int4*>(tabExp + (size_t)m * thetaPad);
+  const int nq = thetaPad / 4;
   double mre = 0.0, mim = 0.0;
-  for (int j = lane; j < thetaPad; j += 32) {
-    const double2 v = row[j];
-    mre = fmax(mre, fabs(ldexp(v.x, te[j])));
-    mim = fmax(mim, fabs(ldexp(v.y, te[j])));
+  for (int j4 = lane; j4 < nq; j4 += 32) {
+    const int4 e = te4[j4];
+    const int ev[4] = {e.x, e.y, e.z, e.w};
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const double2 v = row[4 * j4 + t];
+      mre = fmax(mre, fabs(ldexp(v.x, ev[t])));
+      mim = fmax(mim, fabs(ldexp(v.y, ev[t])));
+    }
   }
   mre = warp_max(mre);
   mim = warp_max(mim);
@@ -293,32 +384,21 @@ __global__ void k_prep_forward_oz(int lmax, int Q, int R, int thetaPad, size_t p
     rowExp[(size_t)m * R + 2 * q + 1] = eim;
   }
   const size_t r0 = ((size_t)m * R + 2 * q) * thetaPad;
-  for (int j = lane; j < thetaPad; j += 32) {
-    const double2 v = row[j];
-    write_slices(ldexp(v.x, te[j] - ere), op + r0 + j, plane);
-    write_slices(ldexp(v.y, te[j] - eim), op + r0 + thetaPad + j, plane);
+  for (int j4 = lane; j4 < nq; j4 += 32) {
+    const int4 e = te4[j4];
+    const int ev[4] = {e.x, e.y, e.z, e.w};
+    double re[4], im[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const double2 v = row[4 * j4 + t];
+      re[t] = ldexp(v.x, ev[t] - ere);
+      im[t] = ldexp(v.y, ev[t] - eim);
+    }
+    write_slices4(re, op + r0 + 4 * j4, plane);
+    write_slices4(im, op + r0 + thetaPad + 4 * j4, plane);
   }
 }
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void* ptr = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(ptr);
-    else
-      cudaGetLastError();
-  }
-  return fn;
-}
 
 // 3-D byte tensor [planes][rows][inner] with a [1][boxRows][boxInner] box.
 gsht_status make_map_i8(CUtensorMap* map, const void* base, uint64_t inner, uint64_t rows,
@@ -338,13 +418,18 @@ gsht_status make_map_i8(CUtensorMap* map, const void* base, uint64_t inner, uint
 }
 
 template <int kDir>
-gsht_status launch_oz(const OzArgs& a, const CUtensorMap& mapA, const CUtensorMap& mapB,
-                      int gridX, cudaStream_t s) {
+gsht_status launch_oz(const gsht_grid* g, const OzArgs& a, const CUtensorMap& mapA,
+                      const CUtensorMap& mapB, cudaStream_t s) {
+  gsht_status st;
+  const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kN, kBK, &st);
+  if (!tl) return st;
   auto kern = k_legendre_oz<kDir>;
   GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSmemBytes));
-  dim3 grid(gridX, (a.R + kN - 1) / kN, a.lmax + 1);
-  kern<<<grid, 192, kSmemBytes, s>>>(mapA, mapB, a);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+  const int blocks = tl->count < sms ? tl->count : sms;
+  kern<<<blocks, kThreads, kSmemBytes, s>>>(mapA, mapB, a, tl->d_tiles, tl->count);
   GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_oz<inverse>" : "k_legendre_oz<forward>");
   return GSHT_OK;
 }
@@ -389,7 +474,7 @@ gsht_status legendre_inverse_oz(const gsht_grid* g, const Table* t, int lmax, in
   a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
-  return launch_oz<0>(a, mapA, mapB, (g->n_theta + kBM - 1) / kBM, s);
+  return launch_oz<0>(g, a, mapA, mapB, s);
 }
 
 gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
@@ -422,9 +507,8 @@ gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, in
   a.rowOff = t->d_row_off; a.tabExp = t->i8_exp; a.rowExp = rowExp;
   a.out = reinterpret_cast<double2*>(coef);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
-  const int kMax = lmax - na + 1;
   StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
-  return launch_oz<1>(a, mapA, mapB, (kMax + kBM - 1) / kBM, s);
+  return launch_oz<1>(g, a, mapA, mapB, s);
 }
 
 }  // namespace gsht

@@ -16,6 +16,7 @@
 // mbarrier wait is bounded (tc_common.cuh) and reports a timeout through
 // the grid's device error word instead of hanging.
 #include <cstdio>
+#include <vector>
 
 #include "gsht_internal.cuh"
 #include "tc_common.cuh"
@@ -26,8 +27,14 @@ namespace {
 using namespace tc;
 
 constexpr int kBM = 128;       // tile rows (TMEM lanes)
-constexpr int kBK = 64;        // K per stage: 64 x 2 B = one 128 B swizzle row
-constexpr int kTileA = kBM * kBK * 2;  // bytes per A split tile (16 KB)
+// K per stage. Inverse: 32 degrees (the MN-major table tile is two
+// 64-colatitude x 32-degree boxes with 128 B swizzle, the K-major field rows
+// one 64 B swizzle row), four 48 KB stages in flight. Forward: 64
+// colatitudes = one 128 B swizzle row of both K-major operands, two 96 KB
+// stages.
+__host__ __device__ constexpr int bk_of(int dir) { return dir == 0 ? 32 : 64; }
+__host__ __device__ constexpr int stages_of(int dir) { return dir == 0 ? 4 : 2; }
+constexpr int kBKInv = bk_of(0);
 
 struct TcArgs {
   int L, lmax, n, na, count, Q, R, nTheta, thetaPad, isReal;
@@ -48,46 +55,55 @@ constexpr int kAccumulators = kBigAcc + 1;
 __host__ __device__ constexpr int prodA(int p) { return p == 0 ? 0 : p == 1 ? 0 : p == 2 ? 1 : p == 3 ? 0 : p == 4 ? 2 : 1; }
 __host__ __device__ constexpr int prodB(int p) { return p == 0 ? 0 : p == 1 ? 1 : p == 2 ? 0 : p == 3 ? 2 : p == 4 ? 0 : 1; }
 
-template <int kNA, int kNB, int kN, int kStages>
+template <int kNA, int kNB, int kN, int kBK, int kStages>
 constexpr size_t tc_smem_bytes() {
-  return (size_t)kStages * (kNA * kTileA + kNB * kN * kBK * 2) + 1024 + 256;
+  return (size_t)kStages * (kNA * kBM * kBK * 2 + kNB * kN * kBK * 2) + 1024 + 256;
 }
 
+constexpr int kEpiWarps = 8;                 // two warps per TMEM lane quarter
+constexpr int kThreads = 32 * (2 + kEpiWarps);
+
+// Persistent kernel: each block walks the tile list with stride gridDim.x.
+// The producer runs ahead across tile boundaries; the epilogue copies its
+// accumulator columns out of TMEM, releases TMEM to the MMA warp (accEmpty),
+// and only then writes results, so stores overlap the next tile's MMAs.
 template <int kDir, int kNA, int kNB, int kNP, int kN, int kStages>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(kThreads, 1)
     k_legendre_tc(const __grid_constant__ CUtensorMap mapA,
-                  const __grid_constant__ CUtensorMap mapB, TcArgs p) {
+                  const __grid_constant__ CUtensorMap mapB, TcArgs p,
+                  const int4* __restrict__ tiles, int numTiles) {
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
-  // 1024-byte alignment for the swizzled tiles.
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
+  constexpr int kBK = bk_of(kDir);
+  constexpr int kTileA = kBM * kBK * 2;
   constexpr int kTileB = kN * kBK * 2;
   constexpr int kStageBytes = kNA * kTileA + kNB * kTileB;
+  constexpr int kCols = kN / 2;  // accumulator columns per epilogue warp
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* accBar = empty + kStages;
-  uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(accBar + 1);
+  uint64_t* accFull = empty + kStages;
+  // The epilogue releases the accumulators in two steps: accEmptyA once it
+  // has copied accumulators 0 and 1 (all the next tile's first K blocks
+  // need), accEmptyB after the hi.hi accumulators 2 and 3.
+  uint64_t* accEmptyA = accFull + 1;
+  uint64_t* accEmptyB = accFull + 2;
+  uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(accFull + 3);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int mtile = blockIdx.x, ntile = blockIdx.y, m = blockIdx.z;
-  const int l0 = m > p.na ? m : p.na;
-  const int Keff = p.lmax - l0 + 1;
-  const int rowsM = kDir == 0 ? p.nTheta : Keff;
-  if (mtile * kBM >= rowsM) return;
   __shared__ int skip;
-  if (threadIdx.x == 0) skip = *reinterpret_cast<volatile int*>(p.err);  // an earlier block timed out
+  if (threadIdx.x == 0) skip = *reinterpret_cast<volatile int*>(p.err);
   __syncthreads();
-  if (skip) return;
-  const int nk = kDir == 0 ? (Keff + kBK - 1) / kBK : (p.thetaPad + kBK - 1) / kBK;
-  const long long tRow = p.rowOff[m];
-  const int bRow = m * p.R + ntile * kN;
+  if (skip || blockIdx.x >= numTiles) return;
 
   if (warp == 0 && lane == 0) {
     for (int s = 0; s < kStages; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accBar, 1);
+    mbar_init(accFull, 1);
+    mbar_init(accEmptyA, kEpiWarps);
+    mbar_init(accEmptyB, kEpiWarps);
     fence_barrier_init();
     prefetch_tmap(&mapA);
     prefetch_tmap(&mapB);
@@ -100,109 +116,187 @@ __global__ void __launch_bounds__(192, 1)
 
   if (warp == 0) {
     if (lane == 0) {
-      for (int kc = 0; kc < nk; kc++) {
-        const int s = kc % kStages;
-        if (kc >= kStages && !mbar_wait(&empty[s], ((kc / kStages) - 1) & 1, p.err, 1)) break;
-        unsigned char* st = smem + s * kStageBytes;
-        mbar_arrive_expect_tx(&full[s], kStageBytes);
-        for (int a = 0; a < kNA; a++) {
-          unsigned char* dst = st + a * kTileA;
-          if (kDir == 0) {
-            // MN-major: two 64-colatitude halves of 64 degree rows each.
-            tma_load_3d(dst, &mapA, &full[s], mtile * kBM, (int)(tRow + kc * kBK), a);
-            tma_load_3d(dst + kTileA / 2, &mapA, &full[s], mtile * kBM + 64, (int)(tRow + kc * kBK), a);
-          } else {
-            tma_load_3d(dst, &mapA, &full[s], kc * kBK, (int)(tRow + mtile * kBM), a);
+      int it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < numTiles && ok; t += gridDim.x) {
+        const int4 tl = tiles[t];  // (m, mtile, ntile, nk)
+        const long long tRow = p.rowOff[tl.x];
+        const int bRow = tl.x * p.R + tl.z * kN;
+        for (int kc = 0; kc < tl.w; kc++, it++) {
+          const int s = it % kStages;
+          if (it >= kStages && !mbar_wait(&empty[s], ((it / kStages) - 1) & 1, p.err, 1)) {
+            ok = false;
+            break;
           }
+          unsigned char* st = smem + s * kStageBytes;
+          mbar_arrive_expect_tx(&full[s], kStageBytes);
+          for (int a = 0; a < kNA; a++) {
+            unsigned char* dst = st + a * kTileA;
+            if (kDir == 0) {
+              // MN-major: two 64-colatitude halves of 64 degree rows each.
+              tma_load_3d(dst, &mapA, &full[s], tl.y * kBM, (int)(tRow + kc * kBK), a);
+              tma_load_3d(dst + kTileA / 2, &mapA, &full[s], tl.y * kBM + 64,
+                          (int)(tRow + kc * kBK), a);
+            } else {
+              tma_load_3d(dst, &mapA, &full[s], kc * kBK, (int)(tRow + tl.y * kBM), a);
+            }
+          }
+          for (int b = 0; b < kNB; b++)
+            tma_load_3d(st + kNA * kTileA + b * kTileB, &mapB, &full[s], kc * kBK, bRow, b);
         }
-        for (int b = 0; b < kNB; b++)
-          tma_load_3d(st + kNA * kTileA + b * kTileB, &mapB, &full[s], kc * kBK, bRow, b);
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t id = idesc(1, 1, kDir == 0 ? 1 : 0, 0, kN, kBM);
-      // hi.hi products go to one of nbig accumulators by K block; the five
-      // smaller products share accumulator 0 (see kAccumulators).
-      const int nbig = nk < kBigAcc ? nk : kBigAcc;
+      int it = 0, tc = 0;
       bool ok = true;
-      for (int kc = 0; kc < nk && ok; kc++) {
-        const int s = kc % kStages;
-        if (!mbar_wait(&full[s], (kc / kStages) & 1, p.err, 2)) {
-          ok = false;
-          break;
-        }
+      for (int t = blockIdx.x; t < numTiles && ok; t += gridDim.x, tc++) {
+        const int nk = tiles[t].w;
+        if (tc > 0 && !mbar_wait(accEmptyA, (tc - 1) & 1, p.err, 4)) break;
         tc_fence_after();
-        const int big = 1 + (kc * nbig) / nk;
-        const int bigFirst = ((big - 1) * nk + nbig - 1) / nbig;
-        const uint32_t st = smem_u32(smem + s * kStageBytes);
-#pragma unroll
-        for (int pr = 0; pr < kNP; pr++) {
-          const uint32_t aBase = st + prodA(pr) * kTileA;
-          const uint32_t bBase = st + kNA * kTileA + prodB(pr) * kTileB;
-          const uint32_t d = tmem + (uint32_t)((pr == 0 ? big : 0) * kN);
-#pragma unroll
-          for (int k16 = 0; k16 < kBK / 16; k16++) {
-            const uint64_t ad = kDir == 0 ? sdesc_sw128(aBase + k16 * 2048, kTileA / 2, 1024)
-                                          : sdesc_sw128(aBase + k16 * 32, 16, 1024);
-            const uint64_t bd = sdesc_sw128(bBase + k16 * 32, 16, 1024);
-            const bool first = pr == 0 ? (kc == bigFirst && k16 == 0)
-                                       : (kc == 0 && k16 == 0 && pr == 1);
-            mma_f16(d, ad, bd, id, first ? 0u : 1u);
+        bool haveB = tc == 0;
+        // hi.hi products go to one of nbig accumulators by K block; the five
+        // smaller products share accumulator 0 (see kAccumulators).
+        const int nbig = nk < kBigAcc ? nk : kBigAcc;
+        for (int kc = 0; kc < nk; kc++, it++) {
+          const int s = it % kStages;
+          if (!mbar_wait(&full[s], (it / kStages) & 1, p.err, 2)) {
+            ok = false;
+            break;
           }
+          tc_fence_after();
+          const int big = 1 + (kc * nbig) / nk;
+          const int bigFirst = ((big - 1) * nk + nbig - 1) / nbig;
+          if (!haveB && big >= 2) {
+            if (!mbar_wait(accEmptyB, (tc - 1) & 1, p.err, 5)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            haveB = true;
+          }
+          const uint32_t st = smem_u32(smem + s * kStageBytes);
+#pragma unroll
+          for (int pr = 0; pr < kNP; pr++) {
+            const uint32_t aBase = st + prodA(pr) * kTileA;
+            const uint32_t bBase = st + kNA * kTileA + prodB(pr) * kTileB;
+            const uint32_t d = tmem + (uint32_t)((pr == 0 ? big : 0) * kN);
+#pragma unroll
+            for (int k16 = 0; k16 < kBK / 16; k16++) {
+              uint64_t ad, bd;
+              if constexpr (kDir == 0) {
+                ad = sdesc_sw128(aBase + k16 * 2048, kTileA / 2, 1024);
+                bd = sdesc_sw64(bBase + k16 * 32, 16, 512);
+              } else {
+                ad = sdesc_sw128(aBase + k16 * 32, 16, 1024);
+                bd = sdesc_sw128(bBase + k16 * 32, 16, 1024);
+              }
+              const bool first = pr == 0 ? (kc == bigFirst && k16 == 0)
+                                         : (kc == 0 && k16 == 0 && pr == 1);
+              mma_f16(d, ad, bd, id, first ? 0u : 1u);
+            }
+          }
+          mma_commit(&empty[s]);
         }
-        mma_commit(&empty[s]);
+        // Keep accEmptyB in step with the tiles even if this one used no
+        // accumulator above 1.
+        if (ok && !haveB && !mbar_wait(accEmptyB, (tc - 1) & 1, p.err, 5)) ok = false;
+        if (!ok) break;
+        mma_commit(accFull);
       }
-      mma_commit(accBar);
     }
   } else {
-    // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31.
+    // Epilogue warps 2..9: lane quarter warp % 4, column half (warp - 2) / 4.
     const int quarter = warp & 3;
+    const int half = (warp - 2) >> 2;
     const int row = quarter * 32 + lane;
-    const bool ready = mbar_wait(accBar, 0, p.err, 3);
-    tc_fence_after();
-    if (ready) {
-      const int tileRow = mtile * kBM + row;
+    int tc = 0;
+    for (int t = blockIdx.x; t < numTiles; t += gridDim.x, tc++) {
+      const int4 tl = tiles[t];
+      const int m = tl.x, nk = tl.w;
+      if (!mbar_wait(accFull, tc & 1, p.err, 3)) break;
+      tc_fence_after();
       const int nbig = nk < kBigAcc ? nk : kBigAcc;
-#pragma unroll 1
-      for (int c = 0; c < kN / 16; c++) {
-        double acc[16];
+      double acc[kCols];
 #pragma unroll
-        for (int i = 0; i < 16; i++) acc[i] = 0.0;
-#pragma unroll 1
-        for (int a = 0; a <= nbig; a++) {
-          uint32_t v[16];
-          tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + a * kN + c * 16, v);
+      for (int i = 0; i < kCols; i++) acc[i] = 0.0;
+      const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + half * kCols;
+      // Two column chunks per wait; accumulators 0 and 1 first.
+      auto drain = [&](int a) {
+#pragma unroll
+        for (int c = 0; c < kCols / 16; c += 2) {
+          uint32_t v0[16], v1[16];
+          tmem_ld16(tbase + a * kN + c * 16, v0);
+          tmem_ld16(tbase + a * kN + (c + 1) * 16, v1);
           tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 16; i++) acc[i] += (double)__uint_as_float(v[i]);
+          for (int i = 0; i < 16; i++) {
+            acc[c * 16 + i] += (double)__uint_as_float(v0[i]);
+            acc[(c + 1) * 16 + i] += (double)__uint_as_float(v1[i]);
+          }
         }
-        const int q0 = (ntile * kN + c * 16) / 2;
-        if (tileRow >= rowsM) continue;
+      };
+      drain(0);
+      drain(1);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(accEmptyA);
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
+      for (int a = 2; a <= kBigAcc; a++)
+        if (a <= nbig) drain(a);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(accEmptyB);
+      const int l0 = m > p.na ? m : p.na;
+      const int keff = p.lmax - l0 + 1;
+      const int tileRow = tl.y * kBM + row;
+      const int rowsM = kDir == 0 ? p.nTheta : keff;
+      if (tileRow >= rowsM) continue;
+      const int q0 = (tl.z * kN + half * kCols) / 2;
+      if (kDir == 0) {
+#pragma unroll
+        for (int i = 0; i < kCols / 2; i++) {
           const int q = q0 + i;
-          if (q >= p.Q) break;
-          double2 val = make_double2(acc[2 * i], acc[2 * i + 1]);
-          if (kDir == 0) {
-            p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] = val;
-          } else {
+          if (q < p.Q)
+            p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
+                make_double2(acc[2 * i], acc[2 * i + 1]);
+        }
+      } else {
+        const int l = l0 + tileRow;
+        // Read-modify-write of the packed coefficients in batches of kRmw,
+        // all loads of a batch issued before its stores.
+        constexpr int kRmw = 2;
+#pragma unroll
+        for (int b0 = 0; b0 < kCols / 2; b0 += kRmw) {
+          double2* ptr[kRmw];
+          double2 old[kRmw];
+#pragma unroll
+          for (int i = 0; i < kRmw; i++) {
+            const int q = q0 + b0 + i;
+            ptr[i] = nullptr;
+            if (q >= p.Q) continue;
             const int sgn = q / p.count, f = q - sgn * p.count;
             if (sgn == 1 && m == 0) continue;
-            const int l = l0 + tileRow;
+            const long idx = p.isReal
+                                 ? (long)l * (l + 1) / 2 - (long)p.na * (p.na + 1) / 2 + m
+                                 : (long)l * l - (long)p.n * p.n + l + (sgn ? -m : m);
+            ptr[i] = p.out + (size_t)f * p.coefSize + idx;
+          }
+#pragma unroll
+          for (int i = 0; i < kRmw; i++)
+            if (ptr[i]) old[i] = *ptr[i];
+#pragma unroll
+          for (int i = 0; i < kRmw; i++) {
+            if (!ptr[i]) continue;
+            const int q = q0 + b0 + i;
+            const int sgn = q / p.count;
+            double2 val = make_double2(acc[2 * (b0 + i)], acc[2 * (b0 + i) + 1]);
             if (sgn == 1 && ((l + p.n) & 1)) val = make_double2(-val.x, -val.y);
-            long idx;
-            if (p.isReal) {
-              idx = (long)l * (l + 1) / 2 - (long)p.na * (p.na + 1) / 2 + m;
-            } else {
-              idx = (long)l * l - (long)p.n * p.n + l + (sgn ? -m : m);
-            }
-            double2* o = p.out + (size_t)f * p.coefSize + idx;
             if (!p.isReal && sgn == 0 && m == p.L && l == p.L && p.lmax == p.L) {
-              *o = make_double2(0.0, 0.0);
+              *ptr[i] = make_double2(0.0, 0.0);  // GaussLegendreGrid.h:209-215
             } else {
-              const double2 c0 = *o;
-              *o = make_double2(c0.x + val.x, c0.y + val.y);
+              *ptr[i] = make_double2(old[i].x + val.x, old[i].y + val.y);
             }
           }
         }
@@ -228,39 +322,52 @@ __device__ __forceinline__ void split3(double x, __nv_bfloat16& h, __nv_bfloat16
   lo = __double2bfloat16(r1 - (double)__bfloat162float(md));
 }
 
-// Inverse: packed coefficients -> B[split][m*R + 2q + part][k], k < Kp_m.
-__global__ void k_prep_inverse_bf16(int lmax, int n, int na, int count, int Q, int R,
-                                    int isReal, long coefSize, int pitch, size_t plane,
-                                    const double2* __restrict__ coef,
-                                    __nv_bfloat16* __restrict__ op) {
-  const int m = blockIdx.y, q = blockIdx.z;
+// Inverse: packed coefficients -> B[split][m*R + 2q + part][k], k = l - l0(m)
+// < Kp_m (zero beyond lmax). One block per 32 degrees x 32 orders of one
+// field row q: the packed layout is contiguous along orders for a fixed
+// degree, so the tile is read order-major (coalesced), transposed in shared
+// memory and written degree-major (each order's operand row segment).
+__global__ void __launch_bounds__(256) k_prep_inverse_bf16(
+    int lmax, int n, int na, int count, int Q, int R, int isReal, long coefSize, int pitch,
+    size_t plane, const double2* __restrict__ coef, __nv_bfloat16* __restrict__ op) {
+  __shared__ double2 tile[32][33];
+  const int lt = blockIdx.x * 32, mt = blockIdx.y * 32, q = blockIdx.z;
   const int sgn = q / count, f = q - sgn * count;
-  const int l0 = m > na ? m : na;
-  const int kp = (lmax - l0 + 1 + kBK - 1) / kBK * kBK;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= kp) return;
-  const int l = l0 + k;
-  double2 v = make_double2(0.0, 0.0);
-  if (l <= lmax && !(sgn == 1 && m == 0)) {
-    long idx;
-    if (isReal) {
-      idx = (long)l * (l + 1) / 2 - (long)na * (na + 1) / 2 + m;
-    } else {
-      idx = (long)l * l - (long)n * n + l + (sgn ? -m : m);
+  if (lt + 31 < (mt > na ? mt : na) || mt > lmax) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int i = warp; i < 32; i += 8) {
+    const int l = lt + i, m = mt + lane;
+    double2 v = make_double2(0.0, 0.0);
+    if (l <= lmax && m <= l && l >= na && !(sgn == 1 && m == 0)) {
+      const long idx = isReal ? (long)l * (l + 1) / 2 - (long)na * (na + 1) / 2 + m
+                              : (long)l * l - (long)n * n + l + (sgn ? -m : m);
+      v = coef[(size_t)f * coefSize + idx];
+      if (sgn == 1 && ((l + n) & 1)) v = make_double2(-v.x, -v.y);
     }
-    v = coef[(size_t)f * coefSize + idx];
-    if (sgn == 1 && ((l + n) & 1)) v = make_double2(-v.x, -v.y);
+    tile[i][lane] = v;
   }
-  const size_t r0 = ((size_t)m * R + 2 * q) * pitch + k;
-  __nv_bfloat16 h, md, lo;
-  split3(v.x, h, md, lo);
-  op[r0] = h;
-  op[plane + r0] = md;
-  op[2 * plane + r0] = lo;
-  split3(v.y, h, md, lo);
-  op[r0 + pitch] = h;
-  op[plane + r0 + pitch] = md;
-  op[2 * plane + r0 + pitch] = lo;
+  __syncthreads();
+#pragma unroll
+  for (int jj = warp; jj < 32; jj += 8) {
+    const int m = mt + jj;
+    if (m > lmax) break;
+    const int l0 = m > na ? m : na;
+    const int kp = (lmax - l0 + 1 + kBKInv - 1) / kBKInv * kBKInv;
+    const int k = lt + lane - l0;
+    if (k < 0 || k >= kp) continue;
+    const double2 v = tile[lane][jj];
+    const size_t r0 = ((size_t)m * R + 2 * q) * pitch + k;
+    __nv_bfloat16 h, md, lo;
+    split3(v.x, h, md, lo);
+    op[r0] = h;
+    op[plane + r0] = md;
+    op[2 * plane + r0] = lo;
+    split3(v.y, h, md, lo);
+    op[r0 + pitch] = h;
+    op[plane + r0 + pitch] = md;
+    op[2 * plane + r0 + pitch] = lo;
+  }
 }
 
 // Forward: weighted spectra (FP64) -> B[split][m*R + 2q + part][j].
@@ -287,30 +394,11 @@ __global__ void k_prep_forward_bf16(int lmax, int Q, int R, int thetaPad, size_t
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void* ptr = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(ptr);
-    else
-      cudaGetLastError();
-  }
-  return fn;
-}
-
-// 3-D BF16 tensor [planes][rows][inner] with a [1][boxRows][64] box, 128 B swizzle.
+// 3-D BF16 tensor [planes][rows][inner] with a [1][boxRows][boxInner] box.
 gsht_status make_map_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t rows,
                           uint64_t planes, uint64_t rowPitchElems, uint64_t planeElems,
-                          uint32_t boxInner, uint32_t boxRows) {
+                          uint32_t boxInner, uint32_t boxRows, CUtensorMapSwizzle sw) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return fail(GSHT_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   cuuint64_t dims[3] = {inner, rows, planes};
@@ -318,32 +406,70 @@ gsht_status make_map_bf16(CUtensorMap* map, const void* base, uint64_t inner, ui
   cuuint32_t box[3] = {boxInner, boxRows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims,
-                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(GSHT_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return GSHT_OK;
 }
 
-constexpr int kNsplit = 3, kNprod = 6, kNTile = 128, kStagesBf = 2;
+constexpr int kNsplit = 3, kNprod = 6, kNTile = 128;
 
 template <int kDir>
 gsht_status launch_bf16(const gsht_grid* g, const Table* t, const TcArgs& a,
-                        const CUtensorMap& mapA, const CUtensorMap& mapB, int gridX,
-                        cudaStream_t s) {
-  auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kNTile, kStagesBf>;
-  const size_t sm = tc_smem_bytes<kNsplit, kNsplit, kNTile, kStagesBf>();
+                        const CUtensorMap& mapA, const CUtensorMap& mapB, cudaStream_t s) {
+  gsht_status st;
+  const TileList* tl =
+      tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kNTile, bk_of(kDir), &st);
+  if (!tl) return st;
+  auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kNTile, stages_of(kDir)>;
+  const size_t sm = tc_smem_bytes<kNsplit, kNsplit, kNTile, bk_of(kDir), stages_of(kDir)>();
   GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  dim3 grid(gridX, (a.R + kNTile - 1) / kNTile, a.lmax + 1);
-  kern<<<grid, 192, sm, s>>>(mapA, mapB, a);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+  const int blocks = tl->count < sms ? tl->count : sms;
+  kern<<<blocks, kThreads, sm, s>>>(mapA, mapB, a, tl->d_tiles, tl->count);
   GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_tc<inverse,bf16x3>" : "k_legendre_tc<forward,bf16x3>");
   return GSHT_OK;
 }
 
 }  // namespace
 
+const TileList* tile_list(const gsht_grid* g, int dir, int lmax, int na, int rows, int ntile,
+                          int kstep, gsht_status* st) {
+  *st = GSHT_OK;
+  for (auto* t : g->tile_lists)
+    if (t->dir == dir && t->lmax == lmax && t->na == na && t->rows == rows && t->ntile == ntile &&
+        t->kstep == kstep)
+      return t;
+  std::vector<int4> v;
+  const int ntiles = (rows + ntile - 1) / ntile;
+  for (int m = 0; m <= lmax; m++) {
+    const int l0 = m > na ? m : na;
+    const int keff = lmax - l0 + 1;
+    const int mtiles = dir == 0 ? (g->n_theta + kBM - 1) / kBM : (keff + kBM - 1) / kBM;
+    const int nk = dir == 0 ? (keff + kstep - 1) / kstep : (g->theta_pad + kstep - 1) / kstep;
+    for (int mt = 0; mt < mtiles; mt++)
+      for (int nt = 0; nt < ntiles; nt++) v.push_back(make_int4(m, mt, nt, nk));
+  }
+  auto* t = new TileList();
+  t->dir = dir; t->lmax = lmax; t->na = na; t->rows = rows; t->ntile = ntile; t->kstep = kstep;
+  t->count = (int)v.size();
+  if (cudaMalloc(&t->d_tiles, sizeof(int4) * v.size()) != cudaSuccess ||
+      cudaMemcpy(t->d_tiles, v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(t->d_tiles);
+    delete t;
+    *st = fail(GSHT_ERR_OOM, "tile list allocation failed");
+    return nullptr;
+  }
+  g->tile_lists.push_back(t);
+  return t;
+}
+
 size_t bf16_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir) {
   const int R = 2 * (is_real ? 1 : 2) * count;
-  const long long pitch = dir == 0 ? g->theta_pad : round_up(lmax + 1, kBK);
+  const long long pitch = dir == 0 ? g->theta_pad : round_up(lmax + 1, kBKInv);
   return sizeof(__nv_bfloat16) * kNsplit * (size_t)(lmax + 1) * R * pitch;
 }
 
@@ -352,13 +478,13 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
                                   cudaStream_t s) {
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
-  const int pitch = (int)round_up(lmax + 1, kBK);
+  const int pitch = (int)round_up(lmax + 1, kBKInv);
   const size_t plane = (size_t)(lmax + 1) * R * pitch;
   auto* op = static_cast<__nv_bfloat16*>(operand);
   {
     StageTimer tm(GSHT_STAGE_PREP_INVERSE, s);
-    dim3 pg((pitch + 127) / 128, lmax + 1, Q);
-    k_prep_inverse_bf16<<<pg, 128, 0, s>>>(lmax, t->n, na, count, Q, R, is_real,
+    dim3 pg((lmax + 63) / 32, (lmax + 32) / 32, Q);
+    k_prep_inverse_bf16<<<pg, 256, 0, s>>>(lmax, t->n, na, count, Q, R, is_real,
                                            coef_size(lmax, t->n, is_real), pitch, plane,
                                            reinterpret_cast<const double2*>(coef), op);
     GSHT_LAUNCH_CHECK("k_prep_inverse_bf16");
@@ -366,9 +492,10 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
   CUtensorMap mapA, mapB;
   const size_t tplane = (size_t)(t->rows + kTablePadRows) * g->theta_pad;
   gsht_status st = make_map_bf16(&mapA, t->tbf, g->theta_pad, t->rows + kTablePadRows, 3,
-                                 g->theta_pad, tplane, 64, 64);
+                                 g->theta_pad, tplane, 64, kBKInv, CU_TENSOR_MAP_SWIZZLE_128B);
   if (st != GSHT_OK) return st;
-  st = make_map_bf16(&mapB, op, pitch, (uint64_t)(lmax + 1) * R, 3, pitch, plane, 64, kNTile);
+  st = make_map_bf16(&mapB, op, pitch, (uint64_t)(lmax + 1) * R, 3, pitch, plane, kBKInv, kNTile,
+                     CU_TENSOR_MAP_SWIZZLE_64B);
   if (st != GSHT_OK) return st;
   TcArgs a{};
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count; a.Q = Q; a.R = R;
@@ -376,7 +503,7 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
   a.rowOff = t->d_row_off; a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
-  return launch_bf16<0>(g, t, a, mapA, mapB, (g->n_theta + kBM - 1) / kBM, s);
+  return launch_bf16<0>(g, t, a, mapA, mapB, s);
 }
 
 gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
@@ -396,19 +523,19 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
   }
   CUtensorMap mapA, mapB;
   const size_t tplane = (size_t)(t->rows + kTablePadRows) * tp;
-  gsht_status st = make_map_bf16(&mapA, t->tbf, tp, t->rows + kTablePadRows, 3, tp, tplane, 64,
-                                 kBM);
+  gsht_status st = make_map_bf16(&mapA, t->tbf, tp, t->rows + kTablePadRows, 3, tp, tplane,
+                                 bk_of(1), kBM, CU_TENSOR_MAP_SWIZZLE_128B);
   if (st != GSHT_OK) return st;
-  st = make_map_bf16(&mapB, op, tp, (uint64_t)(lmax + 1) * R, 3, tp, plane, 64, kNTile);
+  st = make_map_bf16(&mapB, op, tp, (uint64_t)(lmax + 1) * R, 3, tp, plane, bk_of(1), kNTile,
+                     CU_TENSOR_MAP_SWIZZLE_128B);
   if (st != GSHT_OK) return st;
   TcArgs a{};
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count; a.Q = Q; a.R = R;
   a.nTheta = g->n_theta; a.thetaPad = tp; a.isReal = is_real;
   a.rowOff = t->d_row_off; a.out = reinterpret_cast<double2*>(coef);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
-  const int kMax = lmax - na + 1;
   StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
-  return launch_bf16<1>(g, t, a, mapA, mapB, (kMax + kBM - 1) / kBM, s);
+  return launch_bf16<1>(g, t, a, mapA, mapB, s);
 }
 
 }  // namespace gsht

@@ -184,3 +184,64 @@ def test_L1024_vs_reference_and_round_trip(gsht, n, is_real):
         c_ref = R.forward(L, L, n, is_real, f_ref)
     assert relerr(f, f_ref) < TOL
     assert relerr(back, c_ref) < TOL
+
+
+@pytest.mark.parametrize("L", [32, 64, 128, 256, 512])
+def test_power_of_two_ring_lengths_vs_restated(gsht, restated, L):
+    # Every compiled power-of-two ring length: complex fields use nPhi = 2L
+    # points, real ones the half-length transform of L points (32..1024).
+    # Envelope 1/(l+1) as in the L = 64 workload; without one, at L = 512 the
+    # reference's own FP64 error reaches 2e-13 (see the accuracy test below).
+    rng = np.random.default_rng(77 + L)
+    with gsht.GaussLegendreGrid(L, 1) as g:
+        for is_real, n in ((False, 1), (True, 0), (False, -1)):
+            c = oracle.random_coefficients(rng, L, L, n, is_real, 1.0)
+            f = _grid_zero(g, is_real)
+            g.InverseTransformation(L, n, c, f)
+            assert relerr(f, restated.inverse(L, L, n, is_real, c)) < TOL, (is_real, n)
+            out = np.zeros_like(c)
+            g.ForwardTransformation(L, n, f, out)
+            assert relerr(out, restated.forward(L, L, n, is_real, f)) < TOL, (is_real, n)
+
+
+@pytest.mark.parametrize("is_real", [False, True])
+def test_L2048_round_trip(gsht, is_real):
+    # Ring lengths 4096 (complex) and 2048 (real); tables of L = 2048.
+    L = 2048
+    rng = np.random.default_rng(4096)
+    c = oracle.random_coefficients(rng, L, L, 0, is_real, 1.5)
+    with gsht.GaussLegendreGrid(L, 0, nrange=gsht.Single) as g:
+        f = _grid_zero(g, is_real)
+        g.InverseTransformation(L, 0, c, f)
+        back = np.zeros_like(c)
+        g.ForwardTransformation(L, 0, f, back)
+    assert relerr(back, c) < 1e-12
+
+
+def test_fp64_accuracy_at_least_the_references(gsht, reference):
+    # Unit-variance coefficients at L = 512: the reference's double-precision
+    # transforms are 2e-13 away from its own long-double instantiation
+    # (GaussLegendreGrid<long double>), so parity at 1e-13 with the double
+    # build is below both codes' rounding. The bar here: the GPU path is at
+    # least as close to the long-double result as the reference's double path.
+    L = 512
+    rng = np.random.default_rng(589)
+    rd = reference.grid(L, 1, 0, 0)
+    rl = reference.grid(L, 1, 0, 0, long_double=True)
+    try:
+        with gsht.GaussLegendreGrid(L, 1) as g:
+            for is_real, n in ((False, 1), (True, 0)):
+                c = oracle.random_coefficients(rng, L, L, n, is_real)
+                truth = rl.inverse(L, n, is_real, c)
+                f = _grid_zero(g, is_real)
+                g.InverseTransformation(L, n, c, f)
+                e_gpu, e_ref = relerr(f, truth), relerr(rd.inverse(L, n, is_real, c), truth)
+                assert e_gpu <= 1.1 * e_ref + 1e-15, ("inverse", is_real, e_gpu, e_ref)
+                truth_c = rl.forward(L, n, is_real, truth)
+                out = np.zeros_like(c)
+                g.ForwardTransformation(L, n, truth, out)
+                e_gpu, e_ref = relerr(out, truth_c), relerr(rd.forward(L, n, is_real, truth), truth_c)
+                assert e_gpu <= 1.1 * e_ref + 1e-15, ("forward", is_real, e_gpu, e_ref)
+    finally:
+        rd.close()
+        rl.close()
