@@ -23,7 +23,7 @@ import numpy as np
 __all__ = [
     "All", "NonNegative", "Single", "FP64", "BF16X3", "OZAKI",
     "GaussLegendreGrid", "GSHTError", "BadArgument", "library", "launch_count",
-    "coefficient_size",
+    "coefficient_size", "wigner",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -65,6 +65,7 @@ def _load() -> ctypes.CDLL:
     lib.gsht_grid_shape.argtypes = [vp] + [ctypes.POINTER(ip)] * 5
     lib.gsht_grid_nodes.argtypes = [vp, dp, dp]
     lib.gsht_wigner_block.argtypes = [vp, ip, ip, dp, ctypes.POINTER(ctypes.c_long)]
+    lib.gsht_wigner_compute.argtypes = [ip] * 7 + [dp, ip, dp, ctypes.POINTER(ctypes.c_long)]
     lib.gsht_coefficient_size.argtypes = [ip, ip, ip]
     lib.gsht_coefficient_size.restype = ctypes.c_long
     for f in (lib.gsht_forward, lib.gsht_inverse):
@@ -93,6 +94,21 @@ def _check(status: int):
         if status == 1:
             raise BadArgument(status, msg)
         raise GSHTError(status, msg)
+
+
+def wigner(lmax: int, mmax: int, nmax: int, theta, mrange: int = All, nrange: int = Single,
+           four_pi: bool = False, row_major: bool = False) -> np.ndarray:
+    """Wigner<double, Norm, MRange, NRange, AngleRange, Storage>(lMax, mMax,
+    nMax, theta) (Wigner.h:99-159): the values for every (n, angle) block in
+    the reference's storage order, computed on the GPU."""
+    th = np.ascontiguousarray(np.atleast_1d(np.asarray(theta, dtype=np.float64)))
+    dp = ctypes.POINTER(ctypes.c_double)
+    cnt = ctypes.c_long()
+    args = (lmax, mmax, nmax, mrange, nrange, int(four_pi), int(row_major), th.ctypes.data_as(dp), th.size)
+    _check(library.gsht_wigner_compute(*args, None, ctypes.byref(cnt)))
+    out = np.zeros(cnt.value)
+    _check(library.gsht_wigner_compute(*args, out.ctypes.data_as(dp), ctypes.byref(cnt)))
+    return out
 
 
 def coefficient_size(lmax: int, n: int, is_real: bool) -> int:

@@ -377,6 +377,28 @@ gsht_status gsht_wigner_block(const gsht_grid* g, int n, int itheta,
   return GSHT_OK;
 }
 
+gsht_status gsht_wigner_compute(int lmax, int mmax, int nmax, int mrange, int nrange,
+                                int norm, int row_major, const double* theta, int ntheta,
+                                double* out, long* count) {
+  if (lmax < 0 || mmax < 0 || nmax < 0 || nmax > lmax)
+    return fail(GSHT_ERR_BAD_ARG, "need 0 <= nmax <= lmax and mmax >= 0");
+  if (mrange != GSHT_RANGE_ALL && mrange != GSHT_RANGE_NONNEGATIVE)
+    return fail(GSHT_ERR_BAD_ARG, "mrange must be All or NonNegative");
+  if (nrange < GSHT_RANGE_ALL || nrange > GSHT_RANGE_SINGLE)
+    return fail(GSHT_ERR_BAD_ARG, "bad nrange %d", nrange);
+  if (norm != 0 && norm != 1) return fail(GSHT_ERR_BAD_ARG, "norm must be 0 (Ortho) or 1 (FourPi)");
+  if (ntheta < 1 || (!theta && out)) return fail(GSHT_ERR_BAD_ARG, "need at least one angle");
+  if (out) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      return fail(GSHT_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+  }
+  return wigner_compute(lmax, mmax, nmax, mrange, nrange, norm, row_major, theta, ntheta, out,
+                        count);
+}
+
 long gsht_coefficient_size(int lmax, int n, int is_real) {
   if (lmax < 0 || (n < 0 ? -n : n) > lmax) return -1;
   return coef_size(lmax, n, is_real);

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "gsht_internal.cuh"
 
@@ -194,7 +195,7 @@ __global__ void k_wigner_start(int L, int n, int nTheta, int thetaPad,
 // values enter the normal double range. Values are written Ortho-normalised
 // (factor sqrt(2l+1)/(2 sqrt(pi)), Wigner.h:475-485).
 __global__ void __launch_bounds__(128) k_wigner_chain(
-    int L, int n, int nTheta, int thetaPad, const double* __restrict__ theta,
+    int L, int n, int nTheta, int thetaPad, int ortho, const double* __restrict__ theta,
     const double* __restrict__ start_f, const int* __restrict__ start_e,
     const long long* __restrict__ row_off, double* __restrict__ table) {
   extern __shared__ double sh[];
@@ -208,7 +209,8 @@ __global__ void __launch_bounds__(128) k_wigner_chain(
   double* nrm = sh + 3 * K;
   for (int k = threadIdx.x; k < K; k += blockDim.x) {
     const int l = l0 + k;
-    nrm[k] = sqrt((double)(2 * l + 1)) * 0.28209479177387814347;  // 1/(2 sqrt(pi))
+    // Ortho: sqrt(2l+1)/(2 sqrt(pi)); FourPi: unnormalised (Wigner.h:475-485).
+    nrm[k] = ortho ? sqrt((double)(2 * l + 1)) * 0.28209479177387814347 : 1.0;
     a[k] = 0.0;
     b[k] = 0.0;
     g[k] = 0.0;
@@ -343,8 +345,11 @@ gsht_status build_nodes(gsht_grid* g) {
   return GSHT_OK;
 }
 
-gsht_status build_table(gsht_grid* g, Table* t, cudaStream_t s) {
-  const int L = g->L, tp = g->theta_pad, na = t->n < 0 ? -t->n : t->n;
+// Table of upper index t->n for orders 0..L at nTheta colatitudes (device
+// array theta, pitch thetaPad), in the layout described in gsht_internal.cuh.
+static gsht_status compute_table(int L, int nTheta, int thetaPad, const double* d_theta,
+                                 int ortho, Table* t, cudaStream_t s) {
+  const int tp = thetaPad, na = t->n < 0 ? -t->n : t->n;
   t->row_off.assign(L + 2, 0);
   for (int m = 0; m <= L; m++) {
     const int l0 = m > na ? m : na;
@@ -365,8 +370,8 @@ gsht_status build_table(gsht_grid* g, Table* t, cudaStream_t s) {
   int* start_e = nullptr;
   GSHT_CUDA(cudaMalloc(&start_f, sizeof(double) * (size_t)(L + 1) * tp));
   GSHT_CUDA(cudaMalloc(&start_e, sizeof(int) * (size_t)(L + 1) * tp));
-  k_wigner_start<<<(g->n_theta + 127) / 128, 128, 0, s>>>(
-      L, t->n, g->n_theta, tp, g->d_theta, start_f, start_e);
+  k_wigner_start<<<(nTheta + 127) / 128, 128, 0, s>>>(L, t->n, nTheta, tp, d_theta, start_f,
+                                                      start_e);
   GSHT_LAUNCH_CHECK("k_wigner_start");
   const size_t shmem = sizeof(double) * 4 * (L + 1);
   if (shmem > 48 * 1024) {
@@ -375,14 +380,17 @@ gsht_status build_table(gsht_grid* g, Table* t, cudaStream_t s) {
                                    (int)shmem));
   }
   dim3 grid((tp + 127) / 128, L + 1);
-  k_wigner_chain<<<grid, 128, shmem, s>>>(L, t->n, g->n_theta, tp, g->d_theta,
-                                          start_f, start_e, t->d_row_off,
-                                          t->t64);
+  k_wigner_chain<<<grid, 128, shmem, s>>>(L, t->n, nTheta, tp, ortho, d_theta, start_f,
+                                          start_e, t->d_row_off, t->t64);
   GSHT_LAUNCH_CHECK("k_wigner_chain");
   GSHT_CUDA(cudaStreamSynchronize(s));
   cudaFree(start_f);
   cudaFree(start_e);
   return GSHT_OK;
+}
+
+gsht_status build_table(gsht_grid* g, Table* t, cudaStream_t s) {
+  return compute_table(g->L, g->n_theta, g->theta_pad, g->d_theta, 1, t, s);
 }
 
 gsht_status build_forms(gsht_grid* g, Table* t, cudaStream_t s) {
@@ -412,6 +420,75 @@ gsht_status build_forms(gsht_grid* g, Table* t, cudaStream_t s) {
   }
   GSHT_CUDA(cudaStreamSynchronize(s));
   return GSHT_OK;
+}
+
+gsht_status wigner_compute(int lmax, int mmax, int nmax, int mrange, int nrange, int norm,
+                           int row_major, const double* theta, int ntheta, double* out,
+                           long* count) {
+  const bool allM = mrange == GSHT_RANGE_ALL;
+  const int nmin = nrange == GSHT_RANGE_ALL ? -nmax : (nrange == GSHT_RANGE_NONNEGATIVE ? 0 : nmax);
+  const int mm = mmax < lmax ? mmax : lmax;
+  // Block size of GSHIndices<MRange>(lmax, mmax, n) (Indexing.h:104-131).
+  auto block = [&](int n) {
+    const long na = n < 0 ? -n : n;
+    long size = 0;
+    for (long l = na; l <= lmax; l++) {
+      const long ml = l < mm ? l : mm;
+      size += allM ? 2 * ml + 1 : ml + 1;
+    }
+    return size;
+  };
+  long total = 0;
+  for (int n = nmin; n <= nmax; n++) total += block(n) * ntheta;
+  if (count) *count = total;
+  if (!out) return GSHT_OK;
+  const int tp = (int)round_up(ntheta, kThetaPad);
+  double* d_theta = nullptr;
+  GSHT_CUDA(cudaMalloc(&d_theta, sizeof(double) * tp));
+  GSHT_CUDA(cudaMemset(d_theta, 0, sizeof(double) * tp));
+  GSHT_CUDA(cudaMemcpy(d_theta, theta, sizeof(double) * ntheta, cudaMemcpyHostToDevice));
+  // Negative orders at n come from the table of -n: d^l_{-m,n} = (-1)^{m+n} d^l_{m,-n}.
+  std::vector<std::vector<double>> host(2 * nmax + 1);
+  std::vector<Table> tabs(2 * nmax + 1);
+  gsht_status st = GSHT_OK;
+  auto need = [&](int n) { return n >= nmin || (allM && -n >= nmin); };
+  for (int n = -nmax; n <= nmax && st == GSHT_OK; n++) {
+    if (!need(n)) continue;
+    Table* t = &tabs[n + nmax];
+    t->n = n;
+    st = compute_table(lmax, ntheta, tp, d_theta, norm == 0 ? 1 : 0, t, nullptr);
+    if (st != GSHT_OK) break;
+    host[n + nmax].resize((size_t)t->rows * tp);
+    if (cudaMemcpy(host[n + nmax].data(), t->t64, sizeof(double) * host[n + nmax].size(),
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = cuda_fail(cudaGetLastError(), "wigner table download");
+  }
+  if (st == GSHT_OK) {
+    const int nn = nmax - nmin + 1;
+    long off = 0;
+    for (int bi = 0; bi < nn * ntheta; bi++) {
+      // ColumnMajor: n outer, angle inner; RowMajor: angle outer, n inner.
+      const int n = row_major ? nmin + bi % nn : nmin + bi / ntheta;
+      const int it = row_major ? bi / nn : bi % ntheta;
+      const int na = n < 0 ? -n : n;
+      for (int l = na; l <= lmax; l++) {
+        const int ml = l < mm ? l : mm;
+        for (int m = allM ? -ml : 0; m <= ml; m++) {
+          const int am = m < 0 ? -m : m;
+          const int nsrc = m >= 0 ? n : -n;
+          const Table& t = tabs[nsrc + nmax];
+          const int nsa = nsrc < 0 ? -nsrc : nsrc;
+          const int l0 = am > nsa ? am : nsa;
+          double v = host[nsrc + nmax][(size_t)(t.row_off[am] + (l - l0)) * tp + it];
+          if (m < 0 && ((am + n) & 1)) v = -v;
+          out[off++] = v;
+        }
+      }
+    }
+  }
+  for (auto& t : tabs) free_table(&t);
+  cudaFree(d_theta);
+  return st;
 }
 
 void free_table(Table* t) {

@@ -92,6 +92,18 @@ gsht_status gsht_grid_nodes(const gsht_grid* grid, double* colatitudes,
 gsht_status gsht_wigner_block(const gsht_grid* grid, int n, int itheta,
                               double* out, long* count);
 
+/* Wigner<double, Norm, MRange, NRange, AngleRange, Storage>(lMax, mMax, nMax,
+ * theta) (Wigner.h:99-159, 289-486) for arbitrary angles: d^l_{mn}(theta_k)
+ * for every upper index of the NRange (All: -nMax..nMax, NonNegative:
+ * 0..nMax, Single: nMax), computed on the GPU (same recurrence and start
+ * values as the grid tables) and written to host memory in the reference's
+ * storage: one block GSHIndices<MRange>(lMax, mMax, n) per (n, angle), n
+ * outer (ColumnMajor, row_major = 0) or angle outer (RowMajor). norm: 0
+ * Ortho, 1 FourPi. With out == NULL only *count (the total length) is set. */
+gsht_status gsht_wigner_compute(int lmax, int mmax, int nmax, int mrange, int nrange,
+                                int norm, int row_major, const double* theta, int ntheta,
+                                double* out, long* count);
+
 /* Coefficient count for (lmax, n): GridBase.h:79-85 (Real/ComplexCoefficientSize). */
 long gsht_coefficient_size(int lmax, int n, int is_real);
 
@@ -135,6 +147,36 @@ gsht_status gsht_inverse_batch(const gsht_grid* grid, int lmax, int n,
  * order them. Results equal gsht_inverse with GSHT_FP64. */
 gsht_status gsht_inverse_noalloc(const gsht_grid* grid, int lmax, int n, int is_real,
                                  const void* in, void* out, void* stream);
+
+/* Fused pointwise field expressions. Replaces the materialising assignment
+ * of CanonicalComponentField expressions (CanonicalComponentFieldBase.h
+ * :201-339) over the lazy nodes of CanonicalComponentFieldBinary.h:100-305
+ * (+ - * /), CanonicalComponentFieldUnary.h:103-354 (conj, real, imag, unary
+ * minus) and the scalar forms of CanonicalComponentFieldOverloads.h:66-146.
+ * `program` is the expression in postfix order over a value stack; LOAD
+ * pushes input[arg] at the current point (a real input as x + 0i), CONST
+ * pushes re + i im, the binary operations pop b then a and push a op b.
+ * `count` fields are evaluated, field k of every buffer starting at
+ * k * field_stride elements; inputs and output hold complex (interleaved)
+ * or real doubles; a real output keeps the real part. Runs as one kernel on
+ * `stream`: each point reads its inputs once and writes its value once. With
+ * device buffers the call only enqueues; host buffers are staged through a
+ * library workspace and the call returns with the result in host memory. */
+enum {
+  GSHT_OP_LOAD = 0, GSHT_OP_CONST = 1, GSHT_OP_ADD = 2, GSHT_OP_SUB = 3,
+  GSHT_OP_MUL = 4, GSHT_OP_DIV = 5, GSHT_OP_NEG = 6, GSHT_OP_CONJ = 7,
+  GSHT_OP_REAL = 8, GSHT_OP_IMAG = 9
+};
+typedef struct gsht_expr_op {
+  int op;
+  int arg;
+  double re;
+  double im;
+} gsht_expr_op;
+gsht_status gsht_field_eval(const gsht_expr_op* program, int nops,
+                            const void* const* inputs, const int* input_is_real,
+                            int ninputs, void* out, int out_is_real, long npoints,
+                            int count, long field_stride, void* stream);
 
 /* Stage timing. No counterpart in the reference (which has no tracing):
  * while enabled, every stage of a transform call is bracketed by CUDA events

@@ -8,6 +8,8 @@ seeded inputs together with the reference's outputs:
   nodes.npz        colatitudes/weights for several grid degrees
   wigner.npz       table blocks d^l_{mn}(theta_j) (GSHIndices<All> layout)
   transforms.npz   inverse / forward / forward-accumulate cases
+  wigner_single.npz  Wigner<double, Norm, All, All>(lMax, mMax, nMax, theta)
+                     at one angle (tests/CheckAdditionTheorem.h:27 form)
 
 Run from the repository root:  python tests/golden/make_golden.py
 """
@@ -44,8 +46,32 @@ CASES = [
 ]
 
 
+# (lmax, mmax, nmax, theta, fourPi) for wigner_single.npz: mMax == lMax and
+# mMax < lMax, both normalisations, angles near a pole and mid-sphere.
+WIGNER_SINGLE = [
+    (16, 16, 4, 0.7, False),
+    (16, 16, 4, 0.7, True),
+    (24, 9, 3, 2.9, False),
+    (24, 9, 3, 0.05, True),
+]
+
+
+def make_wigner_single(ref):
+    ws = {}
+    for i, (lmax, mmax, nmax, theta, four_pi) in enumerate(WIGNER_SINGLE):
+        ws[f"c{i}_meta"] = np.array([lmax, mmax, nmax, int(four_pi)])
+        ws[f"c{i}_theta"] = np.array([theta])
+        ws[f"c{i}_values"] = ref.wigner_single(lmax, mmax, nmax, theta, four_pi=four_pi)
+    ws["count"] = np.array(len(WIGNER_SINGLE))
+    np.savez_compressed(os.path.join(HERE, "wigner_single.npz"), **ws)
+
+
 def main():
     ref = oracle.Reference()
+    if "--only-wigner-single" in sys.argv:
+        make_wigner_single(ref)
+        return
+    make_wigner_single(ref)
     nodes = {}
     for L in (4, 8, 33, 64, 1024):
         g = ref.grid(L, 0, 0, 2)
@@ -92,7 +118,7 @@ def main():
         g.close()
     tr["count"] = np.array(len(CASES))
     np.savez_compressed(os.path.join(HERE, "transforms.npz"), **tr)
-    for name in ("nodes.npz", "wigner.npz", "transforms.npz"):
+    for name in ("nodes.npz", "wigner.npz", "transforms.npz", "wigner_single.npz"):
         print(name, os.path.getsize(os.path.join(HERE, name)))
 
 

@@ -62,3 +62,23 @@ def test_no_device_is_reported_not_faked():
     with pytest.raises(g.GSHTError) as e:
         g.GaussLegendreGrid(8, 2)
     assert e.value.status == 6
+
+
+def test_wigner_compute_validates_and_sizes_without_a_device():
+    import gshtrans_b200 as g
+
+    lib = g.library
+    cnt = ctypes.c_long()
+    th = (ctypes.c_double * 3)(0.1, 0.2, 0.3)
+    # Count-only query: Wigner<double, Ortho, All, All>(20, 7, 3) at 3 angles.
+    assert lib.gsht_wigner_compute(20, 7, 3, 0, 0, 0, 0, th, 3, None, ctypes.byref(cnt)) == 0
+    want = 0
+    for n in range(-3, 4):
+        want += 3 * sum(2 * min(l, 7) + 1 for l in range(abs(n), 21))
+    assert cnt.value == want
+    with pytest.raises(g.BadArgument):
+        g.wigner(10, 10, 11, 0.5)          # nMax > lMax
+    with pytest.raises(g.BadArgument):
+        g.wigner(10, -1, 1, 0.5)           # negative mMax
+    with pytest.raises(g.BadArgument):
+        g.wigner(10, 10, 1, 0.5, mrange=2)  # MRange must be All or NonNegative

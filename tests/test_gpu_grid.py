@@ -109,3 +109,86 @@ def test_wigner_L2048_unitarity_where_reference_underflows(gsht):
                 blk = d[l * l - 1:l * l - 1 + 2 * l + 1]
                 s = np.dot(blk, blk) * 4 * np.pi / (2 * l + 1)
                 assert abs(s - 1.0) < 1e-11, (it, l, s)
+
+
+def _block_sizes(lmax, mmax, ns, all_m=True):
+    out = []
+    for n in ns:
+        s = 0
+        for l in range(abs(n), lmax + 1):
+            t = min(l, mmax)
+            s += 2 * t + 1 if all_m else t + 1
+        out.append(s)
+    return out
+
+
+def test_wigner_compute_matches_reference_fixture(gsht, golden):
+    # Wigner<double, Norm, All, All>(lMax, mMax, nMax, theta), reference values.
+    ws = golden["wigner_single"]
+    for i in range(int(ws["count"])):
+        lmax, mmax, nmax, fp = (int(x) for x in ws[f"c{i}_meta"])
+        got = gsht.wigner(lmax, mmax, nmax, ws[f"c{i}_theta"], mrange=gsht.All,
+                          nrange=gsht.All, four_pi=bool(fp))
+        want = ws[f"c{i}_values"]
+        assert got.shape == want.shape, i
+        err = np.abs(got - want).max() / np.abs(want).max()
+        assert err < 1e-13, (i, err)
+
+
+def test_wigner_compute_storage_and_ranges(gsht):
+    L, M, N = 20, 7, 3
+    th = np.array([0.3, 1.1, 2.5])
+    ns = list(range(-N, N + 1))
+    sizes = _block_sizes(L, M, ns)
+    col = gsht.wigner(L, M, N, th, nrange=gsht.All)
+    row = gsht.wigner(L, M, N, th, nrange=gsht.All, row_major=True)
+    assert col.size == row.size == 3 * sum(sizes)
+    # ColumnMajor: n outer, angle inner; RowMajor: angle outer, n inner.
+    blocks_col, off = {}, 0
+    for n, sz in zip(ns, sizes):
+        for it in range(3):
+            blocks_col[(n, it)] = col[off:off + sz]
+            off += sz
+    off = 0
+    for it in range(3):
+        for n, sz in zip(ns, sizes):
+            np.testing.assert_array_equal(row[off:off + sz], blocks_col[(n, it)])
+            off += sz
+    # One angle at a time gives the same blocks.
+    for it in range(3):
+        one = gsht.wigner(L, M, N, th[it], nrange=gsht.All)
+        np.testing.assert_array_equal(one, np.concatenate([blocks_col[(n, it)] for n in ns]))
+    # NRange NonNegative / Single select blocks; MRange NonNegative keeps m >= 0.
+    nn = gsht.wigner(L, M, N, th, nrange=gsht.NonNegative)
+    np.testing.assert_array_equal(
+        nn, np.concatenate([blocks_col[(n, it)] for n in range(0, N + 1) for it in range(3)]))
+    single = gsht.wigner(L, M, N, th, nrange=gsht.Single)
+    np.testing.assert_array_equal(single, np.concatenate([blocks_col[(N, it)] for it in range(3)]))
+    half = gsht.wigner(L, M, N, th, mrange=gsht.NonNegative, nrange=gsht.All)
+    parts = []
+    for n in ns:
+        for it in range(3):
+            b, o = blocks_col[(n, it)], 0
+            for l in range(abs(n), L + 1):
+                t = min(l, M)
+                parts.append(b[o + t:o + 2 * t + 1])
+                o += 2 * t + 1
+    np.testing.assert_array_equal(half, np.concatenate(parts))
+
+
+def test_wigner_compute_equals_grid_tables(gsht):
+    L = 64
+    with gsht.GaussLegendreGrid(L, 2) as g:
+        th = g.CoLatitudes()
+        first = _block_sizes(L, L, [-2])[0]
+        for it in (0, 17, 64):
+            cases = {
+                2: gsht.wigner(L, L, 2, th[it], nrange=gsht.Single),
+                0: gsht.wigner(L, L, 0, th[it], nrange=gsht.Single),
+                -2: gsht.wigner(L, L, 2, th[it], nrange=gsht.All)[:first],
+            }
+            for n, got in cases.items():
+                want = g.Wigner(n, it)
+                # The grid's -m rows come from the table at the mirrored node
+                # (pi - theta symmetry), so they differ in the last bits.
+                assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max(), (n, it)

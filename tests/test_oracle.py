@@ -138,3 +138,13 @@ def test_reference_addition_theorem(reference):
                 b = blocks[npr][l * l - npr * npr:l * l - npr * npr + 2 * l + 1]
                 s = np.dot(a, b) - (1.0 if n == npr else 0.0)
                 assert abs(s) < 1000 * np.finfo(float).eps
+
+
+def test_restated_wigner_vs_reference_single_angle_fixture(golden, restated):
+    # Wigner<double, Ortho, All, All>(16, 16, 4, 0.7): blocks n = -4..4.
+    ws = golden["wigner_single"]
+    lmax, mmax, nmax, fp = (int(x) for x in ws["c0_meta"])
+    assert (lmax, mmax, fp) == (16, 16, 0)
+    th = float(ws["c0_theta"][0])
+    got = np.concatenate([restated.wigner_block(lmax, n, th) for n in range(-nmax, nmax + 1)])
+    np.testing.assert_array_equal(got, ws["c0_values"])
