@@ -139,7 +139,7 @@ struct CallScope {
 
 gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
                           int precision, int count, const void* in, void* out,
-                          void* stream_ptr) {
+                          void* stream_ptr, int ntile = 128) {
   gsht_status st = validate(g, lmax, n, is_real, precision, count);
   if (st != GSHT_OK) return st;
   GSHT_CUDA(cudaSetDevice(g->device));
@@ -169,10 +169,19 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
   auto carve = [&](size_t b) { size_t o = off; off += round_up(b, 256); return o; };
   const size_t oSpec = carve(specBytes), oOp = carve(opBytes);
   const size_t oIn = carve(inDev ? 0 : inBytes), oOut = carve(outDev ? 0 : outBytes);
+  // Inside a stream capture (batch graphs) nothing may be allocated, the
+  // calls are serial on one stream, and events recorded outside the capture
+  // may not be waited on.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  GSHT_CUDA(cudaStreamIsCapturing(s, &cap));
+  const bool capturing = cap != cudaStreamCaptureStatusNone;
+  if (capturing && g->ws_bytes < (off > 0 ? off : 256))
+    return fail(GSHT_ERR_UNSUPPORTED, "workspace must be sized by an uncaptured call first");
   st = ensure_workspace(g, off > 0 ? off : 256);
   if (st != GSHT_OK) return st;
   char* ws = static_cast<char*>(g->ws);
-  if (g->ws_done) GSHT_CUDA(cudaStreamWaitEvent(s, g->ws_done, 0));
+  // Calls on other streams may still use the workspace: order after them.
+  if (g->ws_done && !capturing) GSHT_CUDA(cudaStreamWaitEvent(s, g->ws_done, 0));
 
   const double* dIn = inDev ? static_cast<const double*>(in) : reinterpret_cast<double*>(ws + oIn);
   double* dOut = outDev ? static_cast<double*>(out) : reinterpret_cast<double*>(ws + oOut);
@@ -194,7 +203,7 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
       }
       if (st != GSHT_OK) return st;
       if (precision == GSHT_BF16X3) {
-        st = legendre_forward_bf16(g, t, lmax, is_real, count, spec, ws + oOp, dOut, s);
+        st = legendre_forward_bf16(g, t, lmax, is_real, count, spec, ws + oOp, dOut, ntile, s);
       } else if (precision == GSHT_OZAKI) {
         st = legendre_forward_oz(g, t, lmax, is_real, count, spec, ws + oOp, dOut, s);
       } else {
@@ -204,7 +213,7 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
       if (st != GSHT_OK) return st;
     } else {
       if (precision == GSHT_BF16X3) {
-        st = legendre_inverse_bf16(g, t, lmax, is_real, count, dIn, ws + oOp, spec, s);
+        st = legendre_inverse_bf16(g, t, lmax, is_real, count, dIn, ws + oOp, spec, ntile, s);
       } else if (precision == GSHT_OZAKI) {
         st = legendre_inverse_oz(g, t, lmax, is_real, count, dIn, ws + oOp, spec, s);
       } else {
@@ -220,8 +229,10 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
     }
   }
   if (!outDev) GSHT_CUDA(cudaMemcpyAsync(out, dOut, outBytes, cudaMemcpyDeviceToHost, s));
-  if (!g->ws_done) GSHT_CUDA(cudaEventCreateWithFlags(&g->ws_done, cudaEventDisableTiming));
-  GSHT_CUDA(cudaEventRecord(g->ws_done, s));
+  if (!capturing) {
+    if (!g->ws_done) GSHT_CUDA(cudaEventCreateWithFlags(&g->ws_done, cudaEventDisableTiming));
+    GSHT_CUDA(cudaEventRecord(g->ws_done, s));
+  }
   if (!inDev || !outDev) {
     GSHT_CUDA(cudaStreamSynchronize(s));
     int err = 0;
@@ -235,6 +246,12 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
 }
 
 }  // namespace
+
+gsht_status transform(gsht_grid* g, int dir, int lmax, int n, int is_real, int precision,
+                      int count, const void* in, void* out, cudaStream_t s, int ntile) {
+  return run_transform(g, dir, lmax, n, is_real, precision, count, in, out, s, ntile);
+}
+
 }  // namespace gsht
 
 using namespace gsht;

@@ -178,12 +178,17 @@ gsht_status legendre_inverse_fp64_layout(const gsht_grid* g, const Table* t, int
 // Legendre stage, BF16x3 on tcgen05 (legendre_tc.cu). dir 0 = forward
 // (operand rows over colatitudes), 1 = inverse (rows over degrees).
 size_t bf16_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir);
+// One batched transform (the body of gsht_forward_batch / gsht_inverse_batch)
+// with an explicit BF16x3 tile width; dir 0 forward, 1 inverse.
+gsht_status transform(gsht_grid* g, int dir, int lmax, int n, int is_real, int precision,
+                      int count, const void* in, void* out, cudaStream_t s, int ntile);
 gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
                                   int count, const double* coef, void* operand, double* spec,
-                                  cudaStream_t s);
+                                  int ntile, cudaStream_t s);
+// The spectra buffer is reused for the kernel's result rows.
 gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
-                                  int count, const double* spec, void* operand, double* coef,
-                                  cudaStream_t s);
+                                  int count, double* spec, void* operand, double* coef,
+                                  int ntile, cudaStream_t s);
 
 // Legendre stage, Ozaki INT8 slices on tcgen05 (legendre_oz.cu).
 size_t oz_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir);

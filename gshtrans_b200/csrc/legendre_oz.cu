@@ -48,7 +48,7 @@ struct OzArgs {
   int* err;
 };
 
-constexpr int kEpiWarps = 8;  // two warps per TMEM lane quarter
+constexpr int kEpiWarps = 8;  // two warps per TMEM lane quarter, one column group each
 constexpr int kThreads = 32 * (2 + kEpiWarps);
 
 // Persistent kernel over the tile list (see legendre_tc.cu for the protocol):
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
-  constexpr int kCols = kN / 2;
+  constexpr int kCols = kN / (kEpiWarps / 4);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
   uint64_t* accFull = empty + kStages;
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {
     const int quarter = warp & 3;
-    const int half = (warp - 2) >> 2;
+    const int group = (warp - 2) >> 2;
     const int row = quarter * 32 + lane;
     int tc = 0;
     for (int t = blockIdx.x; t < numTiles; t += gridDim.x, tc++) {
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
       for (int d = 0; d < kNDiag; d++) {
         const double w = ldexp(1.0, -7 * (d + 2));
-        const uint32_t ta = tmem + ((uint32_t)(quarter * 32) << 16) + d * kN + half * kCols;
+        const uint32_t ta = tmem + ((uint32_t)(quarter * 32) << 16) + d * kN + group * kCols;
         uint32_t v0[16], v1[16];
         tmem_ld16(ta, v0);
         tmem_ld16(ta + 16, v1);
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int rowsM = kDir == 0 ? p.nTheta : keff;
       if (tileRow >= rowsM) continue;
       const int eA = kDir == 0 ? p.tabExp[(size_t)m * p.thetaPad + tileRow] : 0;
-      const int q0 = (tl.z * kN + half * kCols) / 2;
+      const int q0 = (tl.z * kN + group * kCols) / 2;
       if (kDir == 0) {
 #pragma unroll
         for (int i = 0; i < kCols / 2; i++) {
@@ -421,13 +421,13 @@ template <int kDir>
 gsht_status launch_oz(const gsht_grid* g, const OzArgs& a, const CUtensorMap& mapA,
                       const CUtensorMap& mapB, cudaStream_t s) {
   gsht_status st;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
   const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kN, kBK, &st);
   if (!tl) return st;
   auto kern = k_legendre_oz<kDir>;
   GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSmemBytes));
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
   const int blocks = tl->count < sms ? tl->count : sms;
   kern<<<blocks, kThreads, kSmemBytes, s>>>(mapA, mapB, a, tl->d_tiles, tl->count);
   GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_oz<inverse>" : "k_legendre_oz<forward>");

@@ -60,7 +60,7 @@ constexpr size_t tc_smem_bytes() {
   return (size_t)kStages * (kNA * kBM * kBK * 2 + kNB * kN * kBK * 2) + 1024 + 256;
 }
 
-constexpr int kEpiWarps = 8;                 // two warps per TMEM lane quarter
+constexpr int kEpiWarps = 8;  // two warps per TMEM lane quarter, one column group each
 constexpr int kThreads = 32 * (2 + kEpiWarps);
 
 // Persistent kernel: each block walks the tile list with stride gridDim.x.
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   constexpr int kTileA = kBM * kBK * 2;
   constexpr int kTileB = kN * kBK * 2;
   constexpr int kStageBytes = kNA * kTileA + kNB * kTileB;
-  constexpr int kCols = kN / 2;  // accumulator columns per epilogue warp
+  constexpr int kCols = kN / (kEpiWarps / 4);  // accumulator columns per epilogue warp
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
   uint64_t* accFull = empty + kStages;
@@ -207,9 +207,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   } else {
-    // Epilogue warps 2..9: lane quarter warp % 4, column half (warp - 2) / 4.
+    // Epilogue warps 2..17: lane quarter warp % 4, column group (warp - 2) / 4.
     const int quarter = warp & 3;
-    const int half = (warp - 2) >> 2;
+    const int group = (warp - 2) >> 2;
     const int row = quarter * 32 + lane;
     int tc = 0;
     for (int t = blockIdx.x; t < numTiles; t += gridDim.x, tc++) {
@@ -221,19 +221,20 @@ __global__ void __launch_bounds__(kThreads, 1)
       double acc[kCols];
 #pragma unroll
       for (int i = 0; i < kCols; i++) acc[i] = 0.0;
-      const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + half * kCols;
+      const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + group * kCols;
       // Two column chunks per wait; accumulators 0 and 1 first.
       auto drain = [&](int a) {
 #pragma unroll
         for (int c = 0; c < kCols / 16; c += 2) {
+          constexpr bool kPair = kCols / 16 > 1;
           uint32_t v0[16], v1[16];
           tmem_ld16(tbase + a * kN + c * 16, v0);
-          tmem_ld16(tbase + a * kN + (c + 1) * 16, v1);
+          if (kPair) tmem_ld16(tbase + a * kN + (c + 1) * 16, v1);
           tmem_wait_ld();
 #pragma unroll
           for (int i = 0; i < 16; i++) {
             acc[c * 16 + i] += (double)__uint_as_float(v0[i]);
-            acc[(c + 1) * 16 + i] += (double)__uint_as_float(v1[i]);
+            if (kPair) acc[(c + 1) * 16 + i] += (double)__uint_as_float(v1[i]);
           }
         }
       };
@@ -253,53 +254,16 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int tileRow = tl.y * kBM + row;
       const int rowsM = kDir == 0 ? p.nTheta : keff;
       if (tileRow >= rowsM) continue;
-      const int q0 = (tl.z * kN + half * kCols) / 2;
-      if (kDir == 0) {
+      const int q0 = (tl.z * kN + group * kCols) / 2;
+      // Both directions write order-major rows [m][q][row] (row = colatitude
+      // for the inverse, degree offset l - l0 for the forward); the forward's
+      // rows are added into the packed coefficients by k_accumulate_forward.
 #pragma unroll
-        for (int i = 0; i < kCols / 2; i++) {
-          const int q = q0 + i;
-          if (q < p.Q)
-            p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
-                make_double2(acc[2 * i], acc[2 * i + 1]);
-        }
-      } else {
-        const int l = l0 + tileRow;
-        // Read-modify-write of the packed coefficients in batches of kRmw,
-        // all loads of a batch issued before its stores.
-        constexpr int kRmw = 2;
-#pragma unroll
-        for (int b0 = 0; b0 < kCols / 2; b0 += kRmw) {
-          double2* ptr[kRmw];
-          double2 old[kRmw];
-#pragma unroll
-          for (int i = 0; i < kRmw; i++) {
-            const int q = q0 + b0 + i;
-            ptr[i] = nullptr;
-            if (q >= p.Q) continue;
-            const int sgn = q / p.count, f = q - sgn * p.count;
-            if (sgn == 1 && m == 0) continue;
-            const long idx = p.isReal
-                                 ? (long)l * (l + 1) / 2 - (long)p.na * (p.na + 1) / 2 + m
-                                 : (long)l * l - (long)p.n * p.n + l + (sgn ? -m : m);
-            ptr[i] = p.out + (size_t)f * p.coefSize + idx;
-          }
-#pragma unroll
-          for (int i = 0; i < kRmw; i++)
-            if (ptr[i]) old[i] = *ptr[i];
-#pragma unroll
-          for (int i = 0; i < kRmw; i++) {
-            if (!ptr[i]) continue;
-            const int q = q0 + b0 + i;
-            const int sgn = q / p.count;
-            double2 val = make_double2(acc[2 * (b0 + i)], acc[2 * (b0 + i) + 1]);
-            if (sgn == 1 && ((l + p.n) & 1)) val = make_double2(-val.x, -val.y);
-            if (!p.isReal && sgn == 0 && m == p.L && l == p.L && p.lmax == p.L) {
-              *ptr[i] = make_double2(0.0, 0.0);  // GaussLegendreGrid.h:209-215
-            } else {
-              *ptr[i] = make_double2(old[i].x + val.x, old[i].y + val.y);
-            }
-          }
-        }
+      for (int i = 0; i < kCols / 2; i++) {
+        const int q = q0 + i;
+        if (q < p.Q)
+          p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
+              make_double2(acc[2 * i], acc[2 * i + 1]);
       }
     }
   }
@@ -370,6 +334,48 @@ __global__ void __launch_bounds__(256) k_prep_inverse_bf16(
   }
 }
 
+// Forward: order-major result rows R[m][q][l - l0] (pitch thetaPad) added
+// into the packed coefficients, with the -m rows' factor (-1)^(l+n) and the
+// c_{L,L} = 0 rule of complex fields (GaussLegendreGrid.h:209-215). One block
+// per 32 degrees x 32 orders of one row q: rows are read degree-contiguous,
+// transposed in shared memory, and the packed layout (order-contiguous for a
+// fixed degree) is read-modify-written coalesced.
+__global__ void __launch_bounds__(256) k_accumulate_forward(
+    int L, int lmax, int n, int na, int count, int Q, int isReal, long coefSize, int pitch,
+    const double2* __restrict__ rows, double2* __restrict__ coef) {
+  __shared__ double2 tile[32][33];
+  const int lt = blockIdx.x * 32, mt = blockIdx.y * 32, q = blockIdx.z;
+  if (mt > lt + 31 || mt > lmax) return;
+  const int sgn = q / count, f = q - sgn * count;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int i = warp; i < 32; i += 8) {
+    const int m = mt + i, l = lt + lane;
+    const int l0 = m > na ? m : na;
+    double2 v = make_double2(0.0, 0.0);
+    if (m <= lmax && l <= lmax && l >= l0)
+      v = rows[((size_t)m * Q + q) * pitch + (l - l0)];
+    tile[i][lane] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = warp; i < 32; i += 8) {
+    const int l = lt + i, m = mt + lane;
+    if (l > lmax || l < na || m > l || m > lmax || (sgn == 1 && m == 0)) continue;
+    const long idx = isReal ? (long)l * (l + 1) / 2 - (long)na * (na + 1) / 2 + m
+                            : (long)l * l - (long)n * n + l + (sgn ? -m : m);
+    double2* ptr = coef + (size_t)f * coefSize + idx;
+    double2 v = tile[lane][i];
+    if (sgn == 1 && ((l + n) & 1)) v = make_double2(-v.x, -v.y);
+    if (!isReal && sgn == 0 && m == L && l == L && lmax == L) {
+      *ptr = make_double2(0.0, 0.0);
+    } else {
+      const double2 o = *ptr;
+      *ptr = make_double2(o.x + v.x, o.y + v.y);
+    }
+  }
+}
+
 // Forward: weighted spectra (FP64) -> B[split][m*R + 2q + part][j].
 __global__ void k_prep_forward_bf16(int lmax, int Q, int R, int thetaPad, size_t plane,
                                     const double2* __restrict__ spec,
@@ -412,28 +418,42 @@ gsht_status make_map_bf16(CUtensorMap* map, const void* base, uint64_t inner, ui
   return GSHT_OK;
 }
 
-constexpr int kNsplit = 3, kNprod = 6, kNTile = 128;
+constexpr int kNsplit = 3, kNprod = 6;
 
-template <int kDir>
-gsht_status launch_bf16(const gsht_grid* g, const Table* t, const TcArgs& a,
-                        const CUtensorMap& mapA, const CUtensorMap& mapB, cudaStream_t s) {
+template <int kDir, int kN>
+gsht_status launch_bf16_n(const gsht_grid* g, const TcArgs& a, const CUtensorMap& mapA,
+                          const CUtensorMap& mapB, cudaStream_t s) {
   gsht_status st;
-  const TileList* tl =
-      tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kNTile, bk_of(kDir), &st);
-  if (!tl) return st;
-  auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kNTile, stages_of(kDir)>;
-  const size_t sm = tc_smem_bytes<kNsplit, kNsplit, kNTile, bk_of(kDir), stages_of(kDir)>();
-  GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+  const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kN, bk_of(kDir), &st);
+  if (!tl) return st;
+  auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kN, stages_of(kDir)>;
+  const size_t sm = tc_smem_bytes<kNsplit, kNsplit, kN, bk_of(kDir), stages_of(kDir)>();
+  GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int blocks = tl->count < sms ? tl->count : sms;
   kern<<<blocks, kThreads, sm, s>>>(mapA, mapB, a, tl->d_tiles, tl->count);
   GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_tc<inverse,bf16x3>" : "k_legendre_tc<forward,bf16x3>");
   return GSHT_OK;
 }
 
+// Field-row tile width N of the BF16x3 kernels: 128 by default; 64 and 32
+// waste fewer MMA columns on small batches (chosen by the batch autotuner).
+bool valid_ntile(int ntile) { return ntile == 32 || ntile == 64 || ntile == 128; }
+
+template <int kDir>
+gsht_status launch_bf16(const gsht_grid* g, int ntile, const TcArgs& a, const CUtensorMap& mapA,
+                        const CUtensorMap& mapB, cudaStream_t s) {
+  if (ntile == 32) return launch_bf16_n<kDir, 32>(g, a, mapA, mapB, s);
+  if (ntile == 64) return launch_bf16_n<kDir, 64>(g, a, mapA, mapB, s);
+  return launch_bf16_n<kDir, 128>(g, a, mapA, mapB, s);
+}
+
 }  // namespace
 
+// Tiles (m, M tile, N tile, K blocks), N tiles innermost: neighbouring
+// blocks of the persistent grid work on the same table tile at the same
+// time, so it comes from DRAM once and from L2 for the others.
 const TileList* tile_list(const gsht_grid* g, int dir, int lmax, int na, int rows, int ntile,
                           int kstep, gsht_status* st) {
   *st = GSHT_OK;
@@ -475,7 +495,8 @@ size_t bf16_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, 
 
 gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
                                   int count, const double* coef, void* operand, double* spec,
-                                  cudaStream_t s) {
+                                  int ntile, cudaStream_t s) {
+  if (!valid_ntile(ntile)) return fail(GSHT_ERR_BAD_ARG, "BF16x3 tile width %d not in {32, 64, 128}", ntile);
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
   const int pitch = (int)round_up(lmax + 1, kBKInv);
@@ -494,7 +515,7 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
   gsht_status st = make_map_bf16(&mapA, t->tbf, g->theta_pad, t->rows + kTablePadRows, 3,
                                  g->theta_pad, tplane, 64, kBKInv, CU_TENSOR_MAP_SWIZZLE_128B);
   if (st != GSHT_OK) return st;
-  st = make_map_bf16(&mapB, op, pitch, (uint64_t)(lmax + 1) * R, 3, pitch, plane, kBKInv, kNTile,
+  st = make_map_bf16(&mapB, op, pitch, (uint64_t)(lmax + 1) * R, 3, pitch, plane, kBKInv, ntile,
                      CU_TENSOR_MAP_SWIZZLE_64B);
   if (st != GSHT_OK) return st;
   TcArgs a{};
@@ -503,12 +524,13 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
   a.rowOff = t->d_row_off; a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
-  return launch_bf16<0>(g, t, a, mapA, mapB, s);
+  return launch_bf16<0>(g, ntile, a, mapA, mapB, s);
 }
 
 gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
-                                  int count, const double* spec, void* operand, double* coef,
-                                  cudaStream_t s) {
+                                  int count, double* spec, void* operand, double* coef,
+                                  int ntile, cudaStream_t s) {
+  if (!valid_ntile(ntile)) return fail(GSHT_ERR_BAD_ARG, "BF16x3 tile width %d not in {32, 64, 128}", ntile);
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
   const int tp = g->theta_pad;
@@ -526,16 +548,25 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
   gsht_status st = make_map_bf16(&mapA, t->tbf, tp, t->rows + kTablePadRows, 3, tp, tplane,
                                  bk_of(1), kBM, CU_TENSOR_MAP_SWIZZLE_128B);
   if (st != GSHT_OK) return st;
-  st = make_map_bf16(&mapB, op, tp, (uint64_t)(lmax + 1) * R, 3, tp, plane, bk_of(1), kNTile,
+  st = make_map_bf16(&mapB, op, tp, (uint64_t)(lmax + 1) * R, 3, tp, plane, bk_of(1), ntile,
                      CU_TENSOR_MAP_SWIZZLE_128B);
   if (st != GSHT_OK) return st;
   TcArgs a{};
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count; a.Q = Q; a.R = R;
   a.nTheta = g->n_theta; a.thetaPad = tp; a.isReal = is_real;
-  a.rowOff = t->d_row_off; a.out = reinterpret_cast<double2*>(coef);
+  // The spectra are consumed (split into the BF16 planes) by now: their
+  // buffer holds the kernel's order-major result rows (keff <= thetaPad).
+  a.rowOff = t->d_row_off; a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
-  return launch_bf16<1>(g, t, a, mapA, mapB, s);
+  st = launch_bf16<1>(g, ntile, a, mapA, mapB, s);
+  if (st != GSHT_OK) return st;
+  dim3 ag((lmax + 32) / 32, (lmax + 32) / 32, Q);
+  k_accumulate_forward<<<ag, 256, 0, s>>>(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize,
+                                          tp, reinterpret_cast<const double2*>(spec),
+                                          reinterpret_cast<double2*>(coef));
+  GSHT_LAUNCH_CHECK("k_accumulate_forward");
+  return GSHT_OK;
 }
 
 }  // namespace gsht
