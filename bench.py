@@ -54,6 +54,12 @@ def parse():
     p.add_argument("--lmax", type=int, default=L_MAX)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", default="headline",
+                   choices=["headline", "batch", "large", "pipeline"],
+                   help="headline: 64 fields at lmax 1024 (the metric); batch: 256 fields of "
+                        "uneven lmax in one CUDA graph vs per-field calls; large: one field at "
+                        "lmax 2048 (table streaming, GB/s); pipeline: 64 field-product pairs at "
+                        "lmax 768")
     return p.parse_args()
 
 
@@ -70,10 +76,10 @@ def workload(args):
 
 
 def coefficients(lmax, fields, seed=0):
-    import oracle
+    import gshtrans_b200 as gsht
 
     rng = np.random.default_rng(seed)
-    return np.stack([oracle.random_coefficients(rng, lmax, lmax, N_UPPER, False, ENVELOPE)
+    return np.stack([gsht.random_coefficients(rng, lmax, lmax, N_UPPER, False, ENVELOPE)
                      for _ in range(fields)])
 
 
@@ -157,6 +163,10 @@ def reference_run(lmax, steps, warmup, log=None):
         out = g.roundtrip_batch(lmax, N_UPPER, False, coefs, cores)
     dt = time.perf_counter() - t0
     err = float(np.linalg.norm(out - coefs) / np.linalg.norm(coefs))
+    # the reference's own transform is serial: one field on one core
+    t1 = time.perf_counter()
+    g.roundtrip_batch(lmax, N_UPPER, False, coefs[:1], 1)
+    single_s = time.perf_counter() - t1
     g.close()
     value = steps * cores / dt
     return {
@@ -165,6 +175,7 @@ def reference_run(lmax, steps, warmup, log=None):
                    f"inverse+forward each, reference GaussLegendreGrid.h compiled in place "
                    f"(FFTWpp/GaussQuad stand-ins); table build {build_s:.1f} s untimed"),
         "seconds": dt, "round_trip_rel_err": err,
+        "single_core_value": 1.0 / single_s,
     }, None
 
 
@@ -182,7 +193,8 @@ def impl_reference(args):
         "ms_per_step": 1000.0 * res["seconds"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload(args) | {"fields_per_step": res["cores"]},
-        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                             "single_core_value")},
         "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "round_trip_rel_err": res["round_trip_rel_err"],
     }
@@ -371,7 +383,8 @@ def impl_ours(args):
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             rr, why = reference_run(L, 1, 0)
-            cpu = ({k: rr[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            cpu = ({k: rr[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                       "single_core_value")}
                    if rr else {"value": None, "unavailable": why})
         mode_lines = {}
         for m in modes:
@@ -434,10 +447,222 @@ def e2e_run(gsht, grid, torch, coef_h, precision, args):
                     "the forward output is uploaded because the forward accumulates into it"}
 
 
+# ---------------------------------------------------------------------------
+# Further workloads (reported lines; the headline metric is the default run)
+# ---------------------------------------------------------------------------
+def _event_time(torch, fn, steps, warmup):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def impl_batch(args):
+    """256 fields, lmax uniform in {32, 64, 128, 256, 512}, upper index uniform
+    in -2..2, half real; envelope 1/(l+1); each on its own grid. One round
+    trip (inverse then forward) of all fields per step: one CUDA graph launch
+    of the autotuned batch plan, against per-field single calls."""
+    import torch
+    import gshtrans_b200 as gsht
+
+    prec = args.precision or "bf16x3"
+    rng = np.random.default_rng(2024)
+    fields, host = [], []
+    for i in range(256):
+        lmax = int(rng.choice([32, 64, 128, 256, 512]))
+        n = int(rng.integers(-2, 3))
+        is_real = i % 2 == 1
+        c = gsht.random_coefficients(rng, lmax, lmax, n, is_real, 1.0)
+        cin = torch.from_numpy(c).cuda()
+        npts = (lmax + 1) * 2 * lmax
+        grid = torch.zeros(npts, dtype=torch.float64 if is_real else torch.complex128, device="cuda")
+        fields.append((lmax, n, is_real, cin, grid, torch.zeros_like(cin)))
+        host.append(c)
+    t0 = time.perf_counter()
+    batch = gsht.Batch(fields, precision=prec, autotune=True)
+    plan_s = time.perf_counter() - t0
+    groups, grids, nodes = batch.info()
+    ms_graph = _event_time(torch, batch.round_trip, args.steps, args.warmup)
+    # per-field single calls on grids built once per degree
+    forms = () if prec == "fp64" else (prec,)
+    gridobj = {L: gsht.GaussLegendreGrid(L, 2, forms=forms) for L in sorted({f[0] for f in fields})}
+
+    def per_field():
+        for lmax, n, is_real, cin, grid, cout in fields:
+            g = gridobj[lmax]
+            g.InverseTransformation(lmax, n, cin, grid, prec)
+            g.ForwardTransformation(lmax, n, grid, cout, prec)
+
+    ms_single = _event_time(torch, per_field, max(1, args.steps // 2), 1)
+    # accuracy of one round trip against the FP64 batch
+    err = None
+    if prec != "fp64":
+        outs = [torch.zeros_like(f[5]) for f in fields]
+        b2 = gsht.Batch([f[:5] + (o,) for f, o in zip(fields, outs)], precision=prec, autotune=True)
+        b2.round_trip()
+        outs64 = [torch.zeros_like(f[5]) for f in fields]
+        b3 = gsht.Batch([f[:5] + (o,) for f, o in zip(fields, outs64)], precision="fp64", autotune=False)
+        b3.round_trip()
+        torch.cuda.synchronize()
+        num = sum(float(torch.linalg.norm(a - b) ** 2) for a, b in zip(outs, outs64))
+        den = sum(float(torch.linalg.norm(b) ** 2) for b in outs64)
+        err = (num / den) ** 0.5
+        b2.close()
+        b3.close()
+    for g in gridobj.values():
+        g.close()
+    tiles = {}
+    for lm, n, re, cnt, tile in batch.groups():
+        tiles[tile] = tiles.get(tile, 0) + 1
+    print(json.dumps({
+        "metric": "batched uneven fields, fwd+inv/s (one CUDA graph per step)",
+        "value": 256 / (ms_graph * 1e-3), "unit": UNIT, "ms_per_step": ms_graph,
+        "per_field_calls": {"value": 256 / (ms_single * 1e-3), "ms_per_step": ms_single},
+        "speedup_vs_per_field_calls": ms_single / ms_graph,
+        "precision": prec, "round_trip_rel_err_vs_fp64": err,
+        "groups": groups, "grids": grids, "graph_nodes_round_trip": nodes[2],
+        "autotuned_tile_widths": tiles, "plan_seconds": plan_s,
+        "config": {"workload": "256 fields, lmax in {32,64,128,256,512}, n in -2..2, half real, "
+                               "envelope (l+1)^-1, own grid per field", "steps": args.steps,
+                   "warmup": args.warmup},
+    }))
+    batch.close()
+    return 0
+
+
+def table_rows(L, n):
+    na = abs(n)
+    return sum(L + 1 - max(m, na) for m in range(L + 1))
+
+
+def impl_large(args):
+    """One complex field at lmax 2048 (nTheta 2049, nPhi 4096), n = 1,
+    envelope (l+1)^-2: table streaming, reported in GB/s of the stored table
+    form read per transform."""
+    import torch
+    import gshtrans_b200 as gsht
+
+    L, n = 2048, 1
+    rng = np.random.default_rng(2048)
+    c_h = gsht.random_coefficients(rng, L, L, n, False, 2.0)
+    t0 = time.perf_counter()
+    grid = gsht.GaussLegendreGrid(L, n, nrange=gsht.Single, forms=("ozaki",))
+    build_s = time.perf_counter() - t0
+    coef = torch.from_numpy(c_h).cuda()
+    field = torch.empty(grid.FieldSize(), dtype=torch.complex128, device="cuda")
+    out = torch.zeros_like(coef)
+    tp = (L + 1 + 15) // 16 * 16
+    rows = table_rows(L, n)
+    hbm = None
+    mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(mp):
+        hbm = json.load(open(mp)).get("hbm_gbs")
+    res = {}
+    ref = {}
+    for prec, bytes_per in (("fp64", 8), ("ozaki", 7)):
+        table_bytes = rows * tp * bytes_per
+        ms_inv = _event_time(torch, lambda: grid.InverseTransformation(L, n, coef, field, prec),
+                             args.steps, args.warmup)
+        ms_fwd = _event_time(torch, lambda: grid.ForwardTransformation(L, n, field, out, prec),
+                             args.steps, args.warmup)
+        f = torch.empty_like(field)
+        grid.InverseTransformation(L, n, coef, f, prec)
+        c = torch.zeros_like(coef)
+        grid.ForwardTransformation(L, n, f, c, prec)
+        torch.cuda.synchronize()
+        ref[prec] = (f, c)
+        res[prec] = {"inverse_ms": ms_inv, "forward_ms": ms_fwd,
+                     "table_bytes": table_bytes,
+                     "inverse_table_GBps": table_bytes / (ms_inv * 1e-3) / 1e9,
+                     "forward_table_GBps": table_bytes / (ms_fwd * 1e-3) / 1e9,
+                     "round_trip_rel_err": float(torch.linalg.norm(c - coef) / torch.linalg.norm(coef))}
+        if hbm:
+            res[prec]["frac_of_measured_hbm"] = max(res[prec]["inverse_table_GBps"],
+                                                    res[prec]["forward_table_GBps"]) / hbm
+    f64, c64 = ref["fp64"]
+    foz, coz = ref["ozaki"]
+    res["ozaki"]["inverse_rel_err_vs_fp64"] = float(torch.linalg.norm(foz - f64) / torch.linalg.norm(f64))
+    res["ozaki"]["forward_rel_err_vs_fp64"] = float(torch.linalg.norm(coz - c64) / torch.linalg.norm(c64))
+    print(json.dumps({
+        "metric": "lmax 2048 single field: table streaming GB/s", "unit": "GB/s",
+        "value": res["fp64"]["inverse_table_GBps"], "modes": res, "hbm_peak_GBps": hbm,
+        "grid_build_seconds": build_s,
+        "config": {"workload": "1 complex field, lmax 2048 (nTheta 2049, nPhi 4096), n=1, "
+                               "envelope (l+1)^-2", "table_rows": rows, "theta_pad": tp},
+    }))
+    grid.close()
+    return 0
+
+
+def impl_pipeline(args):
+    """64 pairs (u: n = +1, v: n = -1) at lmax 768 (nPhi 1536 = 2^9 x 3):
+    inverse both, w = u v + conj(u) u (the conjugate taken with upper index
+    -1, so both terms have n = 0) fused in one kernel, forward w."""
+    import torch
+    import gshtrans_b200 as gsht
+    from gshtrans_b200 import fields as F
+
+    L, B = 768, 64
+    rng = np.random.default_rng(768)
+    U = torch.from_numpy(np.stack([gsht.random_coefficients(rng, L, L, 1, False, 1.5)
+                                   for _ in range(B)])).cuda()
+    V = torch.from_numpy(np.stack([gsht.random_coefficients(rng, L, L, -1, False, 1.5)
+                                   for _ in range(B)])).cuda()
+    grid = gsht.GaussLegendreGrid(L, 1, forms=("bf16x3", "ozaki"))
+    fs = grid.FieldSize()
+    Fu = torch.empty((B, fs), dtype=torch.complex128, device="cuda")
+    Fv = torch.empty_like(Fu)
+    W = torch.empty_like(Fu)
+    Cw = torch.zeros((B, gsht.coefficient_size(L, 0, False)), dtype=torch.complex128, device="cuda")
+    u = F.Field(grid, 1, count=B, data=Fu)
+    v = F.Field(grid, -1, count=B, data=Fv)
+    w = F.Field(grid, 0, count=B, data=W)
+    expr = u * v + F.conj(u, upper_index=-1) * u
+    out = {}
+    for prec in ("fp64", "bf16x3", "ozaki"):
+        def step():
+            grid.inverse_batch(L, 1, U, Fu, prec)
+            grid.inverse_batch(L, -1, V, Fv, prec)
+            w.assign(expr)
+            Cw.zero_()
+            grid.forward_batch(L, 0, W, Cw, prec)
+
+        ms = _event_time(torch, step, args.steps, args.warmup)
+        step()
+        torch.cuda.synchronize()
+        out[prec] = {"ms_per_step": ms, "pairs_per_s": B / (ms * 1e-3), "result": Cw.clone()}
+    ref = out["fp64"]["result"]
+    for prec in out:
+        out[prec]["rel_err_vs_fp64"] = float(torch.linalg.norm(out[prec]["result"] - ref) / torch.linalg.norm(ref))
+        del out[prec]["result"]
+    for prec in out:
+        out[prec]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out[prec]["ms_per_step"]
+    print(json.dumps({
+        "metric": "field-product pipeline pairs/s (2 inverses, fused u*v + conj(u)*u, 1 forward)",
+        "unit": "pairs/s", "value": out["ozaki"]["pairs_per_s"], "modes": out,
+        "config": {"workload": "64 pairs, lmax 768 (nTheta 769, nPhi 1536), u n=+1, v n=-1, "
+                               "envelope (l+1)^-1.5", "steps": args.steps, "warmup": args.warmup},
+    }))
+    grid.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return impl_reference(args)
+    if args.workload == "batch":
+        return impl_batch(args)
+    if args.workload == "large":
+        return impl_large(args)
+    if args.workload == "pipeline":
+        return impl_pipeline(args)
     return impl_ours(args)
 
 

@@ -23,7 +23,7 @@ import numpy as np
 __all__ = [
     "All", "NonNegative", "Single", "FP64", "BF16X3", "OZAKI",
     "GaussLegendreGrid", "GSHTError", "BadArgument", "library", "launch_count",
-    "coefficient_size", "wigner",
+    "coefficient_size", "wigner", "Batch", "random_coefficients", "degree_order",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -109,6 +109,39 @@ def wigner(lmax: int, mmax: int, nmax: int, theta, mrange: int = All, nrange: in
     out = np.zeros(cnt.value)
     _check(library.gsht_wigner_compute(*args, out.ctypes.data_as(dp), ctypes.byref(cnt)))
     return out
+
+
+def degree_order(lmax: int, n: int, is_real: bool):
+    """Degree and order of every slot of the packed layout, GSHIndices<All>
+    (complex) or GSHIndices<NonNegative> (real) (Indexing.h:104-131)."""
+    ls = np.arange(abs(n), lmax + 1)
+    width = ls + 1 if is_real else 2 * ls + 1
+    l_of = np.repeat(ls, width)
+    start = np.repeat(np.cumsum(width) - width, width)
+    pos = np.arange(l_of.size) - start
+    m_of = pos if is_real else pos - l_of
+    return l_of, m_of
+
+
+def random_coefficients(rng, grid_lmax: int, lmax: int, n: int, is_real: bool,
+                        envelope=None) -> np.ndarray:
+    """GridBase::RandomComplexCoefficient / RandomRealCoefficient
+    (GridBase.h:124-172) from a NumPy generator: N(0,1) + i N(0,1) per slot
+    (real parts drawn first), times (l+1)^-envelope if given; complex fields
+    get c_{L,L} = 0 and real fields Im c_{l,0} = 0 and Im c_{L,L} = 0 when
+    lmax equals the grid degree L."""
+    size = coefficient_size(lmax, n, is_real)
+    c = rng.standard_normal(size) + 1j * rng.standard_normal(size)
+    ls, ms = degree_order(lmax, n, is_real)
+    if envelope is not None:
+        c = c * (ls + 1.0) ** (-float(envelope))
+    if is_real:
+        c[ms == 0] = c[ms == 0].real
+        if lmax == grid_lmax:
+            c[-1] = c[-1].real
+    elif lmax == grid_lmax:
+        c[-1] = 0
+    return c
 
 
 def coefficient_size(lmax: int, n: int, is_real: bool) -> int:
@@ -311,4 +344,94 @@ class GaussLegendreGrid:
         _check(fn(self._h, lmax, n, int(is_real), _precision(precision), count,
                   ctypes.c_void_p(pin), ctypes.c_void_p(pout),
                   ctypes.c_void_p(stream) if stream else None))
+        return out
+
+
+class _FieldDesc(ctypes.Structure):
+    _fields_ = [("lmax", ctypes.c_int), ("n", ctypes.c_int), ("is_real", ctypes.c_int),
+                ("coef_in", ctypes.c_void_p), ("grid", ctypes.c_void_p),
+                ("coef_out", ctypes.c_void_p)]
+
+
+library.gsht_plan_batch.argtypes = [ctypes.POINTER(_FieldDesc), ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+library.gsht_batch_execute.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+library.gsht_batch_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_long)]
+library.gsht_batch_group.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.POINTER(ctypes.c_int)] * 5
+library.gsht_batch_destroy.argtypes = [ctypes.c_void_p]
+
+BATCH_FORWARD, BATCH_INVERSE, BATCH_ROUND_TRIP = 0, 1, 2
+
+
+class Batch:
+    """Many fields of uneven lmax / upper index / kind, transformed by one CUDA
+    graph launch per call (``gsht_plan_batch``; no reference counterpart: the
+    reference transforms one field per call, GaussLegendreGrid.h:108-321).
+
+    ``fields`` is a list of ``(lmax, n, is_real, coef_in, grid, coef_out)``
+    with CUDA tensors in the layouts of the single-field transforms (each
+    field on its own grid, nTheta = lmax + 1, nPhi = 2 lmax). ``inverse()``
+    writes the grids from ``coef_in``; ``forward()`` adds the grids'
+    coefficients into ``coef_out``; ``round_trip()`` does both. The tensors
+    must stay alive (and in place) for the life of the plan.
+    """
+
+    def __init__(self, fields, precision="bf16x3", autotune=True):
+        descs = []
+        self._keep = []
+        for lmax, n, is_real, cin, grid, cout in fields:
+            for t in (cin, grid, cout):
+                if not getattr(t, "is_cuda", False):
+                    raise BadArgument(1, "batch buffers must be CUDA tensors")
+                self._keep.append(t)
+            descs.append(_FieldDesc(int(lmax), int(n), int(bool(is_real)), cin.data_ptr(),
+                                    grid.data_ptr(), cout.data_ptr()))
+        arr = (_FieldDesc * len(descs))(*descs)
+        h = ctypes.c_void_p()
+        _check(library.gsht_plan_batch(arr, len(descs), _precision(precision), int(bool(autotune)),
+                                       ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library.gsht_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover
+            pass
+
+    def _run(self, mode):
+        import torch
+
+        _check(library.gsht_batch_execute(self._h, mode,
+                                          ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+
+    def forward(self):
+        self._run(BATCH_FORWARD)
+
+    def inverse(self):
+        self._run(BATCH_INVERSE)
+
+    def round_trip(self):
+        self._run(BATCH_ROUND_TRIP)
+
+    def info(self):
+        """(groups, grids, graph nodes per mode [forward, inverse, round trip])."""
+        g, d = ctypes.c_int(), ctypes.c_int()
+        nodes = (ctypes.c_long * 3)()
+        _check(library.gsht_batch_info(self._h, ctypes.byref(g), ctypes.byref(d), nodes))
+        return g.value, d.value, list(nodes)
+
+    def groups(self):
+        """[(lmax, n, is_real, count, tile width)] per group."""
+        g, _, _ = self.info()
+        out = []
+        for i in range(g):
+            v = [ctypes.c_int() for _ in range(5)]
+            _check(library.gsht_batch_group(self._h, i, *[ctypes.byref(x) for x in v]))
+            out.append(tuple(x.value for x in v))
         return out

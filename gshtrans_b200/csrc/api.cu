@@ -43,6 +43,11 @@ std::vector<ProfRecord> g_prof;
 StageTimer::StageTimer(int stage, cudaStream_t s) : stage_(stage), s_(s) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   if (!g_prof_on) return;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return;  // graph capture: stage timing is for direct calls only
+  }
   if (cudaEventCreate(&a_) != cudaSuccess || cudaEventCreate(&b_) != cudaSuccess) {
     cudaGetLastError();
     a_ = b_ = nullptr;

@@ -1,0 +1,379 @@
+// Batched transforms of many fields of uneven sizes in one CUDA graph.
+//
+// No counterpart in the reference, whose transforms take one field per call
+// (GaussLegendreGrid.h:108-321); a caller with many fields loops over them.
+// Here a plan takes a list of fields, each with its own degree lmax (and so
+// its own Gauss-Legendre grid nTheta = lmax + 1, nPhi = 2 lmax), upper index
+// and kind, and
+//   - groups them by (lmax, n, real/complex): one grid per distinct lmax,
+//     whose Wigner tables (one per upper index) every field of that degree
+//     shares, and one batched transform per group (each stage runs once over
+//     the group and reads the table once);
+//   - gathers each group's inputs from the callers' buffers into contiguous
+//     batch buffers and scatters the results back (the forward adds into the
+//     callers' coefficients, as ForwardTransformation does);
+//   - autotunes, for the BF16x3 form, the field-row tile width of the
+//     tensor-core kernels per group (32, 64 or 128 columns: small groups
+//     waste fewer MMA columns with narrow tiles) by timing each candidate;
+//   - captures the whole sequence (gathers, transforms, scatters) for each
+//     direction into a CUDA graph, so an execution is one graph launch.
+#include <algorithm>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "gsht_internal.cuh"
+
+namespace gsht {
+namespace {
+
+// Copies `count` vectors of `elems` 16-byte elements between callers'
+// buffers and a contiguous batch buffer; mode 0: gather (dst contiguous),
+// 1: scatter (src contiguous), 2: scatter-add (src contiguous, dst += src),
+// 3: scatter-add with the last element set to 0 (the c_{L,L} = 0 rule the
+// forward applies to complex fields whose lmax is the grid degree,
+// GaussLegendreGrid.h:209-215; it overwrites rather than adds). For real
+// grids elems counts pairs of doubles (fields are nTheta*nPhi doubles; nPhi
+// is even).
+__global__ void k_batch_copy(int mode, long elems, double2* const* ptrs, double2* contiguous) {
+  const int f = blockIdx.y;
+  double2* user = ptrs[f];
+  double2* flat = contiguous + (size_t)f * elems;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < elems;
+       i += (long)gridDim.x * blockDim.x) {
+    if (mode == 0) {
+      flat[i] = user[i];
+    } else if (mode == 1) {
+      user[i] = flat[i];
+    } else if (mode == 3 && i == elems - 1) {
+      user[i] = make_double2(0.0, 0.0);
+    } else {
+      const double2 a = user[i], b = flat[i];
+      user[i] = make_double2(a.x + b.x, a.y + b.y);
+    }
+  }
+}
+
+struct Group {
+  int lmax = 0, n = 0, isReal = 0, ntile = 128;
+  std::vector<int> fields;
+  gsht_grid* grid = nullptr;
+  long coefElems = 0, gridElems = 0;  // 16-byte elements per field
+  double2* coefIn = nullptr;          // contiguous batch buffers
+  double2* gridBuf = nullptr;
+  double2* coefOut = nullptr;
+  double2** coefInPtrs = nullptr;     // callers' pointers (device arrays)
+  double2** gridPtrs = nullptr;
+  double2** coefOutPtrs = nullptr;
+};
+
+}  // namespace
+}  // namespace gsht
+
+struct gsht_batch {
+  int device = 0, precision = 0;
+  std::vector<gsht_field_desc> fields;
+  std::map<int, gsht_grid*> grids;  // by degree
+  std::vector<gsht::Group> groups;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph[3] = {nullptr, nullptr, nullptr};
+  cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+  size_t nodes[3] = {0, 0, 0};
+};
+
+namespace gsht {
+namespace {
+
+gsht_status copy_group(const Group& gr, int mode, long elems, double2** ptrs, double2* flat,
+                       cudaStream_t s) {
+  const int count = (int)gr.fields.size();
+  long blocks = (elems + 255) / 256;
+  blocks = blocks > 1184 ? 1184 : blocks;
+  dim3 grid((unsigned)blocks, count);
+  k_batch_copy<<<grid, 256, 0, s>>>(mode, elems, ptrs, flat);
+  GSHT_LAUNCH_CHECK("k_batch_copy");
+  return GSHT_OK;
+}
+
+// One direction for one group: 0 forward (grids -> coefficients, added into
+// the callers' coefficients), 1 inverse (coefficients -> grids).
+// `gather`/`scatter` select whether the callers' buffers are read/written.
+gsht_status run_group(gsht_batch* b, Group& gr, int dir, bool gather, bool scatter, cudaStream_t s) {
+  const int count = (int)gr.fields.size();
+  gsht_status st;
+  if (dir == 1) {
+    if (gather && (st = copy_group(gr, 0, gr.coefElems, gr.coefInPtrs, gr.coefIn, s)) != GSHT_OK)
+      return st;
+    st = transform(gr.grid, 1, gr.lmax, gr.n, gr.isReal, b->precision, count, gr.coefIn,
+                   gr.gridBuf, s, gr.ntile);
+    if (st != GSHT_OK) return st;
+    if (scatter && (st = copy_group(gr, 1, gr.gridElems, gr.gridPtrs, gr.gridBuf, s)) != GSHT_OK)
+      return st;
+  } else {
+    if (gather && (st = copy_group(gr, 0, gr.gridElems, gr.gridPtrs, gr.gridBuf, s)) != GSHT_OK)
+      return st;
+    GSHT_CUDA(cudaMemsetAsync(gr.coefOut, 0, sizeof(double2) * gr.coefElems * count, s));
+    st = transform(gr.grid, 0, gr.lmax, gr.n, gr.isReal, b->precision, count, gr.gridBuf,
+                   gr.coefOut, s, gr.ntile);
+    if (st != GSHT_OK) return st;
+    // Every field's lmax is its grid's degree, so complex fields get c_{L,L} = 0.
+    const int mode = gr.isReal ? 2 : 3;
+    if (scatter && (st = copy_group(gr, mode, gr.coefElems, gr.coefOutPtrs, gr.coefOut, s)) != GSHT_OK)
+      return st;
+  }
+  return GSHT_OK;
+}
+
+// Everything one execution of `mode` does (0 forward, 1 inverse, 2 inverse
+// then forward, the grids of the round trip also written back).
+gsht_status run_all(gsht_batch* b, int mode, cudaStream_t s) {
+  gsht_status st;
+  for (auto& gr : b->groups) {
+    if (mode == 2) {
+      if ((st = run_group(b, gr, 1, true, true, s)) != GSHT_OK) return st;
+      if ((st = run_group(b, gr, 0, false, true, s)) != GSHT_OK) return st;
+    } else if ((st = run_group(b, gr, mode, true, true, s)) != GSHT_OK) {
+      return st;
+    }
+  }
+  return GSHT_OK;
+}
+
+void free_batch(gsht_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (int i = 0; i < 3; i++) {
+    if (b->exec[i]) cudaGraphExecDestroy(b->exec[i]);
+    if (b->graph[i]) cudaGraphDestroy(b->graph[i]);
+  }
+  for (auto& gr : b->groups) {
+    cudaFree(gr.coefIn);
+    cudaFree(gr.gridBuf);
+    cudaFree(gr.coefOut);
+    cudaFree(gr.coefInPtrs);
+    cudaFree(gr.gridPtrs);
+    cudaFree(gr.coefOutPtrs);
+  }
+  for (auto& kv : b->grids) gsht_grid_destroy(kv.second);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+gsht_status upload_ptrs(double2*** dst, const std::vector<const void*>& host) {
+  GSHT_CUDA(cudaMalloc(dst, sizeof(double2*) * host.size()));
+  GSHT_CUDA(cudaMemcpy(*dst, host.data(), sizeof(double2*) * host.size(), cudaMemcpyHostToDevice));
+  return GSHT_OK;
+}
+
+bool on_device(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Times one round trip of a group (after a warm-up) on the plan's stream.
+gsht_status time_group(gsht_batch* b, Group& gr, float* ms) {
+  cudaEvent_t e0, e1;
+  GSHT_CUDA(cudaEventCreate(&e0));
+  GSHT_CUDA(cudaEventCreate(&e1));
+  gsht_status st = GSHT_OK;
+  for (int rep = 0; rep < 3 && st == GSHT_OK; rep++) {
+    if (rep == 1) cudaEventRecord(e0, b->stream);
+    st = run_group(b, gr, 1, false, false, b->stream);
+    if (st == GSHT_OK) st = run_group(b, gr, 0, false, false, b->stream);
+  }
+  cudaEventRecord(e1, b->stream);
+  cudaEventSynchronize(e1);
+  cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
+}
+
+gsht_status plan(const gsht_field_desc* fields, int count, int precision, int autotune,
+                 gsht_batch* b) {
+  b->precision = precision;
+  b->fields.assign(fields, fields + count);
+  GSHT_CUDA(cudaGetDevice(&b->device));
+  GSHT_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  // Groups by (lmax, n, kind); grids by lmax with the widest upper index.
+  std::map<std::tuple<int, int, int>, int> index;
+  std::map<int, int> nmax;
+  for (int i = 0; i < count; i++) {
+    const auto& f = fields[i];
+    const auto key = std::make_tuple(f.lmax, f.n, f.is_real ? 1 : 0);
+    auto it = index.find(key);
+    if (it == index.end()) {
+      Group gr;
+      gr.lmax = f.lmax;
+      gr.n = f.n;
+      gr.isReal = f.is_real ? 1 : 0;
+      it = index.emplace(key, (int)b->groups.size()).first;
+      b->groups.push_back(gr);
+    }
+    b->groups[it->second].fields.push_back(i);
+    const int na = f.n < 0 ? -f.n : f.n;
+    nmax[f.lmax] = std::max(nmax[f.lmax], na);
+  }
+  const unsigned forms = GSHT_FORM_FP64 | (precision == GSHT_BF16X3 ? GSHT_FORM_BF16X3 : 0u) |
+                         (precision == GSHT_OZAKI ? GSHT_FORM_OZAKI : 0u);
+  for (auto& kv : nmax) {
+    gsht_grid* g = nullptr;
+    gsht_status st = gsht_grid_create(kv.first, kv.second, GSHT_RANGE_ALL, GSHT_RANGE_ALL, forms, &g);
+    if (st != GSHT_OK) return st;
+    b->grids[kv.first] = g;
+  }
+  for (auto& gr : b->groups) {
+    gr.grid = b->grids[gr.lmax];
+    const int k = (int)gr.fields.size();
+    gr.coefElems = coef_size(gr.lmax, gr.n, gr.isReal);
+    const long points = (long)(gr.lmax + 1) * 2 * gr.lmax;
+    gr.gridElems = gr.isReal ? points / 2 : points;
+    GSHT_CUDA(cudaMalloc(&gr.coefIn, sizeof(double2) * gr.coefElems * k));
+    GSHT_CUDA(cudaMalloc(&gr.gridBuf, sizeof(double2) * gr.gridElems * k));
+    GSHT_CUDA(cudaMalloc(&gr.coefOut, sizeof(double2) * gr.coefElems * k));
+    std::vector<const void*> ci, gp, co;
+    for (int i : gr.fields) {
+      ci.push_back(b->fields[i].coef_in);
+      gp.push_back(b->fields[i].grid);
+      co.push_back(b->fields[i].coef_out);
+    }
+    gsht_status st;
+    if ((st = upload_ptrs(&gr.coefInPtrs, ci)) != GSHT_OK) return st;
+    if ((st = upload_ptrs(&gr.gridPtrs, gp)) != GSHT_OK) return st;
+    if ((st = upload_ptrs(&gr.coefOutPtrs, co)) != GSHT_OK) return st;
+    // Defined batch inputs for the warm-up and tuning runs.
+    GSHT_CUDA(cudaMemsetAsync(gr.coefIn, 0, sizeof(double2) * gr.coefElems * k, b->stream));
+    GSHT_CUDA(cudaMemsetAsync(gr.gridBuf, 0, sizeof(double2) * gr.gridElems * k, b->stream));
+  }
+  // Warm-up (sizes every workspace, builds tile lists and layouts), then
+  // the autotuner: per group, the fastest BF16x3 tile width.
+  for (auto& gr : b->groups) {
+    gsht_status st = run_group(b, gr, 1, false, false, b->stream);
+    if (st == GSHT_OK) st = run_group(b, gr, 0, false, false, b->stream);
+    if (st != GSHT_OK) return st;
+    if (precision == GSHT_BF16X3 && autotune) {
+      float best = 3.4e38f;
+      int bestTile = 128;
+      for (int tile : {32, 64, 128}) {
+        gr.ntile = tile;
+        float ms = 0.f;
+        if ((st = time_group(b, gr, &ms)) != GSHT_OK) return st;
+        if (ms < best) {
+          best = ms;
+          bestTile = tile;
+        }
+      }
+      gr.ntile = bestTile;
+    }
+  }
+  GSHT_CUDA(cudaStreamSynchronize(b->stream));
+  for (auto& kv : b->grids) {
+    gsht_status st = gsht_device_status(kv.second);
+    if (st != GSHT_OK) return st;
+  }
+  // One graph per execution mode.
+  for (int mode = 0; mode < 3; mode++) {
+    GSHT_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
+    gsht_status st = run_all(b, mode, b->stream);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+    if (st != GSHT_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "batch graph capture");
+    b->graph[mode] = graph;
+    GSHT_CUDA(cudaGraphGetNodes(graph, nullptr, &b->nodes[mode]));
+    GSHT_CUDA(cudaGraphInstantiate(&b->exec[mode], graph, 0));
+  }
+  return GSHT_OK;
+}
+
+}  // namespace
+}  // namespace gsht
+
+using namespace gsht;
+
+extern "C" {
+
+gsht_status gsht_plan_batch(const gsht_field_desc* fields, int count, int precision,
+                            int autotune, gsht_batch** out) {
+  if (!out) return fail(GSHT_ERR_BAD_ARG, "output handle pointer is NULL");
+  *out = nullptr;
+  if (!fields || count < 1) return fail(GSHT_ERR_BAD_ARG, "need at least one field");
+  if (precision != GSHT_FP64 && precision != GSHT_BF16X3 && precision != GSHT_OZAKI)
+    return fail(GSHT_ERR_UNSUPPORTED, "precision %d not available", precision);
+  for (int i = 0; i < count; i++) {
+    const auto& f = fields[i];
+    const int na = f.n < 0 ? -f.n : f.n;
+    if (f.lmax < 1 || f.lmax > 8192)
+      return fail(GSHT_ERR_BAD_ARG, "field %d: lmax %d outside [1, 8192]", i, f.lmax);
+    if (na > f.lmax) return fail(GSHT_ERR_BAD_ARG, "field %d: |n| = %d exceeds lmax", i, na);
+    if (!f.coef_in || !f.grid || !f.coef_out)
+      return fail(GSHT_ERR_BAD_ARG, "field %d: coef_in, grid and coef_out must all be set", i);
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(GSHT_ERR_NO_DEVICE, "no CUDA device visible");
+  }
+  for (int i = 0; i < count; i++)
+    if (!on_device(fields[i].coef_in) || !on_device(fields[i].grid) ||
+        !on_device(fields[i].coef_out))
+      return fail(GSHT_ERR_BAD_ARG, "field %d: batch buffers must be device memory", i);
+  auto* b = new gsht_batch();
+  const gsht_status st = plan(fields, count, precision, autotune, b);
+  if (st != GSHT_OK) {
+    const std::string msg = gsht_last_error();
+    free_batch(b);
+    return fail(st, "%s", msg.c_str());
+  }
+  *out = b;
+  return GSHT_OK;
+}
+
+gsht_status gsht_batch_execute(gsht_batch* b, int mode, void* stream) {
+  if (!b) return fail(GSHT_ERR_BAD_ARG, "batch is NULL");
+  if (mode < GSHT_BATCH_FORWARD || mode > GSHT_BATCH_ROUND_TRIP)
+    return fail(GSHT_ERR_BAD_ARG, "bad batch mode %d", mode);
+  GSHT_CUDA(cudaSetDevice(b->device));
+  GSHT_CUDA(cudaGraphLaunch(b->exec[mode], reinterpret_cast<cudaStream_t>(stream)));
+  g_launches += b->nodes[mode];
+  return GSHT_OK;
+}
+
+gsht_status gsht_batch_info(const gsht_batch* b, int* groups, int* grids, long* graph_nodes) {
+  if (!b) return fail(GSHT_ERR_BAD_ARG, "batch is NULL");
+  if (groups) *groups = (int)b->groups.size();
+  if (grids) *grids = (int)b->grids.size();
+  if (graph_nodes) {
+    for (int i = 0; i < 3; i++) graph_nodes[i] = (long)b->nodes[i];
+  }
+  return GSHT_OK;
+}
+
+gsht_status gsht_batch_group(const gsht_batch* b, int index, int* lmax, int* n, int* is_real,
+                             int* count, int* ntile) {
+  if (!b || index < 0 || index >= (int)b->groups.size())
+    return fail(GSHT_ERR_BAD_ARG, "no group %d", index);
+  const auto& gr = b->groups[index];
+  if (lmax) *lmax = gr.lmax;
+  if (n) *n = gr.n;
+  if (is_real) *is_real = gr.isReal;
+  if (count) *count = (int)gr.fields.size();
+  if (ntile) *ntile = gr.ntile;
+  return GSHT_OK;
+}
+
+gsht_status gsht_batch_destroy(gsht_batch* b) {
+  free_batch(b);
+  return GSHT_OK;
+}
+
+}  // extern "C"

@@ -198,6 +198,11 @@ gsht_status legendre_inverse_oz(const gsht_grid* g, const Table* t, int lmax, in
 gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
                                 int count, const double* spec, void* operand, double* coef,
                                 cudaStream_t s);
+// Adds order-major result rows R[m][q][l - l0] (pitch `pitch`) into the
+// packed coefficients of `count` fields (forward accumulate semantics).
+gsht_status accumulate_forward(int L, int lmax, int n, int na, int count, int Q, int is_real,
+                               long coefSize, int pitch, const double* rows, double* coef,
+                               cudaStream_t s);
 
 // Cached operand layout (legendre_fp64.cu); the caller holds g->mu.
 const OperandLayout* operand_layout(const gsht_grid* g, int lmax, int na,

@@ -214,6 +214,152 @@ __global__ void __launch_bounds__(256, 2) k_legendre_fp64(Fp64Args p) {
   }
 }
 
+// Narrow batches (at most kStreamRows complex rows: one or two complex
+// fields, up to four real ones): the contraction is a table-streaming GEMV,
+// bound by HBM, so the table is read once with plain coalesced FP64 loads and
+// FMAs on the CUDA cores instead of DMMA tiles whose rows would be mostly
+// empty. Inverse: one thread per colatitude, the block's operand rows staged
+// in shared memory 256 degrees at a time. Forward: one warp per 4 degree
+// rows, lanes across colatitudes, the spectra staged 256 colatitudes at a
+// time, then a warp reduction.
+constexpr int kStreamRows = 4;
+
+template <int kQ>
+__global__ void __launch_bounds__(256) k_legendre_fp64_stream_inv(Fp64Args p) {
+  __shared__ double2 As[kQ][256];
+  const int m = blockIdx.y;
+  const int l0 = m > p.na ? m : p.na;
+  const int K = p.lmax - l0 + 1;
+  const int kp = p.opPitch[m];
+  const int tid = threadIdx.x;
+  const int j = blockIdx.x * 256 + tid;
+  const int tp = p.thetaPad;
+  const double2* A = p.A + p.opOff[m];
+  const double* T = p.table + (size_t)p.rowOff[m] * tp + (j < tp ? j : 0);
+  double2 acc[kQ];
+#pragma unroll
+  for (int q = 0; q < kQ; q++) acc[q] = make_double2(0.0, 0.0);
+  for (int k0 = 0; k0 < K; k0 += 256) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kQ; q++)
+      As[q][tid] = (q < p.Q && k0 + tid < kp) ? A[(size_t)q * kp + k0 + tid] : make_double2(0.0, 0.0);
+    __syncthreads();
+    const int kn = K - k0 < 256 ? K - k0 : 256;
+    if (j < p.nTheta) {
+#pragma unroll 8
+      for (int kk = 0; kk < kn; kk++) {
+        const double t = __ldg(T + (size_t)(k0 + kk) * tp);
+#pragma unroll
+        for (int q = 0; q < kQ; q++) {
+          acc[q].x = fma(t, As[q][kk].x, acc[q].x);
+          acc[q].y = fma(t, As[q][kk].y, acc[q].y);
+        }
+      }
+    }
+  }
+  if (j < p.nTheta) {
+#pragma unroll
+    for (int q = 0; q < kQ; q++)
+      if (q < p.Q) p.out[((size_t)m * p.Q + q) * tp + j] = acc[q];
+  }
+}
+
+template <int kQ>
+__global__ void __launch_bounds__(256) k_legendre_fp64_stream_fwd(Fp64Args p) {
+  __shared__ double2 Fs[kQ][256];
+  constexpr int kRowsPerWarp = 4;
+  const int m = blockIdx.y;
+  const int l0 = m > p.na ? m : p.na;
+  const int K = p.lmax - l0 + 1;
+  const int kBlock = blockIdx.x * 8 * kRowsPerWarp;
+  if (kBlock >= K) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tp = p.thetaPad;
+  const int k0 = kBlock + warp * kRowsPerWarp;
+  const double2* F = p.A + (size_t)m * p.Q * tp;
+  double2 acc[kRowsPerWarp][kQ];
+#pragma unroll
+  for (int r = 0; r < kRowsPerWarp; r++)
+#pragma unroll
+    for (int q = 0; q < kQ; q++) acc[r][q] = make_double2(0.0, 0.0);
+  for (int j0 = 0; j0 < tp; j0 += 256) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kQ; q++)
+      Fs[q][tid] = (q < p.Q && j0 + tid < tp) ? F[(size_t)q * tp + j0 + tid] : make_double2(0.0, 0.0);
+    __syncthreads();
+    const int jn = tp - j0 < 256 ? tp - j0 : 256;
+#pragma unroll
+    for (int r = 0; r < kRowsPerWarp; r++) {
+      const int k = k0 + r;
+      if (k >= K) break;
+      const double* T = p.table + (size_t)(p.rowOff[m] + k) * tp + j0;
+#pragma unroll 4
+      for (int jj = lane; jj < jn; jj += 32) {
+        const double t = __ldg(T + jj);
+#pragma unroll
+        for (int q = 0; q < kQ; q++) {
+          acc[r][q].x = fma(t, Fs[q][jj].x, acc[r][q].x);
+          acc[r][q].y = fma(t, Fs[q][jj].y, acc[r][q].y);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kRowsPerWarp; r++)
+#pragma unroll
+    for (int q = 0; q < kQ; q++)
+#pragma unroll
+      for (int o = 16; o; o >>= 1) {
+        acc[r][q].x += __shfl_xor_sync(0xffffffffu, acc[r][q].x, o);
+        acc[r][q].y += __shfl_xor_sync(0xffffffffu, acc[r][q].y, o);
+      }
+  if (lane != 0) return;
+#pragma unroll
+  for (int r = 0; r < kRowsPerWarp; r++) {
+    const int k = k0 + r;
+    if (k >= K) break;
+    const int l = l0 + k;
+#pragma unroll
+    for (int q = 0; q < kQ; q++) {
+      if (q >= p.Q) break;
+      const int sgn = q / p.count, f = q - sgn * p.count;
+      if (sgn == 1 && m == 0) continue;
+      double2 v = acc[r][q];
+      if (sgn == 1 && ((l + p.n) & 1)) v = make_double2(-v.x, -v.y);
+      const long idx = p.isReal ? (long)l * (l + 1) / 2 - (long)p.na * (p.na + 1) / 2 + m
+                                : (long)l * l - (long)p.n * p.n + l + (sgn ? -m : m);
+      double2* o = p.out + (size_t)f * p.coefSize + idx;
+      if (!p.isReal && sgn == 0 && m == p.L && l == p.L && p.lmax == p.L) {
+        *o = make_double2(0.0, 0.0);  // GaussLegendreGrid.h:209-215
+      } else {
+        const double2 c = *o;
+        *o = make_double2(c.x + v.x, c.y + v.y);
+      }
+    }
+  }
+}
+
+// Launches the inverse contraction: the streaming kernel for narrow batches,
+// the DMMA tiles otherwise.
+gsht_status launch_inverse_fp64(const gsht_grid* g, const Fp64Args& a, cudaStream_t s) {
+  if (a.Q <= kStreamRows) {
+    dim3 grid((g->n_theta + 255) / 256, a.lmax + 1);
+    if (a.Q <= 1) k_legendre_fp64_stream_inv<1><<<grid, 256, 0, s>>>(a);
+    else if (a.Q <= 2) k_legendre_fp64_stream_inv<2><<<grid, 256, 0, s>>>(a);
+    else k_legendre_fp64_stream_inv<4><<<grid, 256, 0, s>>>(a);
+    GSHT_LAUNCH_CHECK("k_legendre_fp64_stream_inv");
+    return GSHT_OK;
+  }
+  dim3 grid((g->n_theta + BN - 1) / BN, (a.Q + BMC - 1) / BMC, a.lmax + 1);
+  GSHT_CUDA(cudaFuncSetAttribute(k_legendre_fp64<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)fp64_smem_bytes<0>()));
+  k_legendre_fp64<0><<<grid, 256, fp64_smem_bytes<0>(), s>>>(a);
+  GSHT_LAUNCH_CHECK("k_legendre_fp64<inverse>");
+  return GSHT_OK;
+}
+
 // Packed coefficients -> per-order operand rows (inverse A operand):
 // op[m][q = sgn*count + f][k] = c_{l0+k, +/-m} * ((-1)^{l+n} for -m), zero
 // for l > lmax and in the padding.
@@ -335,14 +481,8 @@ gsht_status legendre_inverse_fp64(const gsht_grid* g, const Table* t, int lmax,
   a.isReal = is_real; a.rowOff = t->d_row_off; a.opOff = dOff; a.opPitch = dPitch;
   a.table = t->t64; a.A = op; a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = cs;
-  dim3 grid((g->n_theta + BN - 1) / BN, (Q + BMC - 1) / BMC, lmax + 1);
-  GSHT_CUDA(cudaFuncSetAttribute(k_legendre_fp64<0>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)fp64_smem_bytes<0>()));
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
-  k_legendre_fp64<0><<<grid, 256, fp64_smem_bytes<0>(), s>>>(a);
-  GSHT_LAUNCH_CHECK("k_legendre_fp64<inverse>");
-  return GSHT_OK;
+  return launch_inverse_fp64(g, a, s);
 }
 
 gsht_status legendre_forward_fp64(const gsht_grid* g, const Table* t, int lmax,
@@ -359,6 +499,14 @@ gsht_status legendre_forward_fp64(const gsht_grid* g, const Table* t, int lmax,
   a.out = reinterpret_cast<double2*>(coef);
   a.coefSize = coef_size(lmax, t->n, is_real);
   const int kMax = lmax - na + 1;
+  if (Q <= kStreamRows) {
+    dim3 sg((kMax + 31) / 32, lmax + 1);
+    if (Q <= 1) k_legendre_fp64_stream_fwd<1><<<sg, 256, 0, s>>>(a);
+    else if (Q <= 2) k_legendre_fp64_stream_fwd<2><<<sg, 256, 0, s>>>(a);
+    else k_legendre_fp64_stream_fwd<4><<<sg, 256, 0, s>>>(a);
+    GSHT_LAUNCH_CHECK("k_legendre_fp64_stream_fwd");
+    return GSHT_OK;
+  }
   dim3 grid((kMax + BN - 1) / BN, (Q + BMC - 1) / BMC, lmax + 1);
   GSHT_CUDA(cudaFuncSetAttribute(k_legendre_fp64<1>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -395,13 +543,7 @@ gsht_status legendre_inverse_fp64_layout(const gsht_grid* g, const Table* t, int
   a.isReal = is_real; a.rowOff = t->d_row_off; a.opOff = dOff; a.opPitch = dPitch;
   a.table = t->t64; a.A = op; a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = cs;
-  dim3 grid((g->n_theta + BN - 1) / BN, (Q + BMC - 1) / BMC, lmax + 1);
-  GSHT_CUDA(cudaFuncSetAttribute(k_legendre_fp64<0>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)fp64_smem_bytes<0>()));
-  k_legendre_fp64<0><<<grid, 256, fp64_smem_bytes<0>(), s>>>(a);
-  GSHT_LAUNCH_CHECK("k_legendre_fp64<inverse>");
-  return GSHT_OK;
+  return launch_inverse_fp64(g, a, s);
 }
 
 }  // namespace gsht

@@ -265,18 +265,10 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-__device__ __forceinline__ void write_slices(double y, int8_t* dst, size_t plane) {
-#pragma unroll
-  for (int s = 0; s < kS; s++) {
-    y *= 128.0;
-    const double q = trunc(y);
-    y -= q;
-    dst[s * plane] = (int8_t)q;
-  }
-}
 
 // Four values -> seven slice quads, s-th quad to dst + s * plane (4-byte
-// aligned): the 4-wide form of write_slices.
+// aligned): y is split into seven signed 7-bit truncation slices, y =
+// sum_s S_s 2^{-7(s+1)} (|y| < 1).
 __device__ __forceinline__ void write_slices4(const double (&y0)[4], int8_t* dst, size_t plane) {
   double y[4] = {y0[0], y0[1], y0[2], y0[3]};
 #pragma unroll

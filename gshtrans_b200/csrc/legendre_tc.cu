@@ -561,9 +561,15 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
   StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
   st = launch_bf16<1>(g, ntile, a, mapA, mapB, s);
   if (st != GSHT_OK) return st;
+  return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, tp, spec, coef, s);
+}
+
+gsht_status accumulate_forward(int L, int lmax, int n, int na, int count, int Q, int is_real,
+                               long coefSize, int pitch, const double* rows, double* coef,
+                               cudaStream_t s) {
   dim3 ag((lmax + 32) / 32, (lmax + 32) / 32, Q);
-  k_accumulate_forward<<<ag, 256, 0, s>>>(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize,
-                                          tp, reinterpret_cast<const double2*>(spec),
+  k_accumulate_forward<<<ag, 256, 0, s>>>(L, lmax, n, na, count, Q, is_real, coefSize, pitch,
+                                          reinterpret_cast<const double2*>(rows),
                                           reinterpret_cast<double2*>(coef));
   GSHT_LAUNCH_CHECK("k_accumulate_forward");
   return GSHT_OK;

@@ -178,6 +178,43 @@ gsht_status gsht_field_eval(const gsht_expr_op* program, int nops,
                             int ninputs, void* out, int out_is_real, long npoints,
                             int count, long field_stride, void* stream);
 
+/* Batched transforms of many fields of uneven size in one CUDA graph. No
+ * counterpart in the reference (its transforms take one field per call,
+ * GaussLegendreGrid.h:108-321; callers loop). Each field has its own degree
+ * and Gauss-Legendre grid (nTheta = lmax + 1, nPhi = 2 lmax), upper index and
+ * kind; its buffers are device memory in the layouts of gsht_forward /
+ * gsht_inverse: coef_in (packed coefficients the inverse reads), grid (the
+ * inverse writes, the forward reads), coef_out (the forward ADDS into, like
+ * ForwardTransformation). gsht_plan_batch groups the fields by (lmax, n,
+ * kind), builds one grid per distinct lmax (tables shared by every field of
+ * that degree), autotunes the BF16x3 tensor-core tile width per group when
+ * `autotune` is set, and captures one CUDA graph per mode; the buffers'
+ * addresses are fixed at planning, their contents are read at each
+ * execution. A plan is not thread-safe. */
+typedef struct gsht_field_desc {
+  int lmax;
+  int n;
+  int is_real;
+  const void* coef_in;
+  void* grid;
+  void* coef_out;
+} gsht_field_desc;
+typedef struct gsht_batch gsht_batch;
+enum {
+  GSHT_BATCH_FORWARD = 0,    /* grids -> coef_out += coefficients */
+  GSHT_BATCH_INVERSE = 1,    /* coef_in -> grids */
+  GSHT_BATCH_ROUND_TRIP = 2  /* inverse, then forward of the grids just made */
+};
+gsht_status gsht_plan_batch(const gsht_field_desc* fields, int count, int precision,
+                            int autotune, gsht_batch** out);
+gsht_status gsht_batch_execute(gsht_batch* batch, int mode, void* stream);
+/* Number of (lmax, n, kind) groups, of grids, and of graph nodes per mode. */
+gsht_status gsht_batch_info(const gsht_batch* batch, int* groups, int* grids,
+                            long* graph_nodes /* [3] or NULL */);
+gsht_status gsht_batch_group(const gsht_batch* batch, int index, int* lmax, int* n,
+                             int* is_real, int* count, int* ntile);
+gsht_status gsht_batch_destroy(gsht_batch* batch);
+
 /* Stage timing. No counterpart in the reference (which has no tracing):
  * while enabled, every stage of a transform call is bracketed by CUDA events
  * recorded on the call's stream; gsht_profile_read synchronises those events

@@ -82,3 +82,21 @@ def test_wigner_compute_validates_and_sizes_without_a_device():
         g.wigner(10, -1, 1, 0.5)           # negative mMax
     with pytest.raises(g.BadArgument):
         g.wigner(10, 10, 1, 0.5, mrange=2)  # MRange must be All or NonNegative
+
+
+def test_plan_batch_validates_without_a_device():
+    import gshtrans_b200 as g
+
+    d = g._FieldDesc(64, 0, 0, 1, 1, 1)
+    arr = (g._FieldDesc * 1)(d)
+    h = ctypes.c_void_p()
+    assert g.library.gsht_plan_batch(arr, 0, 1, 1, ctypes.byref(h)) == 1       # no fields
+    bad = (g._FieldDesc * 1)(g._FieldDesc(0, 0, 0, 1, 1, 1))
+    assert g.library.gsht_plan_batch(bad, 1, 1, 1, ctypes.byref(h)) == 1       # lmax 0
+    bad = (g._FieldDesc * 1)(g._FieldDesc(8, 9, 0, 1, 1, 1))
+    assert g.library.gsht_plan_batch(bad, 1, 1, 1, ctypes.byref(h)) == 1       # |n| > lmax
+    bad = (g._FieldDesc * 1)(g._FieldDesc(8, 0, 0, None, 1, 1))
+    assert g.library.gsht_plan_batch(bad, 1, 1, 1, ctypes.byref(h)) == 1       # NULL buffer
+    assert g.library.gsht_plan_batch(arr, 1, 7, 1, ctypes.byref(h)) == 5       # precision
+    assert g.library.gsht_plan_batch(arr, 1, 1, 1, ctypes.byref(h)) == 6       # no device
+    assert g.library.gsht_batch_execute(None, 0, None) == 1

@@ -146,14 +146,16 @@ def test_device_tensors_and_batches_match_single_host_calls(gsht):
             df = torch.zeros((B, g.FieldSize()), dtype=torch.float64 if is_real else torch.complex128, device="cuda")
             g.inverse_batch(L, n, dc, df)
             torch.cuda.synchronize()
-            np.testing.assert_array_equal(df.cpu().numpy(), np.stack(singles))
+            # Single fields take the table-streaming kernels, batches the DMMA
+            # tiles: the same sums, associated differently.
+            assert relerr(df.cpu().numpy(), np.stack(singles)) < 1e-14
             back = torch.zeros_like(dc)
             g.forward_batch(L, n, df, back)
             torch.cuda.synchronize()
             for b in range(B):
                 out = np.zeros_like(cs[b])
                 g.ForwardTransformation(L, n, singles[b], out)
-                np.testing.assert_array_equal(back[b].cpu().numpy(), out)
+                assert relerr(back[b].cpu().numpy(), out) < 1e-14
 
 
 @pytest.mark.parametrize("n,is_real", [(0, False), (2, True), (-2, False)])

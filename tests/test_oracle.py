@@ -148,3 +148,19 @@ def test_restated_wigner_vs_reference_single_angle_fixture(golden, restated):
     th = float(ws["c0_theta"][0])
     got = np.concatenate([restated.wigner_block(lmax, n, th) for n in range(-nmax, nmax + 1)])
     np.testing.assert_array_equal(got, ws["c0_values"])
+
+
+def test_package_coefficient_generator_matches_the_oracle():
+    # bench.py draws its inputs with the package's generator; the tests use
+    # the oracle's. Same seed, same arrays.
+    import gshtrans_b200 as g
+
+    for L, lmax, n, is_real, env in ((8, 8, 0, False, None), (33, 20, -2, False, 1.0),
+                                     (33, 33, 3, True, 1.5), (64, 64, 1, True, None)):
+        a = g.random_coefficients(np.random.default_rng(5), L, lmax, n, is_real, env)
+        b = oracle.random_coefficients(np.random.default_rng(5), L, lmax, n, is_real, env)
+        np.testing.assert_array_equal(a, b)
+        la, ma = g.degree_order(lmax, n, is_real)
+        lb, mb = oracle.degree_order(lmax, n, is_real)
+        np.testing.assert_array_equal(la, lb)
+        np.testing.assert_array_equal(ma, mb)
