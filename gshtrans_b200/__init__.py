@@ -56,7 +56,7 @@ class BadArgument(GSHTError, ValueError):
 def _load() -> ctypes.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python -m gshtrans_b200.build`"
+            f"{LIB_PATH} is missing: build it with `python gshtrans_b200/build.py`"
         )
     lib = ctypes.CDLL(LIB_PATH)
     vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)

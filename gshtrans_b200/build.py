@@ -1,6 +1,8 @@
 """Builds libgsht_cuda.so in-tree from gshtrans_b200/csrc/*.cu for sm_100a.
 
-    python -m gshtrans_b200.build
+    python gshtrans_b200/build.py
+
+(run as a script: importing the package loads the library it builds)
 
 The library is built next to this file so that it travels with the source
 tree; it has no dependency on PyTorch.
