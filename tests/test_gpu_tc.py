@@ -164,3 +164,20 @@ def test_ozaki_L1024_batched(gsht, n, is_real):
             res[prec] = (f.cpu().numpy(), back.cpu().numpy())
     assert relerr(res["ozaki"][0], res["fp64"][0]) < TOL_OZ
     assert relerr(res["ozaki"][1], res["fp64"][1]) < TOL_OZ
+
+
+@pytest.mark.parametrize("is_real", [False, True])
+def test_ozaki_L2048_single_field_vs_fp64(gsht, is_real):
+    # The large single-transform case: lmax 2048, n = 1, envelope (l+1)^-2;
+    # the FP64 reference path itself fails there (its start values
+    # underflow), so the Ozaki form is checked against this FP64 path and
+    # for its own round trip.
+    L, n = 2048, 1
+    rng = np.random.default_rng(2048 + int(is_real))
+    c = oracle.random_coefficients(rng, L, L, n, is_real, 2.0)
+    with gsht.GaussLegendreGrid(L, n, nrange=gsht.Single, forms=("ozaki",)) as g:
+        f64, b64 = _both(g, L, n, is_real, c, "fp64")
+        foz, boz = _both(g, L, n, is_real, c, "ozaki")
+    assert relerr(foz, f64) < TOL_OZ
+    assert relerr(boz, b64) < TOL_OZ
+    assert relerr(boz, c) < TOL_OZ
