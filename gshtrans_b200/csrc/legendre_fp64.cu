@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(256) k_legendre_fp64_stream_inv(Fp64Args p) {
     __syncthreads();
     const int kn = K - k0 < 256 ? K - k0 : 256;
     if (j < p.nTheta) {
-#pragma unroll 8
+#pragma unroll 16
       for (int kk = 0; kk < kn; kk++) {
         const double t = __ldg(T + (size_t)(k0 + kk) * tp);
 #pragma unroll
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(256) k_legendre_fp64_stream_fwd(Fp64Args p) {
       const int k = k0 + r;
       if (k >= K) break;
       const double* T = p.table + (size_t)(p.rowOff[m] + k) * tp + j0;
-#pragma unroll 4
+#pragma unroll 8
       for (int jj = lane; jj < jn; jj += 32) {
         const double t = __ldg(T + jj);
 #pragma unroll
