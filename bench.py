@@ -444,7 +444,8 @@ def e2e_run(gsht, grid, torch, coef_h, precision, args):
     return {"value": B * steps / dt, "unit": UNIT,
             "h2d_bytes_per_step": 2 * nbytes, "d2h_bytes_per_step": nbytes,
             "note": "host coefficients in and out (pinned), grid resident on the GPU; "
-                    "the forward output is uploaded because the forward accumulates into it"}
+                    "the forward output is uploaded because the forward accumulates into it; "
+                    "the library moves host batches in chunks that overlap the transforms"}
 
 
 # ---------------------------------------------------------------------------

@@ -114,6 +114,18 @@ gsht_status ensure_workspace(gsht_grid* g, size_t bytes) {
   return GSHT_OK;
 }
 
+// Copy streams and at least `events` events for the chunked host pipeline.
+gsht_status ensure_copy_streams(gsht_grid* g, int events) {
+  if (!g->h2d) GSHT_CUDA(cudaStreamCreateWithFlags(&g->h2d, cudaStreamNonBlocking));
+  if (!g->d2h) GSHT_CUDA(cudaStreamCreateWithFlags(&g->d2h, cudaStreamNonBlocking));
+  while ((int)g->xfer_ev.size() < events) {
+    cudaEvent_t e;
+    GSHT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    g->xfer_ev.push_back(e);
+  }
+  return GSHT_OK;
+}
+
 gsht_status validate(const gsht_grid* g, int lmax, int n, int is_real,
                      int precision, int count) {
   if (!g) return fail(GSHT_ERR_BAD_ARG, "grid is NULL");
@@ -159,27 +171,46 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
   const size_t outBytes = dir == 0 ? coefBytes : gridBytes;
   const bool inDev = is_device_ptr(in), outDev = is_device_ptr(out);
 
-  // Workspace: [spec][operand][in staging][out staging], 256-byte aligned.
-  const size_t specBytes = lmax > 0 ? sizeof(double) * 2 * spec_elems(g, lmax, is_real, count) : 0;
-  size_t opBytes = 0;
-  if (lmax > 0) {
-    if (precision == GSHT_BF16X3)
-      opBytes = bf16_operand_bytes(g, lmax, is_real, count, dir);
-    else if (precision == GSHT_OZAKI)
-      opBytes = oz_operand_bytes(g, lmax, is_real, count, dir);
-    else if (dir == 1)
-      opBytes = sizeof(double) * 2 * fp64_operand_elems(g, t, lmax, is_real, count);
-  }
-  size_t off = 0;
-  auto carve = [&](size_t b) { size_t o = off; off += round_up(b, 256); return o; };
-  const size_t oSpec = carve(specBytes), oOp = carve(opBytes);
-  const size_t oIn = carve(inDev ? 0 : inBytes), oOut = carve(outDev ? 0 : outBytes);
   // Inside a stream capture (batch graphs) nothing may be allocated, the
   // calls are serial on one stream, and events recorded outside the capture
   // may not be waited on.
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   GSHT_CUDA(cudaStreamIsCapturing(s, &cap));
   const bool capturing = cap != cudaStreamCaptureStatusNone;
+
+  // Host buffers: the fields move in chunks on two copy streams, so that the
+  // upload of chunk i+1, the transform of chunk i and the download of chunk
+  // i-1 overlap (PCIe carries both directions at once). At most kMaxChunks
+  // chunks of at least kMinChunkBytes of transfers each.
+  constexpr int kMaxChunks = 8;
+  constexpr size_t kMinChunkBytes = size_t(64) << 20;
+  const size_t inField = inBytes / count, outField = outBytes / count;
+  int chunk = count;
+  if ((!inDev || !outDev) && !capturing && lmax > 0 && count > 1) {
+    const size_t moved = (inDev ? 0 : inBytes) + (outDev ? 0 : (dir == 0 ? 2 : 1) * outBytes);
+    size_t nch = moved / kMinChunkBytes;
+    if (nch > (size_t)kMaxChunks) nch = kMaxChunks;
+    if (nch > (size_t)count) nch = count;
+    if (nch > 1) chunk = (int)((count + nch - 1) / nch);
+  }
+  const int nChunks = (count + chunk - 1) / chunk;
+
+  // Workspace: [spec][operand][in staging][out staging], 256-byte aligned;
+  // spec and operand hold one chunk, the staging areas all fields.
+  const size_t specBytes = lmax > 0 ? sizeof(double) * 2 * spec_elems(g, lmax, is_real, chunk) : 0;
+  size_t opBytes = 0;
+  if (lmax > 0) {
+    if (precision == GSHT_BF16X3)
+      opBytes = bf16_operand_bytes(g, lmax, is_real, chunk, dir);
+    else if (precision == GSHT_OZAKI)
+      opBytes = oz_operand_bytes(g, lmax, is_real, chunk, dir);
+    else if (dir == 1)
+      opBytes = sizeof(double) * 2 * fp64_operand_elems(g, t, lmax, is_real, chunk);
+  }
+  size_t off = 0;
+  auto carve = [&](size_t b) { size_t o = off; off += round_up(b, 256); return o; };
+  const size_t oSpec = carve(specBytes), oOp = carve(opBytes);
+  const size_t oIn = carve(inDev ? 0 : inBytes), oOut = carve(outDev ? 0 : outBytes);
   if (capturing && g->ws_bytes < (off > 0 ? off : 256))
     return fail(GSHT_ERR_UNSUPPORTED, "workspace must be sized by an uncaptured call first");
   st = ensure_workspace(g, off > 0 ? off : 256);
@@ -190,50 +221,90 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
 
   const double* dIn = inDev ? static_cast<const double*>(in) : reinterpret_cast<double*>(ws + oIn);
   double* dOut = outDev ? static_cast<double*>(out) : reinterpret_cast<double*>(ws + oOut);
-  if (!inDev) GSHT_CUDA(cudaMemcpyAsync(const_cast<double*>(dIn), in, inBytes, cudaMemcpyHostToDevice, s));
-  // The forward accumulates into its output, so host outputs are uploaded
-  // first; the inverse leaves grid points untouched only for lmax == 0.
-  if (!outDev && (dir == 0 || lmax == 0))
-    GSHT_CUDA(cudaMemcpyAsync(dOut, out, outBytes, cudaMemcpyHostToDevice, s));
 
-  if (lmax == 0) {
-    k_lmax0<<<(count + 127) / 128, 128, 0, s>>>(dir, is_real, count, fs, dIn, dOut);
-    GSHT_LAUNCH_CHECK("k_lmax0");
-  } else {
+  // The transform of c fields between device buffers, on stream s.
+  auto compute = [&](int c, const double* dI, double* dO) -> gsht_status {
+    if (lmax == 0) {
+      k_lmax0<<<(c + 127) / 128, 128, 0, s>>>(dir, is_real, c, fs, dI, dO);
+      GSHT_LAUNCH_CHECK("k_lmax0");
+      return GSHT_OK;
+    }
     double* spec = reinterpret_cast<double*>(ws + oSpec);
+    gsht_status r;
     if (dir == 0) {
       {
         StageTimer tm(GSHT_STAGE_FFT_FORWARD, s);
-        st = fft_forward(g, lmax, is_real, count, dIn, spec, s);
+        r = fft_forward(g, lmax, is_real, c, dI, spec, s);
       }
-      if (st != GSHT_OK) return st;
-      if (precision == GSHT_BF16X3) {
-        st = legendre_forward_bf16(g, t, lmax, is_real, count, spec, ws + oOp, dOut, ntile, s);
-      } else if (precision == GSHT_OZAKI) {
-        st = legendre_forward_oz(g, t, lmax, is_real, count, spec, ws + oOp, dOut, s);
-      } else {
-        StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
-        st = legendre_forward_fp64(g, t, lmax, is_real, count, spec, dOut, s);
+      if (r != GSHT_OK) return r;
+      if (precision == GSHT_BF16X3)
+        return legendre_forward_bf16(g, t, lmax, is_real, c, spec, ws + oOp, dO, ntile, s);
+      if (precision == GSHT_OZAKI)
+        return legendre_forward_oz(g, t, lmax, is_real, c, spec, ws + oOp, dO, s);
+      StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
+      return legendre_forward_fp64(g, t, lmax, is_real, c, spec, dO, s);
+    }
+    if (precision == GSHT_BF16X3)
+      r = legendre_inverse_bf16(g, t, lmax, is_real, c, dI, ws + oOp, spec, ntile, s);
+    else if (precision == GSHT_OZAKI)
+      r = legendre_inverse_oz(g, t, lmax, is_real, c, dI, ws + oOp, spec, s);
+    else
+      r = legendre_inverse_fp64(g, t, lmax, is_real, c, dI, reinterpret_cast<double*>(ws + oOp),
+                                spec, s);
+    if (r != GSHT_OK) return r;
+    StageTimer tm(GSHT_STAGE_FFT_INVERSE, s);
+    return fft_inverse(g, lmax, is_real, c, spec, dO, s);
+  };
+
+  if (nChunks == 1) {
+    if (!inDev) GSHT_CUDA(cudaMemcpyAsync(const_cast<double*>(dIn), in, inBytes, cudaMemcpyHostToDevice, s));
+    // The forward accumulates into its output, so host outputs are uploaded
+    // first; the inverse leaves grid points untouched only for lmax == 0.
+    if (!outDev && (dir == 0 || lmax == 0))
+      GSHT_CUDA(cudaMemcpyAsync(dOut, out, outBytes, cudaMemcpyHostToDevice, s));
+    st = compute(count, dIn, dOut);
+    if (st != GSHT_OK) return st;
+    if (!outDev) GSHT_CUDA(cudaMemcpyAsync(out, dOut, outBytes, cudaMemcpyDeviceToHost, s));
+  } else {
+    st = ensure_copy_streams(g, 2 * nChunks + 2);
+    if (st != GSHT_OK) return st;
+    cudaEvent_t* ev = g->xfer_ev.data();
+    // Uploads start after the work already queued on s (which may produce
+    // the host input) and after the workspace's previous users.
+    GSHT_CUDA(cudaEventRecord(ev[0], s));
+    GSHT_CUDA(cudaStreamWaitEvent(g->h2d, ev[0], 0));
+    GSHT_CUDA(cudaStreamWaitEvent(g->d2h, ev[0], 0));
+    for (int i = 0; i < nChunks && st == GSHT_OK; i++) {
+      const int f0 = i * chunk, c = count - f0 < chunk ? count - f0 : chunk;
+      const size_t inOff = inField * f0, outOff = outField * f0;
+      const double* dI = reinterpret_cast<const double*>(reinterpret_cast<const char*>(dIn) + inOff);
+      double* dO = reinterpret_cast<double*>(reinterpret_cast<char*>(dOut) + outOff);
+      if (!inDev)
+        GSHT_CUDA(cudaMemcpyAsync(const_cast<double*>(dI), static_cast<const char*>(in) + inOff,
+                                  inField * c, cudaMemcpyHostToDevice, g->h2d));
+      if (!outDev && dir == 0)
+        GSHT_CUDA(cudaMemcpyAsync(dO, static_cast<const char*>(out) + outOff, outField * c,
+                                  cudaMemcpyHostToDevice, g->h2d));
+      GSHT_CUDA(cudaEventRecord(ev[1 + 2 * i], g->h2d));
+      GSHT_CUDA(cudaStreamWaitEvent(s, ev[1 + 2 * i], 0));
+      st = compute(c, dI, dO);
+      if (st == GSHT_OK && !outDev) {
+        GSHT_CUDA(cudaEventRecord(ev[2 + 2 * i], s));
+        GSHT_CUDA(cudaStreamWaitEvent(g->d2h, ev[2 + 2 * i], 0));
+        GSHT_CUDA(cudaMemcpyAsync(static_cast<char*>(out) + outOff, dO, outField * c,
+                                  cudaMemcpyDeviceToHost, g->d2h));
       }
-      if (st != GSHT_OK) return st;
-    } else {
-      if (precision == GSHT_BF16X3) {
-        st = legendre_inverse_bf16(g, t, lmax, is_real, count, dIn, ws + oOp, spec, ntile, s);
-      } else if (precision == GSHT_OZAKI) {
-        st = legendre_inverse_oz(g, t, lmax, is_real, count, dIn, ws + oOp, spec, s);
-      } else {
-        double* op = reinterpret_cast<double*>(ws + oOp);
-        st = legendre_inverse_fp64(g, t, lmax, is_real, count, dIn, op, spec, s);
-      }
-      if (st != GSHT_OK) return st;
-      {
-        StageTimer tm(GSHT_STAGE_FFT_INVERSE, s);
-        st = fft_inverse(g, lmax, is_real, count, spec, dOut, s);
-      }
-      if (st != GSHT_OK) return st;
+    }
+    // s ends after the copies, also when a chunk failed to launch.
+    GSHT_CUDA(cudaEventRecord(ev[2 * nChunks + 1], g->d2h));
+    GSHT_CUDA(cudaStreamWaitEvent(s, ev[2 * nChunks + 1], 0));
+    GSHT_CUDA(cudaEventRecord(ev[2 * nChunks], g->h2d));
+    GSHT_CUDA(cudaStreamWaitEvent(s, ev[2 * nChunks], 0));
+    if (st != GSHT_OK) {
+      cudaStreamSynchronize(s);
+      return st;
     }
   }
-  if (!outDev) GSHT_CUDA(cudaMemcpyAsync(out, dOut, outBytes, cudaMemcpyDeviceToHost, s));
   if (!capturing) {
     if (!g->ws_done) GSHT_CUDA(cudaEventCreateWithFlags(&g->ws_done, cudaEventDisableTiming));
     GSHT_CUDA(cudaEventRecord(g->ws_done, s));
@@ -344,6 +415,9 @@ gsht_status gsht_grid_destroy(gsht_grid* g) {
   cudaFree(g->d_err);
   cudaFree(g->ws);
   if (g->ws_done) cudaEventDestroy(g->ws_done);
+  for (cudaEvent_t e : g->xfer_ev) cudaEventDestroy(e);
+  if (g->h2d) cudaStreamDestroy(g->h2d);
+  if (g->d2h) cudaStreamDestroy(g->d2h);
   delete g;
   return GSHT_OK;
 }

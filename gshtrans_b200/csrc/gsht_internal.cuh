@@ -133,6 +133,9 @@ struct gsht_grid {
   void* ws = nullptr;
   size_t ws_bytes = 0;
   cudaEvent_t ws_done = nullptr;  // recorded after the last call's kernels
+  // Copy streams and events of the chunked host-buffer pipeline (guarded by mu).
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  std::vector<cudaEvent_t> xfer_ev;
   // Cached operand layouts (guarded by mu).
   mutable std::vector<gsht::OperandLayout*> layouts;
   mutable std::vector<gsht::TileList*> tile_lists;

@@ -158,6 +158,49 @@ def test_device_tensors_and_batches_match_single_host_calls(gsht):
                 assert relerr(back[b].cpu().numpy(), out) < 1e-14
 
 
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+@pytest.mark.parametrize("pinned", [True, False])
+def test_chunked_host_batches_match_device_batches(gsht, precision, pinned):
+    """Host buffers large enough to be moved in chunks (upload, transform and
+    download of different chunks overlapping on three streams) give what the
+    same batch gives between device buffers."""
+    import torch
+
+    L, n, B = 512, 1, 24  # 24 x (4.2 MB coefficients + 8.4 MB grid): 4-6 chunks
+    rng = np.random.default_rng(31)
+    with gsht.GaussLegendreGrid(L, 1, forms=("bf16x3",)) as g:
+        cs = np.stack([oracle.random_coefficients(rng, L, L, n, False, 1.5) for _ in range(B)])
+        dc = torch.from_numpy(cs).cuda()
+        df = torch.zeros((B, g.FieldSize()), dtype=torch.complex128, device="cuda")
+        g.inverse_batch(L, n, dc, df, precision)
+        dback = torch.from_numpy(cs * 0.5).cuda()  # the forward accumulates into it
+        g.forward_batch(L, n, df, dback, precision)
+        torch.cuda.synchronize()
+        ref_f, ref_c = df.cpu().numpy(), dback.cpu().numpy()
+
+        def host(a):
+            t = torch.from_numpy(np.ascontiguousarray(a))
+            return t.pin_memory() if pinned else t
+
+        hc = host(cs)
+        hf = host(np.zeros((B, g.FieldSize()), np.complex128))
+        g.inverse_batch(L, n, hc, hf, precision)
+        hback = host(cs * 0.5)
+        g.forward_batch(L, n, hf, hback, precision)
+        tol = 1e-14 if precision == "fp64" else 1e-12
+        assert relerr(hf.numpy(), ref_f) < tol
+        assert relerr(hback.numpy(), ref_c) < tol
+        # Mixed: device input, host output (forward), and host input, device
+        # output (inverse).
+        hback2 = host(cs * 0.5)
+        g.forward_batch(L, n, df, hback2, precision)
+        assert relerr(hback2.numpy(), ref_c) < tol
+        df2 = torch.zeros_like(df)
+        g.inverse_batch(L, n, hc, df2, precision)
+        torch.cuda.synchronize()
+        assert relerr(df2.cpu().numpy(), ref_f) < tol
+
+
 @pytest.mark.parametrize("n,is_real", [(0, False), (2, True), (-2, False)])
 def test_L1024_vs_reference_and_round_trip(gsht, n, is_real):
     # configs[1]: lmax 1024, n in {0, +2, -2}, real and complex fields,
