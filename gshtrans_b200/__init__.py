@@ -21,7 +21,7 @@ from typing import Optional
 import numpy as np
 
 __all__ = [
-    "All", "NonNegative", "Single", "FP64", "BF16X3", "OZAKI",
+    "All", "NonNegative", "Single", "FP64", "BF16X3", "OZAKI", "RECURRENCE",
     "GaussLegendreGrid", "GSHTError", "BadArgument", "library", "launch_count",
     "coefficient_size", "wigner", "Batch", "random_coefficients", "degree_order",
 ]
@@ -31,9 +31,9 @@ LIB_PATH = os.path.join(_HERE, "libgsht_cuda.so")
 
 # Index ranges (Concepts.h:24-27) and precision forms (include/gsht.h).
 All, NonNegative, Single = 0, 1, 2
-FP64, BF16X3, OZAKI = 0, 1, 2
-_FORM_BIT = {FP64: 1, BF16X3: 2, OZAKI: 4}
-_PRECISION_NAMES = {"fp64": FP64, "bf16x3": BF16X3, "ozaki": OZAKI}
+FP64, BF16X3, OZAKI, RECURRENCE = 0, 1, 2, 3
+_FORM_BIT = {FP64: 1, BF16X3: 2, OZAKI: 4, RECURRENCE: 8}
+_PRECISION_NAMES = {"fp64": FP64, "bf16x3": BF16X3, "ozaki": OZAKI, "recurrence": RECURRENCE}
 
 _STATUS = {
     0: "OK", 1: "BAD_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOUT",
@@ -199,14 +199,19 @@ class GaussLegendreGrid:
     ``mrange`` is ``All`` or ``NonNegative``; ``nrange`` is ``All``,
     ``NonNegative`` or ``Single`` (GaussLegendreGrid.h:24-26). ``forms``
     selects which table forms are built besides FP64: any of ``"bf16x3"``,
-    ``"ozaki"``.
+    ``"ozaki"``, ``"recurrence"``. ``forms=("recurrence",)`` alone stores no
+    table: every transform runs in FP64 with the Wigner values generated by
+    the l-recurrence inside the contraction (precision ``"fp64"`` or
+    ``"recurrence"``).
     """
 
     def __init__(self, lmax: int, nmax: int, mrange: int = All, nrange: int = All,
                  forms=()):
-        mask = 1
+        mask = 0
         for f in forms:
             mask |= _FORM_BIT[_precision(f)]
+        if mask != _FORM_BIT[RECURRENCE]:
+            mask |= _FORM_BIT[FP64]
         h = ctypes.c_void_p()
         _check(library.gsht_grid_create(int(lmax), int(nmax), int(mrange), int(nrange),
                                         mask, ctypes.byref(h)))

@@ -138,8 +138,11 @@ gsht_status validate(const gsht_grid* g, int lmax, int n, int is_real,
     return fail(GSHT_ERR_BAD_ARG, "|n| = %d exceeds lmax = %d", n < 0 ? -n : n, lmax);
   if (!is_real && g->mrange != GSHT_RANGE_ALL)
     return fail(GSHT_ERR_BAD_ARG, "complex fields need MRange = All");
-  if (precision != GSHT_FP64 && precision != GSHT_BF16X3 && precision != GSHT_OZAKI)
+  if (precision != GSHT_FP64 && precision != GSHT_BF16X3 && precision != GSHT_OZAKI &&
+      precision != GSHT_RECURRENCE)
     return fail(GSHT_ERR_UNSUPPORTED, "precision %d not available", precision);
+  if (precision == GSHT_RECURRENCE && !(g->forms & GSHT_FORM_RECURRENCE))
+    return fail(GSHT_ERR_UNSUPPORTED, "the recurrence form was not built for this grid");
   if (precision == GSHT_BF16X3 && !(g->forms & GSHT_FORM_BF16X3))
     return fail(GSHT_ERR_UNSUPPORTED, "the BF16x3 table form was not built for this grid");
   if (precision == GSHT_OZAKI && !(g->forms & GSHT_FORM_OZAKI))
@@ -163,6 +166,8 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream_ptr);
   CallScope scope(g, s);
   const Table* t = g->table(n);
+  // FP64 through the l-recurrence when asked for, or when no table is stored.
+  const bool rec = precision == GSHT_RECURRENCE || (precision == GSHT_FP64 && !t->t64);
   const long cs = coef_size(lmax, n, is_real);
   const long fs = (long)g->n_theta * g->n_phi;
   const size_t coefBytes = sizeof(double) * 2 * cs * (size_t)count;
@@ -206,6 +211,8 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
       opBytes = oz_operand_bytes(g, lmax, is_real, chunk, dir);
     else if (dir == 1)
       opBytes = sizeof(double) * 2 * fp64_operand_elems(g, t, lmax, is_real, chunk);
+    else if (rec)
+      opBytes = rec_forward_bytes(g, t, is_real, chunk);
   }
   size_t off = 0;
   auto carve = [&](size_t b) { size_t o = off; off += round_up(b, 256); return o; };
@@ -241,6 +248,7 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
         return legendre_forward_bf16(g, t, lmax, is_real, c, spec, ws + oOp, dO, ntile, s);
       if (precision == GSHT_OZAKI)
         return legendre_forward_oz(g, t, lmax, is_real, c, spec, ws + oOp, dO, s);
+      if (rec) return legendre_forward_rec(g, t, lmax, is_real, c, spec, ws + oOp, dO, s);
       StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
       return legendre_forward_fp64(g, t, lmax, is_real, c, spec, dO, s);
     }
@@ -248,6 +256,9 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
       r = legendre_inverse_bf16(g, t, lmax, is_real, c, dI, ws + oOp, spec, ntile, s);
     else if (precision == GSHT_OZAKI)
       r = legendre_inverse_oz(g, t, lmax, is_real, c, dI, ws + oOp, spec, s);
+    else if (rec)
+      r = legendre_inverse_rec(g, t, lmax, is_real, c, dI, reinterpret_cast<double*>(ws + oOp),
+                               spec, s);
     else
       r = legendre_inverse_fp64(g, t, lmax, is_real, c, dI, reinterpret_cast<double*>(ws + oOp),
                                 spec, s);
@@ -345,7 +356,7 @@ gsht_status gsht_grid_create(int lmax, int nmax, int mrange, int nrange,
     return fail(GSHT_ERR_BAD_ARG, "mrange must be All or NonNegative");
   if (nrange < GSHT_RANGE_ALL || nrange > GSHT_RANGE_SINGLE)
     return fail(GSHT_ERR_BAD_ARG, "bad nrange %d", nrange);
-  if (forms & ~7u) return fail(GSHT_ERR_BAD_ARG, "unknown form bits 0x%x", forms);
+  if (forms & ~15u) return fail(GSHT_ERR_BAD_ARG, "unknown form bits 0x%x", forms);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -358,7 +369,7 @@ gsht_status gsht_grid_create(int lmax, int nmax, int mrange, int nrange,
   g->nmax = nmax;
   g->mrange = mrange;
   g->nrange = nrange;
-  g->forms = forms | GSHT_FORM_FP64;
+  g->forms = forms == GSHT_FORM_RECURRENCE ? forms : forms | GSHT_FORM_FP64;
   g->min_n = nrange == GSHT_RANGE_ALL ? -nmax : (nrange == GSHT_RANGE_NONNEGATIVE ? 0 : nmax);
   g->n_theta = lmax + 1;
   g->n_phi = 2 * lmax;
@@ -391,8 +402,11 @@ gsht_status gsht_grid_create(int lmax, int nmax, int mrange, int nrange,
     for (int n = g->min_n; n <= g->nmax && st == GSHT_OK; n++) {
       Table* t = &g->tables[n - g->min_n];
       t->n = n;
-      st = build_table(g, t, s);
-      if (st == GSHT_OK) st = build_forms(g, t, s);
+      if (g->forms & GSHT_FORM_FP64) {
+        st = build_table(g, t, s);
+        if (st == GSHT_OK) st = build_forms(g, t, s);
+      }
+      if (st == GSHT_OK && (g->forms & GSHT_FORM_RECURRENCE)) st = build_recurrence(g, t, s);
     }
   }
   if (st != GSHT_OK) {
@@ -453,6 +467,8 @@ gsht_status gsht_wigner_block(const gsht_grid* g, int n, int itheta,
   if (count) *count = total;
   if (!out) return GSHT_OK;
   const Table* t = g->table(n);
+  if (!t->t64)
+    return fail(GSHT_ERR_UNSUPPORTED, "the grid stores no table (recurrence form); use gsht_wigner_compute");
   GSHT_CUDA(cudaSetDevice(g->device));
   std::vector<double> col(t->rows), mir(t->rows);
   const size_t pitch = sizeof(double) * g->theta_pad;

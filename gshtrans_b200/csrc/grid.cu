@@ -189,6 +189,46 @@ __global__ void k_wigner_start(int L, int n, int nTheta, int thetaPad,
   }
 }
 
+// Coefficients of step k = l - l0 of the l-recurrence (Wigner.h:347-472) for
+// order m >= 0 and upper index n: d^l = (a cos(theta) - b) d^{l-1} - g d^{l-2}
+// for k >= 1, and the normalisation of degree l (Ortho: sqrt(2l+1)/(2 sqrt(pi)),
+// FourPi: 1; Wigner.h:475-485). Step 0 (the start value) has a = b = g = 0.
+// Shared by the table build and the on-the-fly recurrence of the transforms.
+__device__ __forceinline__ void chain_coefficients(int n, int m, int l, int k, int ortho,
+                                                   double* a, double* b, double* g,
+                                                   double* nrm) {
+  const int na = n < 0 ? -n : n;
+  *nrm = ortho ? sqrt((double)(2 * l + 1)) * 0.28209479177387814347 : 1.0;
+  *a = 0.0;
+  *b = 0.0;
+  *g = 0.0;
+  if (k == 1) {
+    if (m <= na) {
+      // Row |n|+1, interior orders (Wigner.h:365-373).
+      const double sg = n < 0 ? -1.0 : 1.0;
+      const double c0 = (2.0 * l - 1.0) * rsqrt((double)(l + na)) *
+                        rsqrt((double)(l - m)) * rsqrt((double)(l + m));
+      *a = c0 * l;
+      *b = c0 * sg * m;
+    } else {
+      // One-term recursion at m = l - 1 (Wigner.h:406-413, 448-457).
+      const double c0 = (2.0 * l - 1.0) * rsqrt((double)(l - n)) *
+                        rsqrt((double)(l + n)) * rsqrt((double)(l - m)) *
+                        rsqrt((double)(l + m)) / (double)(l - 1);
+      *a = c0 * l * (l - 1.0);
+      *b = c0 * (double)m * (double)n;
+    }
+  } else if (k >= 2) {
+    // Two-term recursion (Wigner.h:428-445).
+    const double inl = rsqrt((double)(l - n)) * rsqrt((double)(l + n));
+    const double dn = rsqrt((double)(l - m)) * rsqrt((double)(l + m));
+    *a = (2.0 * l - 1.0) * l * inl * dn;
+    *b = (2.0 * l - 1.0) * n * inl / (l - 1.0) * m * dn;
+    *g = l * sqrt((double)(l - 1 - n)) * sqrt((double)(l - 1 + n)) * inl / (l - 1.0) *
+         sqrt((double)(l - 1 - m)) * sqrt((double)(l - 1 + m)) * dn;
+  }
+}
+
 // The l-recurrence (Wigner.h:347-472) for one order m per block (blockIdx.y)
 // and one colatitude per thread. Per-degree coefficients are computed once per
 // block into shared memory; the chain runs in exponent-extended form until its
@@ -207,40 +247,8 @@ __global__ void __launch_bounds__(128) k_wigner_chain(
   double* b = sh + K;
   double* g = sh + 2 * K;  // f2
   double* nrm = sh + 3 * K;
-  for (int k = threadIdx.x; k < K; k += blockDim.x) {
-    const int l = l0 + k;
-    // Ortho: sqrt(2l+1)/(2 sqrt(pi)); FourPi: unnormalised (Wigner.h:475-485).
-    nrm[k] = ortho ? sqrt((double)(2 * l + 1)) * 0.28209479177387814347 : 1.0;
-    a[k] = 0.0;
-    b[k] = 0.0;
-    g[k] = 0.0;
-    if (k == 1) {
-      if (m <= na) {
-        // Row |n|+1, interior orders (Wigner.h:365-373).
-        const double sg = n < 0 ? -1.0 : 1.0;
-        const double c0 = (2.0 * l - 1.0) * rsqrt((double)(l + na)) *
-                          rsqrt((double)(l - m)) * rsqrt((double)(l + m));
-        a[k] = c0 * l;
-        b[k] = c0 * sg * m;
-      } else {
-        // One-term recursion at m = l - 1 (Wigner.h:406-413, 448-457).
-        const double c0 = (2.0 * l - 1.0) * rsqrt((double)(l - n)) *
-                          rsqrt((double)(l + n)) * rsqrt((double)(l - m)) *
-                          rsqrt((double)(l + m)) / (double)(l - 1);
-        a[k] = c0 * l * (l - 1.0);
-        b[k] = c0 * (double)m * (double)n;
-      }
-    } else if (k >= 2) {
-      // Two-term recursion (Wigner.h:428-445).
-      const double inl = rsqrt((double)(l - n)) * rsqrt((double)(l + n));
-      const double dn = rsqrt((double)(l - m)) * rsqrt((double)(l + m));
-      a[k] = (2.0 * l - 1.0) * l * inl * dn;
-      b[k] = (2.0 * l - 1.0) * n * inl / (l - 1.0) * m * dn;
-      g[k] = l * sqrt((double)(l - 1 - n)) * sqrt((double)(l - 1 + n)) * inl /
-             (l - 1.0) * sqrt((double)(l - 1 - m)) * sqrt((double)(l - 1 + m)) *
-             dn;
-    }
-  }
+  for (int k = threadIdx.x; k < K; k += blockDim.x)
+    chain_coefficients(n, m, l0 + k, k, ortho, &a[k], &b[k], &g[k], &nrm[k]);
   __syncthreads();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= thetaPad) return;
@@ -393,6 +401,74 @@ gsht_status build_table(gsht_grid* g, Table* t, cudaStream_t s) {
   return compute_table(g->L, g->n_theta, g->theta_pad, g->d_theta, 1, t, s);
 }
 
+// Recurrence-form coefficients per table row (m, k). The recurrence
+// d_k = (a_k c - b_k) d_{k-1} - g_k d_{k-2} (c = cos theta) is carried for
+// e_k = d_k / s_k with s_0 = s_1 = 1, s_k = g_k s_{k-2}, which turns it into
+// e_k = (a'_k c - b'_k) e_{k-1} - e_{k-2}, a'_k = a_k s_{k-1} / s_k (same for
+// b): two FMAs per step instead of three. Stored: (a'_k, b'_k) and the
+// factor sc_k = norm_k s_k that turns e_k into the normalised value; step 0 is
+// (a', b') = (0, -1), so that with the initial state e_{-1} = 0, e_{-2} =
+// -d_0 every step runs the same update. One thread per order m (the s_k are a
+// running product over k).
+__global__ void k_rec_coefficients(int L, int n, int ortho, const long long* __restrict__ row_off,
+                                   double2* __restrict__ ab, double* __restrict__ sc) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m > L) return;
+  const int na = n < 0 ? -n : n;
+  const int l0 = m > na ? m : na;
+  const int K = L - l0 + 1;
+  const size_t r0 = (size_t)row_off[m];
+  double s1 = 1.0, s2 = 1.0;  // s_{k-1}, s_{k-2}
+  for (int k = 0; k < K; k++) {
+    double a, b, g, nrm;
+    chain_coefficients(n, m, l0 + k, k, ortho, &a, &b, &g, &nrm);
+    double sk = 1.0;
+    if (k == 0) {
+      a = 0.0;
+      b = -1.0;
+    } else if (k >= 2) {
+      sk = g * s2;
+      const double r = s1 / sk;
+      a *= r;
+      b *= r;
+    }
+    ab[r0 + k] = make_double2(a, b);
+    sc[r0 + k] = nrm * sk;
+    s2 = s1;
+    s1 = sk;
+  }
+}
+
+gsht_status build_recurrence(gsht_grid* g, Table* t, cudaStream_t s) {
+  const int L = g->L, tp = g->theta_pad, na = t->n < 0 ? -t->n : t->n;
+  if (!t->d_row_off) {
+    t->row_off.assign(L + 2, 0);
+    for (int m = 0; m <= L; m++) {
+      const int l0 = m > na ? m : na;
+      t->row_off[m + 1] = t->row_off[m] + (L - l0 + 1);
+    }
+    t->rows = t->row_off[L + 1];
+    GSHT_CUDA(cudaMalloc(&t->d_row_off, sizeof(long long) * (L + 2)));
+    GSHT_CUDA(cudaMemcpy(t->d_row_off, t->row_off.data(), sizeof(long long) * (L + 2),
+                         cudaMemcpyHostToDevice));
+  }
+  if (cudaMalloc(&t->rec_f, sizeof(double) * (size_t)(L + 1) * tp) != cudaSuccess ||
+      cudaMalloc(&t->rec_e, sizeof(int) * (size_t)(L + 1) * tp) != cudaSuccess ||
+      cudaMalloc(&t->rec_ab, sizeof(double2) * (size_t)t->rows) != cudaSuccess ||
+      cudaMalloc(&t->rec_sc, sizeof(double) * (size_t)t->rows) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(GSHT_ERR_OOM, "recurrence form allocation failed");
+  }
+  k_wigner_start<<<(g->n_theta + 127) / 128, 128, 0, s>>>(L, t->n, g->n_theta, tp, g->d_theta,
+                                                          t->rec_f, t->rec_e);
+  GSHT_LAUNCH_CHECK("k_wigner_start");
+  k_rec_coefficients<<<(L + 1 + 127) / 128, 128, 0, s>>>(L, t->n, 1, t->d_row_off, t->rec_ab,
+                                                          t->rec_sc);
+  GSHT_LAUNCH_CHECK("k_rec_coefficients");
+  GSHT_CUDA(cudaStreamSynchronize(s));
+  return GSHT_OK;
+}
+
 gsht_status build_forms(gsht_grid* g, Table* t, cudaStream_t s) {
   const int L = g->L, tp = g->theta_pad;
   const size_t plane = (size_t)(t->rows + kTablePadRows) * tp;
@@ -497,6 +573,10 @@ void free_table(Table* t) {
   cudaFree(t->tbf);
   cudaFree(t->ti8);
   cudaFree(t->i8_exp);
+  cudaFree(t->rec_f);
+  cudaFree(t->rec_e);
+  cudaFree(t->rec_ab);
+  cudaFree(t->rec_sc);
   *t = Table{};
 }
 

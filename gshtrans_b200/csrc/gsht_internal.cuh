@@ -84,6 +84,14 @@ struct Table {
   __nv_bfloat16* tbf = nullptr;       // 3 planes (hi, mid, lo), same layout
   int8_t* ti8 = nullptr;              // kTableSlices planes, same layout
   int* i8_exp = nullptr;              // (L+1) x thetaPad column exponents
+  // Recurrence form (no stored values): start values d^{l0(m)}_{mn}(theta_j)
+  // = rec_f * 2^rec_e, [m][thetaPad], and per row the coefficients (a', b')
+  // of the rescaled recurrence e_k = (a' cos(theta) - b') e_{k-1} - e_{k-2}
+  // and the factor rec_sc with d_k * norm_k = rec_sc * e_k (grid.cu).
+  double* rec_f = nullptr;
+  int* rec_e = nullptr;
+  double2* rec_ab = nullptr;
+  double* rec_sc = nullptr;
 };
 
 // Per-order layout of field-side operand rows for one (lmax, |n|, rows,
@@ -152,6 +160,7 @@ namespace gsht {
 gsht_status build_nodes(gsht_grid* g);
 gsht_status build_table(gsht_grid* g, Table* t, cudaStream_t s);
 gsht_status build_forms(gsht_grid* g, Table* t, cudaStream_t s);
+gsht_status build_recurrence(gsht_grid* g, Table* t, cudaStream_t s);
 void free_table(Table* t);
 gsht_status wigner_compute(int lmax, int mmax, int nmax, int mrange, int nrange, int norm,
                            int row_major, const double* theta, int ntheta, double* out,
@@ -170,6 +179,10 @@ gsht_status legendre_inverse_fp64(const gsht_grid* g, const Table* t, int lmax,
                                   int is_real, int count, const double* coef,
                                   double* operand, double* spec,
                                   cudaStream_t s);
+// Packed coefficients -> FP64 operand rows op[m][q][k] (the inverse's A).
+gsht_status prep_inverse_fp64(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                              int count, const double* coef, double* operand,
+                              const OperandLayout** layout, cudaStream_t s);
 gsht_status legendre_forward_fp64(const gsht_grid* g, const Table* t, int lmax,
                                   int is_real, int count, const double* spec,
                                   double* coef, cudaStream_t s);
@@ -201,6 +214,17 @@ gsht_status legendre_inverse_oz(const gsht_grid* g, const Table* t, int lmax, in
 gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
                                 int count, const double* spec, void* operand, double* coef,
                                 cudaStream_t s);
+// Legendre stage, FP64 with the Wigner values generated by the l-recurrence
+// inside the contraction (legendre_rec.cu); no stored table.
+size_t rec_forward_bytes(const gsht_grid* g, const Table* t, int is_real, int count);
+gsht_status legendre_inverse_rec(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                                 int count, const double* coef, double* operand, double* spec,
+                                 cudaStream_t s);
+// spec is overwritten with the result rows; partial holds rec_forward_bytes.
+gsht_status legendre_forward_rec(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                                 int count, double* spec, void* partial, double* coef,
+                                 cudaStream_t s);
+
 // Adds order-major result rows R[m][q][l - l0] (pitch `pitch`) into the
 // packed coefficients of `count` fields (forward accumulate semantics).
 gsht_status accumulate_forward(int L, int lmax, int n, int na, int count, int Q, int is_real,

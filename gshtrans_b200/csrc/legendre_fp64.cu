@@ -468,6 +468,26 @@ size_t fp64_operand_elems(const gsht_grid* g, const Table* t, int lmax,
   return o ? (size_t)o->total : 0;
 }
 
+gsht_status prep_inverse_fp64(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                              int count, const double* coef, double* operand,
+                              const OperandLayout** layout, cudaStream_t s) {
+  const int na = t->n < 0 ? -t->n : t->n;
+  const int sgnCount = is_real ? 1 : 2;
+  const int Q = sgnCount * count;
+  gsht_status st;
+  const OperandLayout* lay = operand_layout(g, lmax, na, Q, kDegreePadFp64, &st);
+  if (!lay) return st;
+  *layout = lay;
+  StageTimer tm(GSHT_STAGE_PREP_INVERSE, s);
+  dim3 pg((lay->pitch_max + 127) / 128, lmax + 1, Q);
+  k_prep_inverse_fp64<<<pg, 128, 0, s>>>(lmax, t->n, na, count, sgnCount, is_real,
+                                         coef_size(lmax, t->n, is_real),
+                                         reinterpret_cast<const double2*>(coef), lay->d_off,
+                                         lay->d_pitch, reinterpret_cast<double2*>(operand));
+  GSHT_LAUNCH_CHECK("k_prep_inverse_fp64");
+  return GSHT_OK;
+}
+
 gsht_status legendre_inverse_fp64(const gsht_grid* g, const Table* t, int lmax,
                                   int is_real, int count, const double* coef,
                                   double* operand, double* spec,
@@ -475,28 +495,16 @@ gsht_status legendre_inverse_fp64(const gsht_grid* g, const Table* t, int lmax,
   const int na = t->n < 0 ? -t->n : t->n;
   const int sgnCount = is_real ? 1 : 2;
   const int Q = sgnCount * count;
-  gsht_status st;
-  const OperandLayout* lay = operand_layout(g, lmax, na, Q, kDegreePadFp64, &st);
-  if (!lay) return st;
-  const long long* dOff = lay->d_off;
-  const int* dPitch = lay->d_pitch;
-  double2* op = reinterpret_cast<double2*>(operand);
-  const long cs = coef_size(lmax, t->n, is_real);
-  const int kpMax = lay->pitch_max;
-  {
-    StageTimer tm(GSHT_STAGE_PREP_INVERSE, s);
-    dim3 pg((kpMax + 127) / 128, lmax + 1, Q);
-    k_prep_inverse_fp64<<<pg, 128, 0, s>>>(lmax, t->n, na, count, sgnCount, is_real,
-                                           cs, reinterpret_cast<const double2*>(coef),
-                                           dOff, dPitch, op);
-    GSHT_LAUNCH_CHECK("k_prep_inverse_fp64");
-  }
+  const OperandLayout* lay = nullptr;
+  gsht_status st = prep_inverse_fp64(g, t, lmax, is_real, count, coef, operand, &lay, s);
+  if (st != GSHT_OK) return st;
   Fp64Args a{};
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count;
   a.sgnCount = sgnCount; a.Q = Q; a.nTheta = g->n_theta; a.thetaPad = g->theta_pad;
-  a.isReal = is_real; a.rowOff = t->d_row_off; a.opOff = dOff; a.opPitch = dPitch;
-  a.table = t->t64; a.A = op; a.out = reinterpret_cast<double2*>(spec);
-  a.coefSize = cs;
+  a.isReal = is_real; a.rowOff = t->d_row_off; a.opOff = lay->d_off; a.opPitch = lay->d_pitch;
+  a.table = t->t64; a.A = reinterpret_cast<double2*>(operand);
+  a.out = reinterpret_cast<double2*>(spec);
+  a.coefSize = coef_size(lmax, t->n, is_real);
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
   return launch_inverse_fp64(g, a, s);
 }

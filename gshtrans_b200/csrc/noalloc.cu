@@ -92,6 +92,7 @@ extern "C" gsht_status gsht_inverse_noalloc(const gsht_grid* g, int lmax, int n,
     return fail(GSHT_ERR_BAD_ARG, "gsht_inverse_noalloc needs device pointers for in and out");
 
   const Table* t = g->table(n);
+  if (!t->t64) return fail(GSHT_ERR_UNSUPPORTED, "gsht_inverse_noalloc needs the stored FP64 table");
   const int na = n < 0 ? -n : n;
   const int Q = is_real ? 1 : 2;  // one field: rows for +m (and -m)
   // Scratch layout: [off (lmax+2) x int64][pitch (lmax+1) x int32][operand][spec].

@@ -53,11 +53,20 @@ enum { GSHT_RANGE_ALL = 0, GSHT_RANGE_NONNEGATIVE = 1, GSHT_RANGE_SINGLE = 2 };
 enum {
   GSHT_FP64 = 0,   /* FP64 tensor-core (DMMA) contraction: the drop-in path   */
   GSHT_BF16X3 = 1, /* hi/mid/lo BF16 split products, FP32 accumulation       */
-  GSHT_OZAKI = 2   /* Ozaki INT8 slices, exact INT32 accumulation, FP64 sum   */
+  GSHT_OZAKI = 2,  /* Ozaki INT8 slices, exact INT32 accumulation, FP64 sum   */
+  GSHT_RECURRENCE = 3 /* FP64 with d^l_mn(theta) generated by the l-recurrence
+                         inside the contraction kernels (no stored table); the
+                         path GSHT_FP64 takes on grids built without FP64 table */
 };
 
-/* Table forms built by gsht_grid_create (bit mask). */
-enum { GSHT_FORM_FP64 = 1, GSHT_FORM_BF16X3 = 2, GSHT_FORM_OZAKI = 4 };
+/* Table forms built by gsht_grid_create (bit mask). GSHT_FORM_RECURRENCE
+ * alone builds no table at all: only the recurrence's start values and
+ * coefficients (about (L+1)^2 x 28 B per upper index instead of
+ * (L+1)^2 (L+1) x 4 B); transforms then run in FP64 through the recurrence,
+ * and the BF16x3 / Ozaki forms and gsht_wigner_block are unavailable. No
+ * counterpart in the reference, whose grid always stores the table
+ * (GaussLegendreGrid.h:52-53). */
+enum { GSHT_FORM_FP64 = 1, GSHT_FORM_BF16X3 = 2, GSHT_FORM_OZAKI = 4, GSHT_FORM_RECURRENCE = 8 };
 
 typedef struct gsht_grid gsht_grid;
 
@@ -67,7 +76,8 @@ typedef struct gsht_grid gsht_grid;
  * Wigner.h:116-137): computes the Gauss-Legendre nodes and the Wigner tables
  * for every upper index in the NRange (GridBase.h:17-33) on the GPU.
  * mrange: GSHT_RANGE_ALL or GSHT_RANGE_NONNEGATIVE; nrange: any range;
- * forms: GSHT_FORM_* mask (FP64 is always built). */
+ * forms: GSHT_FORM_* mask (the FP64 table is built unless forms is exactly
+ * GSHT_FORM_RECURRENCE). */
 gsht_status gsht_grid_create(int lmax, int nmax, int mrange, int nrange,
                              unsigned forms, gsht_grid** grid);
 
