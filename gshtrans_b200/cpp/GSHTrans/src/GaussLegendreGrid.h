@@ -19,8 +19,15 @@
 namespace GSHTrans {
 
 // Legendre-stage precision of a grid's transforms (an extension of the
-// reference interface): FP64 is the drop-in default.
-enum class Precision { FP64 = GSHT_FP64, BF16x3 = GSHT_BF16X3, Ozaki = GSHT_OZAKI };
+// reference interface): FP64 is the drop-in default. Recurrence is FP64 with
+// no stored table: the grid keeps only the l-recurrence's start values and
+// coefficients, and the transforms generate the Wigner values as they go.
+enum class Precision {
+  FP64 = GSHT_FP64,
+  BF16x3 = GSHT_BF16X3,
+  Ozaki = GSHT_OZAKI,
+  Recurrence = GSHT_RECURRENCE
+};
 
 template <RealFloatingPoint _Real, OrderIndexRange _MRange, IndexRange _NRange>
 class GaussLegendreGrid : public GridBase<GaussLegendreGrid<_Real, _MRange, _NRange>> {
@@ -41,11 +48,13 @@ class GaussLegendreGrid : public GridBase<GaussLegendreGrid<_Real, _MRange, _NRa
   template <typename Flag = int>
   GaussLegendreGrid(int lMax, int nMax, Flag = Flag{}) : GaussLegendreGrid(lMax, nMax, Precision::FP64) {}
 
-  // Extension: also build the table form of a tensor-core precision.
+  // Extension: also build the table form of a tensor-core precision, or
+  // (Recurrence) no table at all.
   GaussLegendreGrid(int lMax, int nMax, Precision precision) : _lMax{lMax}, _nMax{nMax}, _prec{precision} {
     unsigned forms = GSHT_FORM_FP64;
     if (precision == Precision::BF16x3) forms |= GSHT_FORM_BF16X3;
     if (precision == Precision::Ozaki) forms |= GSHT_FORM_OZAKI;
+    if (precision == Precision::Recurrence) forms = GSHT_FORM_RECURRENCE;
     gsht_grid* g = nullptr;
     Backend::Check(gsht_grid_create(lMax, nMax, Backend::RangeCode<MRange>(),
                                     Backend::RangeCode<NRange>(), forms, &g));

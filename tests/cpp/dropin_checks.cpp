@@ -31,11 +31,11 @@ static std::mt19937_64 g_gen{20241203};
 static Int Uniform(Int a, Int b) { return std::uniform_int_distribution<Int>(a, b)(g_gen); }
 
 template <typename Scalar, typename MRange, typename NRange>
-double Coeff2Coeff(Int lMaxGrid, Int lMax) {
+double Coeff2Coeff(Int lMaxGrid, Int lMax, Precision prec = Precision::FP64) {
   using Complex = std::complex<double>;
   using Grid = GaussLegendreGrid<double, MRange, NRange>;
   const Int nMax = std::min<Int>(lMax, 4);
-  Grid grid{int(lMaxGrid), int(nMax)};
+  Grid grid{int(lMaxGrid), int(nMax), prec};
   const Int n = std::same_as<NRange, All> ? Uniform(-nMax, nMax) : Uniform(0, nMax);
   const Int size = RealFloatingPoint<Scalar> ? grid.RealCoefficientSize(lMax, n) : grid.ComplexCoefficientSize(lMax, n);
   std::vector<Complex> flm(size), glm(size);
@@ -154,6 +154,11 @@ int main() {
     Report("Coeff2Coeff R2C <NonNeg,NonNeg>" + tag, e < 1e-12, e);
     e = Coeff2Coeff<std::complex<double>, All, NonNegative>(lg, l);
     Report("Coeff2Coeff C2C <All,NonNeg>" + tag, e < 1e-12, e);
+    // Extension: a grid without a stored table (l-recurrence in the kernels).
+    e = Coeff2Coeff<std::complex<double>, All, All>(lg, l, Precision::Recurrence);
+    Report("Coeff2Coeff C2C <All,All> recurrence" + tag, e < 1e-12, e);
+    e = Coeff2Coeff<double, All, All>(lg, l, Precision::Recurrence);
+    Report("Coeff2Coeff R2C <All,All> recurrence" + tag, e < 1e-12, e);
   }
   std::uniform_real_distribution<double> angle(0.0, std::numbers::pi);
   for (int trial = 0; trial < 3; trial++) {
