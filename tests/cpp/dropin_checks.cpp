@@ -141,6 +141,30 @@ static void Fields() {
   Report("field -> forward -> inverse", e5 < 1e-13, e5);
 }
 
+// Expansions (the reference's CanonicalComponentExpansion container, here
+// wired to the transforms): coefficients -> field -> coefficients.
+template <typename Value>
+static double ExpansionRoundTrip(Int L) {
+  using Grid = GaussLegendreGrid<double, All, All>;
+  Grid grid(int(L), 2);
+  CanonicalComponentExpansion<1, Grid, Value> e(grid);
+  std::normal_distribution<double> nd;
+  for (auto [l, m] : e.Indices()) {
+    e[l, m] = {nd(g_gen), std::same_as<Value, RealValued> && m == 0 ? 0.0 : nd(g_gen)};
+  }
+  if constexpr (std::same_as<Value, ComplexValued>) e[L, L] = 0;  // alias of (L, -L)
+  else e[L, L] = e[L, L].real();
+  auto f = e.ToField();
+  CanonicalComponentExpansion<1, Grid, Value> back(f);
+  back -= e;
+  double err = 0, ref = 0;
+  for (auto [l, m] : e.Indices()) {
+    err = std::max(err, std::abs(back[l, m]));
+    ref = std::max(ref, std::abs(e[l, m]));
+  }
+  return err / ref;
+}
+
 int main() {
   for (int trial = 0; trial < 3; trial++) {
     const Int lg = Uniform(4, 256), l = Uniform(4, lg);
@@ -169,6 +193,12 @@ int main() {
     Report("addition theorem (FourPi, All, All)", e2 <= 1000 * std::numeric_limits<double>::epsilon(), e2);
   }
   Fields();
+  for (Int L : {31, 96}) {
+    const double ec = ExpansionRoundTrip<ComplexValued>(L);
+    Report("expansion -> field -> expansion (complex) L=" + std::to_string(L), ec < 1e-12, ec);
+    const double er = ExpansionRoundTrip<RealValued>(L);
+    Report("expansion -> field -> expansion (real) L=" + std::to_string(L), er < 1e-12, er);
+  }
   std::printf("%d failed\n", g_failures);
   return g_failures;
 }
