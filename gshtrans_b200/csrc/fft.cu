@@ -703,9 +703,10 @@ __global__ void __launch_bounds__(256) k_fft_forward_p2(
 // are free of bank conflicts (checked by enumeration of the quarter-warp
 // access sets).
 // ---------------------------------------------------------------------------
-template <int N>
+template <int N, int kPts>
 struct P3 {
-  static constexpr int kPoints = N > 4096 ? N : 4096;
+  static constexpr int kPoints = N > kPts ? N : kPts;
+  static constexpr int kThreads = kPoints / 16;
   static constexpr int R = kPoints / N;
   static constexpr int RS = N + N / 16 + (R > 8 ? 1 : (R > 1 ? 8 / R : 0));
   static constexpr int kSmem = R * RS;  // double2 units
@@ -755,7 +756,7 @@ __device__ __forceinline__ void p3_twiddle(double2 (&v)[P], const double2* __res
 }
 
 // Middle stages (every stage after the first and before the last), in place.
-template <int N, int M>
+template <int N, int kPts, int M>
 __device__ __forceinline__ void p3_middle(double2* buf, const double2* __restrict__ tw,
                                           int twStride, int sign) {
   constexpr int P = P3Radix<N, M>::P;
@@ -766,25 +767,25 @@ __device__ __forceinline__ void p3_middle(double2* buf, const double2* __restric
     double2 v[NB][P];
 #pragma unroll
     for (int b = 0; b < NB; b++) {
-      const int g = threadIdx.x + b * 256;
+      const int g = threadIdx.x + b * P3<N, kPts>::kThreads;
       const int ring = g >> ilog2(NBR), bi = g & (NBR - 1);
       const int j = bi >> ilog2(M), k = bi & (M - 1);
 #pragma unroll
-      for (int q = 0; q < P; q++) v[b][q] = buf[P3<N>::at(ring, k + j * M + q * L * M)];
+      for (int q = 0; q < P; q++) v[b][q] = buf[P3<N, kPts>::at(ring, k + j * M + q * L * M)];
     }
     __syncthreads();
 #pragma unroll
     for (int b = 0; b < NB; b++) {
-      const int g = threadIdx.x + b * 256;
+      const int g = threadIdx.x + b * P3<N, kPts>::kThreads;
       const int ring = g >> ilog2(NBR), bi = g & (NBR - 1);
       const int j = bi >> ilog2(M), k = bi & (M - 1);
       dft_reg<P>(v[b], sign);
       p3_twiddle<P>(v[b], tw, j * M, twStride, sign);
 #pragma unroll
-      for (int r = 0; r < P; r++) buf[P3<N>::at(ring, k + j * P * M + r * M)] = v[b][r];
+      for (int r = 0; r < P; r++) buf[P3<N, kPts>::at(ring, k + j * P * M + r * M)] = v[b][r];
     }
     __syncthreads();
-    p3_middle<N, M * P>(buf, tw, twStride, sign);
+    p3_middle<N, kPts, M * P>(buf, tw, twStride, sign);
   }
 }
 
@@ -805,8 +806,8 @@ constexpr int kSpecBox = 64;
 // the strided 16R-byte row segments cost no load instructions or registers;
 // the first stage reads them from shared memory. Without kTma the first
 // stage loads them from global memory directly.
-template <bool kReal, int N, bool kTma>
-__global__ void __launch_bounds__(256, 2) k_fft_inverse_p3(
+template <bool kReal, int N, bool kTma, int kPts>
+__global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
     const __grid_constant__ CUtensorMap specMap, int L, int lmax, int nTheta, int thetaPad,
     int count, const double2* __restrict__ spec, const double2* __restrict__ tw,
     double* __restrict__ out, int* err, int smemElems) {
@@ -816,7 +817,7 @@ __global__ void __launch_bounds__(256, 2) k_fft_inverse_p3(
   double2* smem = reinterpret_cast<double2*>(
       (reinterpret_cast<uintptr_t>(p3_raw) + 127) & ~uintptr_t(127));
   uint64_t& bar = *reinterpret_cast<uint64_t*>(smem + smemElems);
-  constexpr int R = P3<N>::R;
+  constexpr int R = P3<N, kPts>::R;
   const int j0 = blockIdx.x * R, f = blockIdx.y;
   const int nPhi = 2 * L;
   const int sgnCount = kReal ? 1 : 2;
@@ -882,10 +883,10 @@ __global__ void __launch_bounds__(256, 2) k_fft_inverse_p3(
     dft_reg<16>(v, +1);
     p3_twiddle<16>(v, tw, jj, twStride, +1);
 #pragma unroll
-    for (int q = 0; q < 16; q++) smem[P3<N>::at(r, jj * 16 + q)] = v[q];
+    for (int q = 0; q < 16; q++) smem[P3<N, kPts>::at(r, jj * 16 + q)] = v[q];
   }
   __syncthreads();
-  p3_middle<N, 16>(smem, tw, twStride, +1);
+  p3_middle<N, kPts, 16>(smem, tw, twStride, +1);
   // Last stage (L = 1, no twiddles), ring-major so that lanes write
   // consecutive longitudes.
   constexpr int M = p3_last_m<N>();
@@ -893,11 +894,11 @@ __global__ void __launch_bounds__(256, 2) k_fft_inverse_p3(
   constexpr int NB = 16 / P;
 #pragma unroll
   for (int b = 0; b < NB; b++) {
-    const int g = threadIdx.x + b * 256;
+    const int g = threadIdx.x + b * P3<N, kPts>::kThreads;
     const int ring = g >> ilog2(M), k = g & (M - 1);
     double2 v[P];
 #pragma unroll
-    for (int q = 0; q < P; q++) v[q] = smem[P3<N>::at(ring, k + q * M)];
+    for (int q = 0; q < P; q++) v[q] = smem[P3<N, kPts>::at(ring, k + q * M)];
     dft_reg<P>(v, +1);
     const int th = j0 + ring;
     if (th < nTheta) {
@@ -909,13 +910,13 @@ __global__ void __launch_bounds__(256, 2) k_fft_inverse_p3(
   }
 }
 
-template <bool kReal, int N>
-__global__ void __launch_bounds__(256, 2) k_fft_forward_p3(
+template <bool kReal, int N, int kPts>
+__global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
     int L, int lmax, int nTheta, int thetaPad, int count, const double* __restrict__ in,
     const double* __restrict__ weight, const double2* __restrict__ tw,
     double2* __restrict__ spec) {
   extern __shared__ double2 smem[];
-  constexpr int R = P3<N>::R;
+  constexpr int R = P3<N, kPts>::R;
   const int j0 = blockIdx.x * R, f = blockIdx.y;
   const int nPhi = 2 * L;
   const int sgnCount = kReal ? 1 : 2;
@@ -925,7 +926,7 @@ __global__ void __launch_bounds__(256, 2) k_fft_forward_p3(
   };
   if (j0 <= nTheta - 1 && nTheta - 1 < j0 + R) {
     const int padW = thetaPad - nTheta;
-    for (int i = threadIdx.x; i < (lmax + 1) * sgnCount * padW; i += 256) {
+    for (int i = threadIdx.x; i < (lmax + 1) * sgnCount * padW; i += P3<N, kPts>::kThreads) {
       const int q = i / padW, jj = nTheta + (i - q * padW);
       S(q / sgnCount, q % sgnCount, jj) = make_double2(0.0, 0.0);
     }
@@ -943,10 +944,10 @@ __global__ void __launch_bounds__(256, 2) k_fft_forward_p3(
     dft_reg<16>(v, -1);
     p3_twiddle<16>(v, tw, jj, twStride, -1);
 #pragma unroll
-    for (int q = 0; q < 16; q++) smem[P3<N>::at(ring, jj * 16 + q)] = v[q];
+    for (int q = 0; q < 16; q++) smem[P3<N, kPts>::at(ring, jj * 16 + q)] = v[q];
   }
   __syncthreads();
-  p3_middle<N, 16>(smem, tw, twStride, -1);
+  p3_middle<N, kPts, 16>(smem, tw, twStride, -1);
   constexpr int M = p3_last_m<N>();
   constexpr int P = N / M;
   constexpr int NB = 16 / P;
@@ -956,11 +957,11 @@ __global__ void __launch_bounds__(256, 2) k_fft_forward_p3(
     // consecutive colatitudes of one spectral row.
 #pragma unroll
     for (int b = 0; b < NB; b++) {
-      const int g = threadIdx.x + b * 256;
+      const int g = threadIdx.x + b * P3<N, kPts>::kThreads;
       const int ring = g & (R - 1), k = g >> ilog2(R);
       double2 v[P];
 #pragma unroll
-      for (int q = 0; q < P; q++) v[q] = smem[P3<N>::at(ring, k + q * M)];
+      for (int q = 0; q < P; q++) v[q] = smem[P3<N, kPts>::at(ring, k + q * M)];
       dft_reg<P>(v, -1);
       const int th = j0 + ring;
       if (th < nTheta) {
@@ -979,31 +980,31 @@ __global__ void __launch_bounds__(256, 2) k_fft_forward_p3(
     double2 v[NB][P];
 #pragma unroll
     for (int b = 0; b < NB; b++) {
-      const int g = threadIdx.x + b * 256;
+      const int g = threadIdx.x + b * P3<N, kPts>::kThreads;
       const int ring = g >> ilog2(M), k = g & (M - 1);
 #pragma unroll
-      for (int q = 0; q < P; q++) v[b][q] = smem[P3<N>::at(ring, k + q * M)];
+      for (int q = 0; q < P; q++) v[b][q] = smem[P3<N, kPts>::at(ring, k + q * M)];
     }
     __syncthreads();
 #pragma unroll
     for (int b = 0; b < NB; b++) {
-      const int g = threadIdx.x + b * 256;
+      const int g = threadIdx.x + b * P3<N, kPts>::kThreads;
       const int ring = g >> ilog2(M), k = g & (M - 1);
       dft_reg<P>(v[b], -1);
 #pragma unroll
-      for (int r = 0; r < P; r++) smem[P3<N>::at(ring, k + r * M)] = v[b][r];
+      for (int r = 0; r < P; r++) smem[P3<N, kPts>::at(ring, k + r * M)] = v[b][r];
     }
     __syncthreads();
     // Real field: unpack the half-length transform, X(m) from z(m) and
     // conj z(M - m), M = nPhi / 2.
-    for (int e = threadIdx.x; e < R * (lmax + 1); e += 256) {
+    for (int e = threadIdx.x; e < R * (lmax + 1); e += P3<N, kPts>::kThreads) {
       const int r = e & (R - 1), m = e >> ilog2(R);
       const int th = j0 + r;
       if (th >= nTheta) continue;
       const double scale = weight[th] * twoPiOverN;
       const int Mh = L;
-      const double2 z0 = smem[P3<N>::at(r, m == Mh ? 0 : m)];
-      const double2 zc = cconj(smem[P3<N>::at(r, m == 0 ? 0 : Mh - m)]);
+      const double2 z0 = smem[P3<N, kPts>::at(r, m == Mh ? 0 : m)];
+      const double2 zc = cconj(smem[P3<N, kPts>::at(r, m == 0 ? 0 : Mh - m)]);
       const double2 w = twiddle(tw, m, 1, -1);
       const double2 ev = cscale(cadd(z0, zc), 0.5);
       const double2 od = cscale(cmul_si(csub(z0, zc), -1), 0.5);
@@ -1028,11 +1029,12 @@ bool spec_map(CUtensorMap* map, double* spec, int thetaPad, int count, int sgnCo
             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int N>
-gsht_status launch_p3(const gsht_grid* g, int dir, int lmax, int is_real, int count,
-                      const double* src, double* dst, cudaStream_t s) {
-  size_t shmem = sizeof(double2) * P3<N>::kSmem;
-  constexpr int R = P3<N>::R;
+template <int N, int kPts>
+gsht_status launch_p3_dir(const gsht_grid* g, int dir, int lmax, int is_real, int count,
+                          const double* src, double* dst, cudaStream_t s) {
+  constexpr int kThr = P3<N, kPts>::kThreads;
+  size_t shmem = sizeof(double2) * P3<N, kPts>::kSmem;
+  constexpr int R = P3<N, kPts>::R;
   dim3 grid((g->n_theta + R - 1) / R, count);
   const double2* tw = reinterpret_cast<const double2*>(g->d_twiddle);
   if (dir == 1) {
@@ -1041,33 +1043,52 @@ gsht_status launch_p3(const gsht_grid* g, int dir, int lmax, int is_real, int co
     const size_t staged =
         sizeof(double2) * sgnCount * (size_t)((lmax + kSpecBox) / kSpecBox) * kSpecBox * R;
     CUtensorMap map{};
-    const bool tma = staged <= 110 * 1024 &&
+    const bool tma = staged <= (shmem > 110 * 1024 ? shmem : 110 * 1024) &&
                      spec_map(&map, const_cast<double*>(src), g->theta_pad, count, sgnCount, lmax, R);
     if (tma) shmem = shmem > staged ? shmem : staged;
     const int smemElems = (int)(shmem / sizeof(double2));
     shmem += 128 + 16;
     if (tma) {
-      auto k = is_real ? k_fft_inverse_p3<true, N, true> : k_fft_inverse_p3<false, N, true>;
+      auto k = is_real ? k_fft_inverse_p3<true, N, true, kPts> : k_fft_inverse_p3<false, N, true, kPts>;
       GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
-      k<<<grid, 256, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count,
+      k<<<grid, kThr, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count,
                                  reinterpret_cast<const double2*>(src), tw, dst, g->d_err,
                                  smemElems);
     } else {
-      auto k = is_real ? k_fft_inverse_p3<true, N, false> : k_fft_inverse_p3<false, N, false>;
+      auto k = is_real ? k_fft_inverse_p3<true, N, false, kPts> : k_fft_inverse_p3<false, N, false, kPts>;
       GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
-      k<<<grid, 256, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count,
+      k<<<grid, kThr, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count,
                                  reinterpret_cast<const double2*>(src), tw, dst, g->d_err,
                                  smemElems);
     }
     GSHT_LAUNCH_CHECK("k_fft_inverse_p3");
   } else {
-    auto k = is_real ? k_fft_forward_p3<true, N> : k_fft_forward_p3<false, N>;
+    auto k = is_real ? k_fft_forward_p3<true, N, kPts> : k_fft_forward_p3<false, N, kPts>;
     GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
-    k<<<grid, 256, shmem, s>>>(g->L, lmax, g->n_theta, g->theta_pad, count, src, g->d_weight,
+    k<<<grid, kThr, shmem, s>>>(g->L, lmax, g->n_theta, g->theta_pad, count, src, g->d_weight,
                                tw, reinterpret_cast<double2*>(dst));
     GSHT_LAUNCH_CHECK("k_fft_forward_p3");
   }
   return GSHT_OK;
+}
+
+// Points per block of the three-pass kernels for ring length N: 4096 (two
+// blocks of 256 threads per SM), except the forward at N = 2048, whose
+// spectral rows are written 4 colatitudes (64 B) at a time from 8192-point
+// blocks of 512 threads (1.07 against 1.19 ms at lmax 1024, 64 fields).
+// Measured and not kept: 2048-point blocks (one ring, 16 B row segments)
+// ran 2x slower at N = 2048; 8192-point blocks made the inverse at N = 2048
+// (1.30 ms) and both directions at N = 1024 slower.
+template <int N, bool kForward>
+constexpr int p3_points() {
+  return (kForward && N == 2048) ? 8192 : 4096;
+}
+
+template <int N>
+gsht_status launch_p3(const gsht_grid* g, int dir, int lmax, int is_real, int count,
+                      const double* src, double* dst, cudaStream_t s) {
+  if (dir == 0) return launch_p3_dir<N, p3_points<N, true>()>(g, dir, lmax, is_real, count, src, dst, s);
+  return launch_p3_dir<N, p3_points<N, false>()>(g, dir, lmax, is_real, count, src, dst, s);
 }
 
 template <int N>
