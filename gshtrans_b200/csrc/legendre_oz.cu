@@ -260,30 +260,63 @@ __global__ void __launch_bounds__(kThreads, 1)
 // Field-side slicing: one warp per (m, complex row q) handles the re and im
 // real rows 2q, 2q+1: row maxima -> exponents -> 7 truncation slices.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double warp_max(double v) {
-  for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
+
+
+// frexp exponent of x (|x| = f 2^e, f in [0.5, 1)) read from its bits;
+// kNoExp for zero. Subnormals included.
+constexpr int kNoExp = -100000;
+__device__ __forceinline__ int exp_of(double x) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  const int eb = (int)((b >> 52) & 0x7FF);
+  if (eb != 0) return eb - 1022;
+  const unsigned long long mant = b & ((1ull << 52) - 1);
+  return mant == 0 ? kNoExp : -1010 - __clzll((long long)mant);
 }
 
+// floor(|x| 2^(sc + 49)) for |x| 2^sc < 1, from the bits of x: the 49 bits
+// of y = x 2^sc that seven 7-bit slices keep, exactly (no rounding, so the
+// same digits as truncating y * 128 seven times).
+__device__ __forceinline__ unsigned long long digits49(double x, int sc) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  const int eb = (int)((b >> 52) & 0x7FF);
+  unsigned long long m = b & ((1ull << 52) - 1);
+  int e = 1;
+  if (eb != 0) {
+    m |= 1ull << 52;
+    e = eb;
+  }
+  const int sh = 1026 - e - sc;  // |x| 2^(sc+49) = m 2^(e + sc - 1026)
+  return sh >= 64 ? 0ull : (sh <= 0 ? 0ull : m >> sh);
+}
 
-// Four values -> seven slice quads, s-th quad to dst + s * plane (4-byte
-// aligned): y is split into seven signed 7-bit truncation slices, y =
-// sum_s S_s 2^{-7(s+1)} (|y| < 1).
-__device__ __forceinline__ void write_slices4(const double (&y0)[4], int8_t* dst, size_t plane) {
-  double y[4] = {y0[0], y0[1], y0[2], y0[3]};
+// Four values y_t = x_t 2^{sc_t} (|y_t| < 1) -> seven slice quads, s-th quad
+// to dst + s * plane (4-byte aligned): y = sum_s S_s 2^{-7(s+1)} with signed
+// 7-bit truncation digits S_s, taken from the integer floor(|y| 2^49).
+__device__ __forceinline__ void write_slices4(const double (&x)[4], const int (&sc)[4],
+                                              int8_t* dst, size_t plane) {
+  unsigned long long Y[4];
+  bool neg[4];
+#pragma unroll
+  for (int t = 0; t < 4; t++) {
+    Y[t] = digits49(x[t], sc[t]);
+    neg[t] = x[t] < 0.0;
+  }
 #pragma unroll
   for (int s = 0; s < kS; s++) {
-    char4 c;
-    int8_t* cc = reinterpret_cast<int8_t*>(&c);
+    unsigned int w = 0;
 #pragma unroll
     for (int t = 0; t < 4; t++) {
-      y[t] *= 128.0;
-      const double q = trunc(y[t]);
-      y[t] -= q;
-      cc[t] = (int8_t)q;
+      int d = (int)((Y[t] >> (42 - 7 * s)) & 127u);
+      if (neg[t]) d = -d;
+      w |= ((unsigned int)d & 0xFFu) << (8 * t);
     }
-    *reinterpret_cast<char4*>(dst + s * plane) = c;
+    *reinterpret_cast<unsigned int*>(dst + s * plane) = w;
   }
+}
+
+__device__ __forceinline__ int warp_max_int(int v) {
+  for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
 }
 
 // Inverse: packed coefficients -> slices over degrees, K pitch `pitch` (a
@@ -312,32 +345,34 @@ __global__ void k_prep_inverse_oz(int lmax, int n, int na, int count, int Q, int
     }
     return v;
   };
-  double mre = 0.0, mim = 0.0;
+  // Row exponents: the frexp exponent of each row's largest magnitude (0
+  // for an all-zero row), from the exponent bits.
+  int ere = kNoExp, eim = kNoExp;
   for (int k = lane; k < keff; k += 32) {
     const double2 v = value(k);
-    mre = fmax(mre, fabs(v.x));
-    mim = fmax(mim, fabs(v.y));
+    ere = max(ere, exp_of(v.x));
+    eim = max(eim, exp_of(v.y));
   }
-  mre = warp_max(mre);
-  mim = warp_max(mim);
-  int ere = 0, eim = 0;
-  if (mre > 0.0) frexp(mre, &ere);
-  if (mim > 0.0) frexp(mim, &eim);
+  ere = warp_max_int(ere);
+  eim = warp_max_int(eim);
+  if (ere == kNoExp) ere = 0;
+  if (eim == kNoExp) eim = 0;
   const size_t r0 = ((size_t)m * R + 2 * q) * pitch;
   if (lane == 0) {
     rowExp[(size_t)m * R + 2 * q] = ere;
     rowExp[(size_t)m * R + 2 * q + 1] = eim;
   }
+  const int sre[4] = {-ere, -ere, -ere, -ere}, sim[4] = {-eim, -eim, -eim, -eim};
   for (int k4 = 4 * lane; k4 < kp; k4 += 128) {
     double re[4], im[4];
 #pragma unroll
     for (int t = 0; t < 4; t++) {
       const double2 v = value(k4 + t);
-      re[t] = ldexp(v.x, -ere);
-      im[t] = ldexp(v.y, -eim);
+      re[t] = v.x;
+      im[t] = v.y;
     }
-    write_slices4(re, op + r0 + k4, plane);
-    write_slices4(im, op + r0 + pitch + k4, plane);
+    write_slices4(re, sre, op + r0 + k4, plane);
+    write_slices4(im, sim, op + r0 + pitch + k4, plane);
   }
 }
 
@@ -355,22 +390,24 @@ __global__ void k_prep_forward_oz(int lmax, int Q, int R, int thetaPad, size_t p
   const double2* row = spec + ((size_t)m * Q + q) * thetaPad;
   const int4* te4 = reinterpret_cast<const int4*>(tabExp + (size_t)m * thetaPad);
   const int nq = thetaPad / 4;
-  double mre = 0.0, mim = 0.0;
+  // Row exponents of the column-scaled values x 2^{e_j}: the largest
+  // exp(x) + e_j (0 for an all-zero row).
+  int ere = kNoExp, eim = kNoExp;
   for (int j4 = lane; j4 < nq; j4 += 32) {
     const int4 e = te4[j4];
     const int ev[4] = {e.x, e.y, e.z, e.w};
 #pragma unroll
     for (int t = 0; t < 4; t++) {
       const double2 v = row[4 * j4 + t];
-      mre = fmax(mre, fabs(ldexp(v.x, ev[t])));
-      mim = fmax(mim, fabs(ldexp(v.y, ev[t])));
+      const int xr = exp_of(v.x), xi = exp_of(v.y);
+      if (xr != kNoExp) ere = max(ere, xr + ev[t]);
+      if (xi != kNoExp) eim = max(eim, xi + ev[t]);
     }
   }
-  mre = warp_max(mre);
-  mim = warp_max(mim);
-  int ere = 0, eim = 0;
-  if (mre > 0.0) frexp(mre, &ere);
-  if (mim > 0.0) frexp(mim, &eim);
+  ere = warp_max_int(ere);
+  eim = warp_max_int(eim);
+  if (ere == kNoExp) ere = 0;
+  if (eim == kNoExp) eim = 0;
   if (lane == 0) {
     rowExp[(size_t)m * R + 2 * q] = ere;
     rowExp[(size_t)m * R + 2 * q + 1] = eim;
@@ -380,14 +417,17 @@ __global__ void k_prep_forward_oz(int lmax, int Q, int R, int thetaPad, size_t p
     const int4 e = te4[j4];
     const int ev[4] = {e.x, e.y, e.z, e.w};
     double re[4], im[4];
+    int sre[4], sim[4];
 #pragma unroll
     for (int t = 0; t < 4; t++) {
       const double2 v = row[4 * j4 + t];
-      re[t] = ldexp(v.x, ev[t] - ere);
-      im[t] = ldexp(v.y, ev[t] - eim);
+      re[t] = v.x;
+      im[t] = v.y;
+      sre[t] = ev[t] - ere;
+      sim[t] = ev[t] - eim;
     }
-    write_slices4(re, op + r0 + 4 * j4, plane);
-    write_slices4(im, op + r0 + thetaPad + 4 * j4, plane);
+    write_slices4(re, sre, op + r0 + 4 * j4, plane);
+    write_slices4(im, sim, op + r0 + thetaPad + 4 * j4, plane);
   }
 }
 
