@@ -211,8 +211,9 @@ size_t oz_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, in
 gsht_status legendre_inverse_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
                                 int count, const double* coef, void* operand, double* spec,
                                 cudaStream_t s);
+// The spectra buffer is reused for the kernel's result rows.
 gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
-                                int count, const double* spec, void* operand, double* coef,
+                                int count, double* spec, void* operand, double* coef,
                                 cudaStream_t s);
 // Legendre stage, FP64 with the Wigner values generated by the l-recurrence
 // inside the contraction (legendre_rec.cu); no stored table.

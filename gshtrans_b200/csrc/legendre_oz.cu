@@ -212,54 +212,17 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (tileRow >= rowsM) continue;
       const int eA = kDir == 0 ? p.tabExp[(size_t)m * p.thetaPad + tileRow] : 0;
       const int q0 = (tl.z * kN + group * kCols) / 2;
-      if (kDir == 0) {
+      // Both directions write order-major rows [m][q][row] (row = colatitude
+      // for the inverse, degree offset l - l0 for the forward, whose rows
+      // k_accumulate_forward then adds into the packed coefficients).
 #pragma unroll
-        for (int i = 0; i < kCols / 2; i++) {
-          const int q = q0 + i;
-          if (q >= p.Q) break;
-          const int ere = p.rowExp[(size_t)m * p.R + 2 * q];
-          const int eim = p.rowExp[(size_t)m * p.R + 2 * q + 1];
-          p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
-              make_double2(ldexp(acc[2 * i], eA + ere), ldexp(acc[2 * i + 1], eA + eim));
-        }
-      } else {
-        const int l = l0 + tileRow;
-#pragma unroll
-        for (int b0 = 0; b0 < kCols / 2; b0 += 4) {
-          double2* ptr[4];
-          double2 old[4];
-#pragma unroll
-          for (int i = 0; i < 4; i++) {
-            const int q = q0 + b0 + i;
-            ptr[i] = nullptr;
-            if (q >= p.Q) continue;
-            const int sgn = q / p.count, f = q - sgn * p.count;
-            if (sgn == 1 && m == 0) continue;
-            const long idx = p.isReal
-                                 ? (long)l * (l + 1) / 2 - (long)p.na * (p.na + 1) / 2 + m
-                                 : (long)l * l - (long)p.n * p.n + l + (sgn ? -m : m);
-            ptr[i] = p.out + (size_t)f * p.coefSize + idx;
-          }
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-            if (ptr[i]) old[i] = *ptr[i];
-#pragma unroll
-          for (int i = 0; i < 4; i++) {
-            if (!ptr[i]) continue;
-            const int q = q0 + b0 + i;
-            const int sgn = q / p.count;
-            const int ere = p.rowExp[(size_t)m * p.R + 2 * q];
-            const int eim = p.rowExp[(size_t)m * p.R + 2 * q + 1];
-            double2 val = make_double2(ldexp(acc[2 * (b0 + i)], ere),
-                                       ldexp(acc[2 * (b0 + i) + 1], eim));
-            if (sgn == 1 && ((l + p.n) & 1)) val = make_double2(-val.x, -val.y);
-            if (!p.isReal && sgn == 0 && m == p.L && l == p.L && p.lmax == p.L) {
-              *ptr[i] = make_double2(0.0, 0.0);  // GaussLegendreGrid.h:209-215
-            } else {
-              *ptr[i] = make_double2(old[i].x + val.x, old[i].y + val.y);
-            }
-          }
-        }
+      for (int i = 0; i < kCols / 2; i++) {
+        const int q = q0 + i;
+        if (q >= p.Q) break;
+        const int ere = p.rowExp[(size_t)m * p.R + 2 * q];
+        const int eim = p.rowExp[(size_t)m * p.R + 2 * q + 1];
+        p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
+            make_double2(ldexp(acc[2 * i], eA + ere), ldexp(acc[2 * i + 1], eA + eim));
       }
     }
   }
@@ -525,7 +488,7 @@ gsht_status legendre_inverse_oz(const gsht_grid* g, const Table* t, int lmax, in
 }
 
 gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
-                                int count, const double* spec, void* operand, double* coef,
+                                int count, double* spec, void* operand, double* coef,
                                 cudaStream_t s) {
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
@@ -552,10 +515,14 @@ gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, in
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count; a.Q = Q; a.R = R;
   a.nTheta = g->n_theta; a.thetaPad = tp; a.isReal = is_real;
   a.rowOff = t->d_row_off; a.tabExp = t->i8_exp; a.rowExp = rowExp;
-  a.out = reinterpret_cast<double2*>(coef);
+  // The spectra, sliced above, are no longer needed: the kernel's result rows
+  // go into their buffer and are then added into the coefficients.
+  a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
-  return launch_oz<1>(g, a, mapA, mapB, s);
+  st = launch_oz<1>(g, a, mapA, mapB, s);
+  if (st != GSHT_OK) return st;
+  return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, tp, spec, coef, s);
 }
 
 }  // namespace gsht
