@@ -55,6 +55,14 @@ struct OzArgs {
 constexpr int kEpiWarps = 8;  // two warps per TMEM lane quarter, one column group each
 constexpr int kThreads = 32 * (2 + kEpiWarps);
 
+// Exact INT32 -> FP64 on the FP64 pipe: the double with high word 0x43300000
+// and low word v + 2^31 is 2^52 + v + 2^31. Same value as a conversion
+// instruction, without its lower-throughput pipe (the epilogue converts 7 x
+// 32 accumulators per thread per tile).
+__device__ __forceinline__ double i32_to_f64(uint32_t v) {
+  return __hiloint2double(0x43300000, (int)(v ^ 0x80000000u)) - 4503601774854144.0;
+}
+
 // Persistent kernel over the tile list (see legendre_tc.cu for the protocol):
 // the epilogue sums the 7 diagonal accumulators of its 32 columns in FP64,
 // releases TMEM, then writes.
@@ -198,8 +206,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         tmem_wait_ld();
 #pragma unroll
         for (int i = 0; i < 16; i++) {
-          acc[i] = fma((double)(int)v0[i], w, acc[i]);
-          acc[16 + i] = fma((double)(int)v1[i], w, acc[16 + i]);
+          acc[i] = fma(i32_to_f64(v0[i]), w, acc[i]);
+          acc[16 + i] = fma(i32_to_f64(v1[i]), w, acc[16 + i]);
         }
       }
       tc_fence_before();
