@@ -187,7 +187,7 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
   // upload of chunk i+1, the transform of chunk i and the download of chunk
   // i-1 overlap (PCIe carries both directions at once). At most kMaxChunks
   // chunks of at least kMinChunkBytes of transfers each.
-  constexpr int kMaxChunks = 8;
+  constexpr int kMaxChunks = 16;
   constexpr size_t kMinChunkBytes = size_t(64) << 20;
   const size_t inField = inBytes / count, outField = outBytes / count;
   int chunk = count;
