@@ -237,15 +237,20 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
       return GSHT_OK;
     }
     double* spec = reinterpret_cast<double*>(ws + oSpec);
+    // The BF16x3 form (~1e-6) keeps its spectra in FP32 where the three-pass
+    // ring FFTs run: half the bytes through the FFT, the Legendre epilogue
+    // and the operand preparation, at ~3e-8 of rounding.
+    const bool spec32 = precision == GSHT_BF16X3 && fft_spec32_supported(g, is_real);
     gsht_status r;
     if (dir == 0) {
       {
         StageTimer tm(GSHT_STAGE_FFT_FORWARD, s);
-        r = fft_forward(g, lmax, is_real, c, dI, spec, s);
+        r = spec32 ? fft_forward32(g, lmax, is_real, c, dI, reinterpret_cast<float*>(spec), s)
+                   : fft_forward(g, lmax, is_real, c, dI, spec, s);
       }
       if (r != GSHT_OK) return r;
       if (precision == GSHT_BF16X3)
-        return legendre_forward_bf16(g, t, lmax, is_real, c, spec, ws + oOp, dO, ntile, s);
+        return legendre_forward_bf16(g, t, lmax, is_real, c, spec, ws + oOp, dO, ntile, s, spec32);
       if (precision == GSHT_OZAKI)
         return legendre_forward_oz(g, t, lmax, is_real, c, spec, ws + oOp, dO, s);
       if (rec) return legendre_forward_rec(g, t, lmax, is_real, c, spec, ws + oOp, dO, s);
@@ -253,7 +258,7 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
       return legendre_forward_fp64(g, t, lmax, is_real, c, spec, dO, s);
     }
     if (precision == GSHT_BF16X3)
-      r = legendre_inverse_bf16(g, t, lmax, is_real, c, dI, ws + oOp, spec, ntile, s);
+      r = legendre_inverse_bf16(g, t, lmax, is_real, c, dI, ws + oOp, spec, ntile, s, spec32);
     else if (precision == GSHT_OZAKI)
       r = legendre_inverse_oz(g, t, lmax, is_real, c, dI, ws + oOp, spec, s);
     else if (rec)
@@ -264,7 +269,8 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
                                 spec, s);
     if (r != GSHT_OK) return r;
     StageTimer tm(GSHT_STAGE_FFT_INVERSE, s);
-    return fft_inverse(g, lmax, is_real, c, spec, dO, s);
+    return spec32 ? fft_inverse32(g, lmax, is_real, c, reinterpret_cast<const float*>(spec), dO, s)
+                  : fft_inverse(g, lmax, is_real, c, spec, dO, s);
   };
 
   if (nChunks == 1) {

@@ -20,6 +20,7 @@
 // Real fields use the half-length complex FFT with the standard pre/post
 // twiddle (pack even/odd samples as real/imaginary parts).
 #include <cstring>
+#include <type_traits>
 
 #include "gsht_internal.cuh"
 #include "tc_common.cuh"
@@ -51,6 +52,17 @@ FftPlan make_plan(int n, int tableLen) {
 }
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+// Spectral buffer elements: FP64 (double2) or FP32 (float2) complex.
+__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.y); }
+template <typename T>
+__device__ __forceinline__ T from_d2(double2 v);
+template <>
+__device__ __forceinline__ double2 from_d2<double2>(double2 v) { return v; }
+template <>
+__device__ __forceinline__ float2 from_d2<float2>(double2 v) {
+  return make_float2((float)v.x, (float)v.y);
+}
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
@@ -806,11 +818,17 @@ constexpr int kSpecBox = 64;
 // the strided 16R-byte row segments cost no load instructions or registers;
 // the first stage reads them from shared memory. Without kTma the first
 // stage loads them from global memory directly.
-template <bool kReal, int N, bool kTma, int kPts>
+//
+// SpecT: double2 (the FP64 layout above) or float2, the spectra of the
+// BF16x3 form, which keeps its -m rows at their own colatitudes (no mirror:
+// the Legendre epilogue and operand preparation of that form apply it), so
+// both signs' TMA boxes start at colatitude j0.
+template <bool kReal, int N, bool kTma, int kPts, typename SpecT>
 __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
     const __grid_constant__ CUtensorMap specMap, int L, int lmax, int nTheta, int thetaPad,
-    int count, const double2* __restrict__ spec, const double2* __restrict__ tw,
+    int count, const SpecT* __restrict__ spec, const double2* __restrict__ tw,
     double* __restrict__ out, int* err, int smemElems) {
+  constexpr bool kMir = std::is_same<SpecT, double2>::value;
   // TMA destinations want 128-byte alignment: round the dynamic base up (the
   // launch adds 128 bytes of slack plus the barrier word after the buffer).
   extern __shared__ unsigned char p3_raw[];
@@ -824,8 +842,9 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
   const int twStride = nPhi / N;
   const int nbox = (lmax + 1 + kSpecBox - 1) / kSpecBox;
   const int M1 = nbox * kSpecBox;  // staged rows per sign
+  SpecT* staged = reinterpret_cast<SpecT*>(smem);
   auto S = [&](int m, int sgn, int jj) {
-    return spec[((size_t)(m * sgnCount + sgn) * count + f) * thetaPad + jj];
+    return to_d2(spec[((size_t)(m * sgnCount + sgn) * count + f) * thetaPad + jj]);
   };
   if constexpr (kTma) {
     if (threadIdx.x == 0) {
@@ -835,13 +854,14 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
     __syncthreads();
     if (threadIdx.x == 0) {
       tc::prefetch_tmap(&specMap);
-      tc::mbar_arrive_expect_tx(&bar, (uint32_t)(sgnCount * M1 * R * sizeof(double2)));
+      tc::mbar_arrive_expect_tx(&bar, (uint32_t)(sgnCount * M1 * R * sizeof(SpecT)));
       for (int sg = 0; sg < sgnCount; sg++) {
-        // Colatitudes j0.. (sign 0) or their mirror images nTheta-j0-R.. (sign 1).
-        const int x = 2 * (sg == 0 ? j0 : nTheta - j0 - R);
+        // Colatitudes j0.. (sign 0, and sign 1 without mirror) or their mirror
+        // images nTheta-j0-R.. (sign 1, FP64 layout).
+        const int x = 2 * ((sg == 0 || !kMir) ? j0 : nTheta - j0 - R);
         for (int b = 0; b < nbox; b++)
-          tc::tma_load_4d(smem + (size_t)(sg * M1 + b * kSpecBox) * R, &specMap, &bar, x, f, sg,
-                          b * kSpecBox);
+          tc::tma_load_4d(staged + (size_t)(sg * M1 + b * kSpecBox) * R, &specMap, &bar, x, f,
+                          sg, b * kSpecBox);
       }
     }
     tc::mbar_wait(&bar, 0, err, 21);
@@ -855,7 +875,8 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
     // Row m of sign sg (staged): colatitude j0 + r is element r, its mirror
     // nTheta-1-(j0+r) element R-1-r.
     auto T = [&](int m, int sg) {
-      return sg == 0 ? smem[(size_t)m * R + r] : smem[(size_t)(M1 + m) * R + (R - 1 - r)];
+      return to_d2(sg == 0 ? staged[(size_t)m * R + r]
+                           : staged[(size_t)(M1 + m) * R + (kMir ? R - 1 - r : r)]);
     };
 #pragma unroll
     for (int q = 0; q < 16; q++) {
@@ -865,7 +886,7 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
         if (!kReal) {
           if (bin <= lmax) x = kTma ? T(bin, 0) : S(bin, 0, th);
           if (bin >= nPhi - lmax)
-            x = cadd(x, kTma ? T(nPhi - bin, 1) : S(nPhi - bin, 1, nTheta - 1 - th));
+            x = cadd(x, kTma ? T(nPhi - bin, 1) : S(nPhi - bin, 1, kMir ? nTheta - 1 - th : th));
         } else {
           const int M = L, bc = M - bin;
           double2 x0 = bin <= lmax ? (kTma ? T(bin, 0) : S(bin, 0, th)) : make_double2(0.0, 0.0);
@@ -910,25 +931,27 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
   }
 }
 
-template <bool kReal, int N, int kPts>
+// SpecT as for the inverse: float2 spectra keep the -m rows unmirrored.
+template <bool kReal, int N, int kPts, typename SpecT>
 __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
     int L, int lmax, int nTheta, int thetaPad, int count, const double* __restrict__ in,
     const double* __restrict__ weight, const double2* __restrict__ tw,
-    double2* __restrict__ spec) {
+    SpecT* __restrict__ spec) {
+  constexpr bool kMir = std::is_same<SpecT, double2>::value;
   extern __shared__ double2 smem[];
   constexpr int R = P3<N, kPts>::R;
   const int j0 = blockIdx.x * R, f = blockIdx.y;
   const int nPhi = 2 * L;
   const int sgnCount = kReal ? 1 : 2;
   const int twStride = nPhi / N;
-  auto S = [&](int m, int sgn, int jj) -> double2& {
+  auto S = [&](int m, int sgn, int jj) -> SpecT& {
     return spec[((size_t)(m * sgnCount + sgn) * count + f) * thetaPad + jj];
   };
   if (j0 <= nTheta - 1 && nTheta - 1 < j0 + R) {
     const int padW = thetaPad - nTheta;
     for (int i = threadIdx.x; i < (lmax + 1) * sgnCount * padW; i += P3<N, kPts>::kThreads) {
       const int q = i / padW, jj = nTheta + (i - q * padW);
-      S(q / sgnCount, q % sgnCount, jj) = make_double2(0.0, 0.0);
+      S(q / sgnCount, q % sgnCount, jj) = from_d2<SpecT>(make_double2(0.0, 0.0));
     }
   }
   // First stage, ring-major: lanes read consecutive longitudes.
@@ -970,9 +993,10 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
         for (int r = 0; r < P; r++) {
           const int bin = k + r * M;
           const double2 x = cscale(v[r], scale);
-          if (bin <= lmax) S(bin, 0, th) = x;
-          if (bin == 0) S(0, 1, nTheta - 1 - th) = make_double2(0.0, 0.0);
-          else if (bin >= nPhi - lmax) S(nPhi - bin, 1, nTheta - 1 - th) = x;
+          const int thm = kMir ? nTheta - 1 - th : th;
+          if (bin <= lmax) S(bin, 0, th) = from_d2<SpecT>(x);
+          if (bin == 0) S(0, 1, thm) = from_d2<SpecT>(make_double2(0.0, 0.0));
+          else if (bin >= nPhi - lmax) S(nPhi - bin, 1, thm) = from_d2<SpecT>(x);
         }
       }
     }
@@ -1008,65 +1032,76 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
       const double2 w = twiddle(tw, m, 1, -1);
       const double2 ev = cscale(cadd(z0, zc), 0.5);
       const double2 od = cscale(cmul_si(csub(z0, zc), -1), 0.5);
-      S(m, 0, th) = cscale(cadd(ev, cmul(w, od)), scale);
+      S(m, 0, th) = from_d2<SpecT>(cscale(cadd(ev, cmul(w, od)), scale));
     }
   }
 }
 
-// Tensor map of the spectral buffer as FP64 [m][sign][field][2 * thetaPad]
-// with a 2R x 1 x 1 x kSpecBox box (R colatitudes of kSpecBox rows).
-bool spec_map(CUtensorMap* map, double* spec, int thetaPad, int count, int sgnCount, int lmax,
-              int R) {
+// Tensor map of the spectral buffer as FP64 or FP32 [m][sign][field][2 *
+// thetaPad] with a 2R x 1 x 1 x kSpecBox box (R colatitudes of kSpecBox
+// rows).
+template <typename SpecT>
+bool spec_map(CUtensorMap* map, const SpecT* spec, int thetaPad, int count, int sgnCount,
+              int lmax, int R) {
   tc::EncodeTiledFn fn = tc::encode_fn();
   if (!fn) return false;
+  constexpr cuuint64_t kE = sizeof(SpecT) / 2;  // bytes per real component
   const cuuint64_t tp2 = 2 * (cuuint64_t)thetaPad;
   cuuint64_t dims[4] = {tp2, (cuuint64_t)count, (cuuint64_t)sgnCount, (cuuint64_t)lmax + 1};
-  cuuint64_t strides[3] = {tp2 * 8, tp2 * 8 * count, tp2 * 8 * count * sgnCount};
+  cuuint64_t strides[3] = {tp2 * kE, tp2 * kE * count, tp2 * kE * count * sgnCount};
   cuuint32_t box[4] = {(cuuint32_t)(2 * R), 1, 1, kSpecBox};
   cuuint32_t estr[4] = {1, 1, 1, 1};
-  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, spec, dims, strides, box, estr,
+  const CUtensorMapDataType dt =
+      kE == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return fn(map, dt, 4, const_cast<SpecT*>(spec), dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int N, int kPts>
+template <int N, int kPts, typename SpecT>
 gsht_status launch_p3_dir(const gsht_grid* g, int dir, int lmax, int is_real, int count,
-                          const double* src, double* dst, cudaStream_t s) {
+                          const void* src, void* dst, cudaStream_t s) {
   constexpr int kThr = P3<N, kPts>::kThreads;
   size_t shmem = sizeof(double2) * P3<N, kPts>::kSmem;
   constexpr int R = P3<N, kPts>::R;
   dim3 grid((g->n_theta + R - 1) / R, count);
   const double2* tw = reinterpret_cast<const double2*>(g->d_twiddle);
   if (dir == 1) {
+    const SpecT* spec = static_cast<const SpecT*>(src);
+    double* out = static_cast<double*>(dst);
     // Staged spectral rows: sign x ceil((lmax+1)/kSpecBox) boxes x R colatitudes.
     const int sgnCount = is_real ? 1 : 2;
     const size_t staged =
-        sizeof(double2) * sgnCount * (size_t)((lmax + kSpecBox) / kSpecBox) * kSpecBox * R;
+        sizeof(SpecT) * sgnCount * (size_t)((lmax + kSpecBox) / kSpecBox) * kSpecBox * R;
     CUtensorMap map{};
-    const bool tma = staged <= (shmem > 110 * 1024 ? shmem : 110 * 1024) &&
-                     spec_map(&map, const_cast<double*>(src), g->theta_pad, count, sgnCount, lmax, R);
+    // TMA boxes start at x = 2 j0 components: 16-byte aligned for FP64
+    // always, for FP32 when R (and so j0) is even; the box is 2R components.
+    const bool aligned = sizeof(SpecT) == 16 || R % 2 == 0;
+    const bool tma = aligned && staged <= (shmem > 110 * 1024 ? shmem : 110 * 1024) &&
+                     spec_map(&map, spec, g->theta_pad, count, sgnCount, lmax, R);
     if (tma) shmem = shmem > staged ? shmem : staged;
     const int smemElems = (int)(shmem / sizeof(double2));
     shmem += 128 + 16;
     if (tma) {
-      auto k = is_real ? k_fft_inverse_p3<true, N, true, kPts> : k_fft_inverse_p3<false, N, true, kPts>;
+      auto k = is_real ? k_fft_inverse_p3<true, N, true, kPts, SpecT>
+                       : k_fft_inverse_p3<false, N, true, kPts, SpecT>;
       GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
-      k<<<grid, kThr, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count,
-                                 reinterpret_cast<const double2*>(src), tw, dst, g->d_err,
-                                 smemElems);
+      k<<<grid, kThr, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count, spec, tw, out,
+                                  g->d_err, smemElems);
     } else {
-      auto k = is_real ? k_fft_inverse_p3<true, N, false, kPts> : k_fft_inverse_p3<false, N, false, kPts>;
+      auto k = is_real ? k_fft_inverse_p3<true, N, false, kPts, SpecT>
+                       : k_fft_inverse_p3<false, N, false, kPts, SpecT>;
       GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
-      k<<<grid, kThr, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count,
-                                 reinterpret_cast<const double2*>(src), tw, dst, g->d_err,
-                                 smemElems);
+      k<<<grid, kThr, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count, spec, tw, out,
+                                  g->d_err, smemElems);
     }
     GSHT_LAUNCH_CHECK("k_fft_inverse_p3");
   } else {
-    auto k = is_real ? k_fft_forward_p3<true, N, kPts> : k_fft_forward_p3<false, N, kPts>;
+    auto k = is_real ? k_fft_forward_p3<true, N, kPts, SpecT> : k_fft_forward_p3<false, N, kPts, SpecT>;
     GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
-    k<<<grid, kThr, shmem, s>>>(g->L, lmax, g->n_theta, g->theta_pad, count, src, g->d_weight,
-                               tw, reinterpret_cast<double2*>(dst));
+    k<<<grid, kThr, shmem, s>>>(g->L, lmax, g->n_theta, g->theta_pad, count,
+                                static_cast<const double*>(src), g->d_weight, tw,
+                                static_cast<SpecT*>(dst));
     GSHT_LAUNCH_CHECK("k_fft_forward_p3");
   }
   return GSHT_OK;
@@ -1084,11 +1119,12 @@ constexpr int p3_points() {
   return (kForward && N == 2048) ? 8192 : 4096;
 }
 
-template <int N>
+template <int N, typename SpecT = double2>
 gsht_status launch_p3(const gsht_grid* g, int dir, int lmax, int is_real, int count,
-                      const double* src, double* dst, cudaStream_t s) {
-  if (dir == 0) return launch_p3_dir<N, p3_points<N, true>()>(g, dir, lmax, is_real, count, src, dst, s);
-  return launch_p3_dir<N, p3_points<N, false>()>(g, dir, lmax, is_real, count, src, dst, s);
+                      const void* src, void* dst, cudaStream_t s) {
+  if (dir == 0)
+    return launch_p3_dir<N, p3_points<N, true>(), SpecT>(g, dir, lmax, is_real, count, src, dst, s);
+  return launch_p3_dir<N, p3_points<N, false>(), SpecT>(g, dir, lmax, is_real, count, src, dst, s);
 }
 
 template <int N>
@@ -1255,6 +1291,35 @@ gsht_status fft_forward(const gsht_grid* g, int lmax, int is_real, int count,
   }
   GSHT_LAUNCH_CHECK("k_fft_forward");
   return GSHT_OK;
+}
+
+bool fft_spec32_supported(const gsht_grid* g, int is_real) {
+  const int n = is_real ? g->n_phi / 2 : g->n_phi;
+  return n >= 256 && n <= 4096 && (n & (n - 1)) == 0;
+}
+
+// The three-pass kernels with FP32 spectra (unmirrored -m rows); only for the
+// ring lengths fft_spec32_supported accepts.
+gsht_status fft_spec32(const gsht_grid* g, int dir, int lmax, int is_real, int count,
+                       const void* src, void* dst, cudaStream_t s) {
+  switch (is_real ? g->n_phi / 2 : g->n_phi) {
+    case 256: return launch_p3<256, float2>(g, dir, lmax, is_real, count, src, dst, s);
+    case 512: return launch_p3<512, float2>(g, dir, lmax, is_real, count, src, dst, s);
+    case 1024: return launch_p3<1024, float2>(g, dir, lmax, is_real, count, src, dst, s);
+    case 2048: return launch_p3<2048, float2>(g, dir, lmax, is_real, count, src, dst, s);
+    case 4096: return launch_p3<4096, float2>(g, dir, lmax, is_real, count, src, dst, s);
+    default: return fail(GSHT_ERR_UNSUPPORTED, "no FP32-spectrum FFT for this ring length");
+  }
+}
+
+gsht_status fft_inverse32(const gsht_grid* g, int lmax, int is_real, int count, const float* spec,
+                          double* out, cudaStream_t s) {
+  return fft_spec32(g, 1, lmax, is_real, count, spec, out, s);
+}
+
+gsht_status fft_forward32(const gsht_grid* g, int lmax, int is_real, int count, const double* in,
+                          float* spec, cudaStream_t s) {
+  return fft_spec32(g, 0, lmax, is_real, count, in, spec, s);
 }
 
 }  // namespace gsht

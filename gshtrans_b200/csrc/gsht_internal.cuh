@@ -171,6 +171,13 @@ gsht_status fft_inverse(const gsht_grid* g, int lmax, int is_real, int count,
                         const double* spec, double* out, cudaStream_t s);
 gsht_status fft_forward(const gsht_grid* g, int lmax, int is_real, int count,
                         const double* in, double* spec, cudaStream_t s);
+// FP32 spectra (BF16x3 form): the -m rows are stored at their own
+// colatitudes (no mirror). Ring lengths 256..4096 (powers of two) only.
+bool fft_spec32_supported(const gsht_grid* g, int is_real);
+gsht_status fft_inverse32(const gsht_grid* g, int lmax, int is_real, int count, const float* spec,
+                          double* out, cudaStream_t s);
+gsht_status fft_forward32(const gsht_grid* g, int lmax, int is_real, int count, const double* in,
+                          float* spec, cudaStream_t s);
 
 // Legendre stage, FP64 (legendre_fp64.cu).
 size_t fp64_operand_elems(const gsht_grid* g, const Table* t, int lmax,
@@ -198,13 +205,15 @@ size_t bf16_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, 
 // with an explicit BF16x3 tile width; dir 0 forward, 1 inverse.
 gsht_status transform(gsht_grid* g, int dir, int lmax, int n, int is_real, int precision,
                       int count, const void* in, void* out, cudaStream_t s, int ntile);
+// spec32: the spectra are FP32 with unmirrored -m rows (fft_inverse32 /
+// fft_forward32); the buffer is still sized for FP64 spectra.
 gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
                                   int count, const double* coef, void* operand, double* spec,
-                                  int ntile, cudaStream_t s);
+                                  int ntile, cudaStream_t s, bool spec32 = false);
 // The spectra buffer is reused for the kernel's result rows.
 gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
                                   int count, double* spec, void* operand, double* coef,
-                                  int ntile, cudaStream_t s);
+                                  int ntile, cudaStream_t s, bool spec32 = false);
 
 // Legendre stage, Ozaki INT8 slices on tcgen05 (legendre_oz.cu).
 size_t oz_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir);

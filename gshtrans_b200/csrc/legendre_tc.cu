@@ -16,6 +16,7 @@
 // mbarrier wait is bounded (tc_common.cuh) and reports a timeout through
 // the grid's device error word instead of hanging.
 #include <cstdio>
+#include <type_traits>
 #include <vector>
 
 #include "gsht_internal.cuh"
@@ -40,6 +41,9 @@ struct TcArgs {
   int L, lmax, n, na, count, Q, R, nTheta, thetaPad, isReal;
   const long long* rowOff;
   double2* out;
+  // Inverse only: when set, the spectra are written here in FP32 with the -m
+  // rows at their own colatitudes (the FP32 spectral layout of fft.cu).
+  float2* out32;
   long coefSize;
   int* err;
 };
@@ -258,12 +262,25 @@ __global__ void __launch_bounds__(kThreads, 1)
       // Both directions write order-major rows [m][q][row] (row = colatitude
       // for the inverse, degree offset l - l0 for the forward); the forward's
       // rows are added into the packed coefficients by k_accumulate_forward.
+      if (kDir == 0 && p.out32) {
 #pragma unroll
-      for (int i = 0; i < kCols / 2; i++) {
-        const int q = q0 + i;
-        if (q < p.Q)
-          p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
-              make_double2(acc[2 * i], acc[2 * i + 1]);
+        for (int i = 0; i < kCols / 2; i++) {
+          const int q = q0 + i;
+          if (q >= p.Q) break;
+          // Table column tileRow holds +m at colatitude tileRow and -m at
+          // its mirror nTheta-1-tileRow.
+          const int col = q >= p.count ? p.nTheta - 1 - tileRow : tileRow;
+          p.out32[((size_t)m * p.Q + q) * p.thetaPad + col] =
+              make_float2((float)acc[2 * i], (float)acc[2 * i + 1]);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < kCols / 2; i++) {
+          const int q = q0 + i;
+          if (q < p.Q)
+            p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
+                make_double2(acc[2 * i], acc[2 * i + 1]);
+        }
       }
     }
   }
@@ -376,15 +393,27 @@ __global__ void __launch_bounds__(256) k_accumulate_forward(
   }
 }
 
-// Forward: weighted spectra (FP64) -> B[split][m*R + 2q + part][j].
-__global__ void k_prep_forward_bf16(int lmax, int Q, int R, int thetaPad, size_t plane,
-                                    const double2* __restrict__ spec,
+// Forward: weighted spectra (FP64, or FP32 with unmirrored -m rows) ->
+// B[split][m*R + 2q + part][j]; column j of a -m row is the spectrum at the
+// mirrored colatitude nTheta-1-j (zero in the padding).
+template <typename SpecT>
+__global__ void k_prep_forward_bf16(int lmax, int Q, int R, int count, int nTheta, int thetaPad,
+                                    size_t plane, const SpecT* __restrict__ spec,
                                     __nv_bfloat16* __restrict__ op) {
   const int m = blockIdx.y;
   const int q = blockIdx.z;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= thetaPad) return;
-  const double2 v = spec[((size_t)m * Q + q) * thetaPad + j];
+  double2 v = make_double2(0.0, 0.0);
+  if constexpr (std::is_same<SpecT, double2>::value) {
+    v = spec[((size_t)m * Q + q) * thetaPad + j];
+  } else {
+    const int col = q >= count ? nTheta - 1 - j : j;
+    if (col >= 0 && col < nTheta) {
+      const float2 f = spec[((size_t)m * Q + q) * thetaPad + col];
+      v = make_double2(f.x, f.y);
+    }
+  }
   const size_t r0 = ((size_t)m * R + 2 * q) * thetaPad + j;
   __nv_bfloat16 h, md, lo;
   split3(v.x, h, md, lo);
@@ -495,7 +524,7 @@ size_t bf16_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, 
 
 gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
                                   int count, const double* coef, void* operand, double* spec,
-                                  int ntile, cudaStream_t s) {
+                                  int ntile, cudaStream_t s, bool spec32) {
   if (!valid_ntile(ntile)) return fail(GSHT_ERR_BAD_ARG, "BF16x3 tile width %d not in {32, 64, 128}", ntile);
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
@@ -522,6 +551,7 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count; a.Q = Q; a.R = R;
   a.nTheta = g->n_theta; a.thetaPad = g->theta_pad; a.isReal = is_real;
   a.rowOff = t->d_row_off; a.out = reinterpret_cast<double2*>(spec);
+  a.out32 = spec32 ? reinterpret_cast<float2*>(spec) : nullptr;
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
   return launch_bf16<0>(g, ntile, a, mapA, mapB, s);
@@ -529,7 +559,7 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
 
 gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
                                   int count, double* spec, void* operand, double* coef,
-                                  int ntile, cudaStream_t s) {
+                                  int ntile, cudaStream_t s, bool spec32) {
   if (!valid_ntile(ntile)) return fail(GSHT_ERR_BAD_ARG, "BF16x3 tile width %d not in {32, 64, 128}", ntile);
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
@@ -539,8 +569,12 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
   {
     StageTimer tm(GSHT_STAGE_PREP_FORWARD, s);
     dim3 pg((tp + 127) / 128, lmax + 1, Q);
-    k_prep_forward_bf16<<<pg, 128, 0, s>>>(lmax, Q, R, tp, plane,
-                                           reinterpret_cast<const double2*>(spec), op);
+    if (spec32)
+      k_prep_forward_bf16<float2><<<pg, 128, 0, s>>>(lmax, Q, R, count, g->n_theta, tp, plane,
+                                                     reinterpret_cast<const float2*>(spec), op);
+    else
+      k_prep_forward_bf16<double2><<<pg, 128, 0, s>>>(lmax, Q, R, count, g->n_theta, tp, plane,
+                                                      reinterpret_cast<const double2*>(spec), op);
     GSHT_LAUNCH_CHECK("k_prep_forward_bf16");
   }
   CUtensorMap mapA, mapB;

@@ -101,6 +101,38 @@ def test_bf16x3_L1024_batched(gsht, n, is_real):
     assert relerr(res["bf16x3"][1], res["fp64"][1]) < 2 * TOL_BF16
 
 
+@pytest.mark.parametrize("L", [128, 256, 512, 1024, 2048])
+def test_bf16x3_fp32_spectra_every_ring_length(gsht, L):
+    # Where the ring FFTs are the three-pass kernels (256..4096 points: nPhi
+    # = 2L for complex fields, L for real ones), the BF16x3 form keeps its
+    # spectra in FP32 with unmirrored -m rows; 4096-point rings load them
+    # without TMA. Both field kinds, a negative upper index (mirror signs).
+    import torch
+
+    rng = np.random.default_rng(500 + L)
+    with gsht.GaussLegendreGrid(L, 1, forms=("bf16x3",)) as g:
+        for is_real, n in ((False, -1), (True, 1)):
+            if is_real and L < 256:
+                continue  # 64-point real rings take the other FFT kernels
+            c = torch.from_numpy(oracle.random_coefficients(rng, L, L, n, is_real, 1.5)).cuda()
+            res = {}
+            for prec in ("fp64", "bf16x3"):
+                f = torch.zeros(g.FieldSize(), dtype=torch.float64 if is_real else torch.complex128,
+                                device="cuda")
+                g.InverseTransformation(L, n, c, f, prec)
+                back = torch.zeros_like(c)
+                g.ForwardTransformation(L, n, f, back, prec)
+                g.device_status()
+                res[prec] = (f.cpu().numpy(), back.cpu().numpy())
+            # lmax 2048 contracts 2049 degrees: the hi*hi FP32 accumulators
+            # take ~43 roundings per K range instead of ~21 and the form sits
+            # at ~1.4e-6 there (the FP32 spectra add ~3e-8); 1e-6 is the bar
+            # up to lmax 1024, the size the form is specified for.
+            tol = TOL_BF16 if L <= 1024 else 2 * TOL_BF16
+            assert relerr(res["bf16x3"][0], res["fp64"][0]) < tol, (L, is_real)
+            assert relerr(res["bf16x3"][1], res["fp64"][1]) < 2 * tol, (L, is_real)
+
+
 # --- Ozaki INT8 slices (tcgen05 kind::i8, exact INT32 accumulation) --------
 
 TOL_OZ = 1e-12
