@@ -307,10 +307,13 @@ def legendre_roofline(precision, res, args, peaks):
     else:
         peak, src = peaks.get("int8"), "2 x MEASURED_PEAKS.json bf16_tflops (dense INT8 = 2x BF16 rate)"
         unit = "TOP/s"
+    # DRAM bytes (read + write) per launch, mean of the inverse and forward
+    # launches, from one ncu capture of this workload (lmax 1024, 64 complex
+    # fields, n = 0; profiles/traffic_legendre_lmax1024.md); None elsewhere.
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(f"legendre_{precision}")
+    if L == L_MAX and B == 64 and N_UPPER == 0:
+        traffic = {"fp64": (7.575e9 + 8.788e9) / 2, "bf16x3": (5.384e9 + 6.302e9) / 2,
+                   "ozaki": (7.154e9 + 6.875e9) / 2}[precision]
     return {
         "kernel": {"fp64": "k_legendre_fp64", "bf16x3": "k_legendre_tc (kind::f16)",
                    "ozaki": "k_legendre_oz (kind::i8)"}[precision] + " inverse+forward",
