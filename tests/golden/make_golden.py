@@ -36,7 +36,7 @@ CASES = [
     (33, 33, -2, False, 4, 1.0),
     (33, 33, 3, True, 5, 1.0),
     (33, 20, 1, True, 6, None),
-    (64, 64, 0, False, 7, 1.0),   # configs[0]: L = 64, n = 0, envelope 1/(l+1)
+    (64, 64, 0, False, 7, 1.0),   # the L = 64 round-trip case: n = 0, envelope 1/(l+1)
     (10, 10, 0, True, 8, None),
     (6, 6, 1, False, 9, None),
     (7, 7, -3, True, 10, None),

@@ -1,5 +1,5 @@
 """Fused field expressions (CanonicalComponentField algebra) and the
-field-product pipeline of configs[4] on the GPU.
+field-product pipeline (64 pairs at lmax 768) on the GPU.
 
 The pointwise kernel is compared with the same expression evaluated
 elementwise in PyTorch (bit-identical for + - * conj real imag; division
@@ -93,7 +93,7 @@ def test_compound_assignment_in_place(gsht):
 
 @pytest.mark.parametrize("precision,tol", [("fp64", None), ("bf16x3", 3e-6), ("ozaki", 1e-12)])
 def test_field_product_pipeline(gsht, precision, tol):
-    # pairs (u: n=+1, v: n=-1) at lmax 768 (nPhi = 1536 = 2^9 3),
+    # The field-product workload: pairs (u: n=+1, v: n=-1) at lmax 768 (nPhi = 1536 = 2^9 3),
     # envelope (l+1)^-1.5; inverse both, w = u*v + conj(u)*u (upper index 0),
     # forward w at lmax 768. Batched (8 pairs here; the shapes of 64).
     import torch

@@ -81,7 +81,7 @@ def test_bf16x3_golden(gsht, golden):
 
 @pytest.mark.parametrize("n,is_real", [(0, False), (0, True), (2, False), (-2, True)])
 def test_bf16x3_L1024_batched(gsht, n, is_real):
-    # configs[1] shapes: lmax 1024, n in {0, +-2}, envelope (l+1)^-1.5.
+    # The headline shapes: lmax 1024, n in {0, +-2}, envelope (l+1)^-1.5.
     import torch
 
     L, B = 1024, 4

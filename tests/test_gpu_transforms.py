@@ -203,7 +203,7 @@ def test_chunked_host_batches_match_device_batches(gsht, precision, pinned):
 
 @pytest.mark.parametrize("n,is_real", [(0, False), (2, True), (-2, False)])
 def test_L1024_vs_reference_and_round_trip(gsht, n, is_real):
-    # lmax 1024, n in {0, +2, -2}, real and complex fields,
+    # The headline size: lmax 1024, n in {0, +2, -2}, real and complex fields,
     # envelope (l+1)^-1.5. Parity against the reference build where present,
     # else against the C restatement.
     import oracle as O
