@@ -1,7 +1,7 @@
 """CPU oracle for the Gauss-Legendre GSHT path — TEST INFRASTRUCTURE ONLY.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` import this package, and only as the checker. The product
+``bench.py`` import this package, and only to check results against. The product
 (``gshtrans_b200`` and ``libgsht_cuda.so``) never imports, links or runs it.
 
 Two oracles live here:
