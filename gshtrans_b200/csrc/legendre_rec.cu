@@ -88,6 +88,9 @@ __device__ __forceinline__ double chain_step(Chain& c, double a, double b) {
 // Colatitudes per thread (inverse): 1 ran 8% slower, 4 (98 registers) 43%
 // slower at lmax 2048.
 constexpr int kInvT = 2;
+// Blocks per SM asked of the compiler for one or two rows: 4 (64 registers)
+// ran the lmax 2048 inverse in 2.67 ms against 3.10 ms at 98 registers.
+constexpr int kInvMinBlocks = 4;
 
 // Inverse: block (colatitude block of 256 x kInvT, order m, row group of kQ).
 // The block's operand rows (times sc_k) and recurrence coefficients are
@@ -116,7 +119,7 @@ __device__ __forceinline__ void rec_inv_steps(int kn, const double2* sAB,
 }
 
 template <int kQ>
-__global__ void __launch_bounds__(256) k_legendre_rec_inv(RecArgs p) {
+__global__ void __launch_bounds__(256, kQ <= 2 ? kInvMinBlocks : 1) k_legendre_rec_inv(RecArgs p) {
   __shared__ double2 sAB[256];
   __shared__ double2 sA[kQ][256];
   const int m = blockIdx.y, q0 = blockIdx.z * kQ;
