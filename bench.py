@@ -8,7 +8,7 @@ seed; one inverse transform (coefficients -> grid) and one forward transform
 when the timed region starts; each step touches ~1.1 GB of coefficients and
 ~2.2 GB of grid values, far more than the 126 MB L2, so no flush is needed.
 
-    python bench.py [--gpus N --steps K --warmup W] [--precision fp64|bf16x3|ozaki]
+    python bench.py [--gpus N --steps K --warmup W] [--precision fp64|bf16x3|ozaki|ozaki4]
     python bench.py --impl reference     # the reference's CPU path (oracle/_ref)
 
 Multi-GPU runs (torchrun, one process per GPU) are independent replicas: each
@@ -38,7 +38,7 @@ L_MAX = 1024
 N_UPPER = 0
 FIELDS = 64
 ENVELOPE = 1.5
-DTYPE = {"fp64": "f64", "bf16x3": "bf16", "ozaki": "int8"}
+DTYPE = {"fp64": "f64", "bf16x3": "bf16", "ozaki": "int8", "ozaki4": "int8"}
 STAGES = ["prep_inverse", "legendre_inverse", "fft_inverse", "fft_forward",
           "prep_forward", "legendre_forward"]
 
@@ -49,7 +49,7 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--precision", default=None, choices=[None, "fp64", "bf16x3", "ozaki"])
+    p.add_argument("--precision", default=None, choices=[None, "fp64", "bf16x3", "ozaki", "ozaki4"])
     p.add_argument("--fields", type=int, default=FIELDS)
     p.add_argument("--lmax", type=int, default=L_MAX)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -296,7 +296,7 @@ def legendre_roofline(precision, res, args, peaks):
     entries = ((L + 1) ** 2 - N_UPPER ** 2) * (L + 1)
     flops_per_dir = 4.0 * B * entries
     t = res["legendre_ms"] * 1e-3 / 2  # per launch (one direction)
-    pipe = {"fp64": 1, "bf16x3": 6, "ozaki": 28}[precision]
+    pipe = {"fp64": 1, "bf16x3": 6, "ozaki": 28, "ozaki4": 10}[precision]
     achieved = pipe * flops_per_dir / t / 1e12
     if precision == "fp64":
         peak, src = peaks.get("fp64"), "cuBLAS DGEMM 8192^3 measured in this run"
@@ -313,10 +313,11 @@ def legendre_roofline(precision, res, args, peaks):
     traffic = None
     if L == L_MAX and B == 64 and N_UPPER == 0:
         traffic = {"fp64": (7.575e9 + 8.788e9) / 2, "bf16x3": (5.384e9 + 6.302e9) / 2,
-                   "ozaki": (7.154e9 + 6.875e9) / 2}[precision]
+                   "ozaki": (7.154e9 + 6.875e9) / 2}.get(precision)
     return {
         "kernel": {"fp64": "k_legendre_fp64", "bf16x3": "k_legendre_tc (kind::f16)",
-                   "ozaki": "k_legendre_oz (kind::i8)"}[precision] + " inverse+forward",
+                   "ozaki": "k_legendre_oz (kind::i8)",
+                   "ozaki4": "k_legendre_oz (kind::i8, 4 slices)"}[precision] + " inverse+forward",
         "bound": "tensor", "achieved": achieved, "peak": peak, "unit": unit,
         "frac": achieved / peak if peak else None, "peak_source": src,
         "algorithmic_flops_per_launch": flops_per_dir,
@@ -338,7 +339,7 @@ def impl_ours(args):
     dev = torch.device("cuda", local)
     import gshtrans_b200 as gsht
 
-    modes = [args.precision] if args.precision else ["ozaki", "bf16x3", "fp64"]
+    modes = [args.precision] if args.precision else ["ozaki", "ozaki4", "bf16x3", "fp64"]
     headline = modes[0]
     L, B = args.lmax, args.fields
     grid = gsht.GaussLegendreGrid(L, N_UPPER, nrange=gsht.Single,

@@ -21,7 +21,7 @@ from typing import Optional
 import numpy as np
 
 __all__ = [
-    "All", "NonNegative", "Single", "FP64", "BF16X3", "OZAKI", "RECURRENCE",
+    "All", "NonNegative", "Single", "FP64", "BF16X3", "OZAKI", "RECURRENCE", "OZAKI4",
     "GaussLegendreGrid", "GSHTError", "BadArgument", "library", "launch_count",
     "coefficient_size", "wigner", "Batch", "random_coefficients", "degree_order",
 ]
@@ -31,9 +31,10 @@ LIB_PATH = os.path.join(_HERE, "libgsht_cuda.so")
 
 # Index ranges (Concepts.h:24-27) and precision forms (include/gsht.h).
 All, NonNegative, Single = 0, 1, 2
-FP64, BF16X3, OZAKI, RECURRENCE = 0, 1, 2, 3
-_FORM_BIT = {FP64: 1, BF16X3: 2, OZAKI: 4, RECURRENCE: 8}
-_PRECISION_NAMES = {"fp64": FP64, "bf16x3": BF16X3, "ozaki": OZAKI, "recurrence": RECURRENCE}
+FP64, BF16X3, OZAKI, RECURRENCE, OZAKI4 = 0, 1, 2, 3, 4
+_FORM_BIT = {FP64: 1, BF16X3: 2, OZAKI: 4, RECURRENCE: 8, OZAKI4: 4}
+_PRECISION_NAMES = {"fp64": FP64, "bf16x3": BF16X3, "ozaki": OZAKI, "recurrence": RECURRENCE,
+                    "ozaki4": OZAKI4}
 
 _STATUS = {
     0: "OK", 1: "BAD_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOUT",

@@ -139,13 +139,13 @@ gsht_status validate(const gsht_grid* g, int lmax, int n, int is_real,
   if (!is_real && g->mrange != GSHT_RANGE_ALL)
     return fail(GSHT_ERR_BAD_ARG, "complex fields need MRange = All");
   if (precision != GSHT_FP64 && precision != GSHT_BF16X3 && precision != GSHT_OZAKI &&
-      precision != GSHT_RECURRENCE)
+      precision != GSHT_RECURRENCE && precision != GSHT_OZAKI4)
     return fail(GSHT_ERR_UNSUPPORTED, "precision %d not available", precision);
   if (precision == GSHT_RECURRENCE && !(g->forms & GSHT_FORM_RECURRENCE))
     return fail(GSHT_ERR_UNSUPPORTED, "the recurrence form was not built for this grid");
   if (precision == GSHT_BF16X3 && !(g->forms & GSHT_FORM_BF16X3))
     return fail(GSHT_ERR_UNSUPPORTED, "the BF16x3 table form was not built for this grid");
-  if (precision == GSHT_OZAKI && !(g->forms & GSHT_FORM_OZAKI))
+  if ((precision == GSHT_OZAKI || precision == GSHT_OZAKI4) && !(g->forms & GSHT_FORM_OZAKI))
     return fail(GSHT_ERR_UNSUPPORTED, "the Ozaki table form was not built for this grid");
   return GSHT_OK;
 }
@@ -207,8 +207,8 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
   if (lmax > 0) {
     if (precision == GSHT_BF16X3)
       opBytes = bf16_operand_bytes(g, lmax, is_real, chunk, dir);
-    else if (precision == GSHT_OZAKI)
-      opBytes = oz_operand_bytes(g, lmax, is_real, chunk, dir);
+    else if (precision == GSHT_OZAKI || precision == GSHT_OZAKI4)
+      opBytes = oz_operand_bytes(g, lmax, is_real, chunk, dir, precision == GSHT_OZAKI4 ? 4 : 7);
     else if (dir == 1)
       opBytes = sizeof(double) * 2 * fp64_operand_elems(g, t, lmax, is_real, chunk);
     else if (rec)
@@ -251,16 +251,18 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
       if (r != GSHT_OK) return r;
       if (precision == GSHT_BF16X3)
         return legendre_forward_bf16(g, t, lmax, is_real, c, spec, ws + oOp, dO, ntile, s, spec32);
-      if (precision == GSHT_OZAKI)
-        return legendre_forward_oz(g, t, lmax, is_real, c, spec, ws + oOp, dO, s);
+      if (precision == GSHT_OZAKI || precision == GSHT_OZAKI4)
+        return legendre_forward_oz(g, t, lmax, is_real, c, spec, ws + oOp, dO, s,
+                                   precision == GSHT_OZAKI4 ? 4 : 7);
       if (rec) return legendre_forward_rec(g, t, lmax, is_real, c, spec, ws + oOp, dO, s);
       StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
       return legendre_forward_fp64(g, t, lmax, is_real, c, spec, dO, s);
     }
     if (precision == GSHT_BF16X3)
       r = legendre_inverse_bf16(g, t, lmax, is_real, c, dI, ws + oOp, spec, ntile, s, spec32);
-    else if (precision == GSHT_OZAKI)
-      r = legendre_inverse_oz(g, t, lmax, is_real, c, dI, ws + oOp, spec, s);
+    else if (precision == GSHT_OZAKI || precision == GSHT_OZAKI4)
+      r = legendre_inverse_oz(g, t, lmax, is_real, c, dI, ws + oOp, spec, s,
+                              precision == GSHT_OZAKI4 ? 4 : 7);
     else if (rec)
       r = legendre_inverse_rec(g, t, lmax, is_real, c, dI, reinterpret_cast<double*>(ws + oOp),
                                spec, s);

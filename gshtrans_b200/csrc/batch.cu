@@ -221,7 +221,7 @@ gsht_status plan(const gsht_field_desc* fields, int count, int precision, int au
     nmax[f.lmax] = std::max(nmax[f.lmax], na);
   }
   const unsigned forms = GSHT_FORM_FP64 | (precision == GSHT_BF16X3 ? GSHT_FORM_BF16X3 : 0u) |
-                         (precision == GSHT_OZAKI ? GSHT_FORM_OZAKI : 0u);
+                         ((precision == GSHT_OZAKI || precision == GSHT_OZAKI4) ? GSHT_FORM_OZAKI : 0u);
   for (auto& kv : nmax) {
     gsht_grid* g = nullptr;
     gsht_status st = gsht_grid_create(kv.first, kv.second, GSHT_RANGE_ALL, GSHT_RANGE_ALL, forms, &g);
@@ -307,7 +307,8 @@ gsht_status gsht_plan_batch(const gsht_field_desc* fields, int count, int precis
   if (!out) return fail(GSHT_ERR_BAD_ARG, "output handle pointer is NULL");
   *out = nullptr;
   if (!fields || count < 1) return fail(GSHT_ERR_BAD_ARG, "need at least one field");
-  if (precision != GSHT_FP64 && precision != GSHT_BF16X3 && precision != GSHT_OZAKI)
+  if (precision != GSHT_FP64 && precision != GSHT_BF16X3 && precision != GSHT_OZAKI &&
+      precision != GSHT_OZAKI4)
     return fail(GSHT_ERR_UNSUPPORTED, "precision %d not available", precision);
   for (int i = 0; i < count; i++) {
     const auto& f = fields[i];

@@ -215,15 +215,17 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
                                   int count, double* spec, void* operand, double* coef,
                                   int ntile, cudaStream_t s, bool spec32 = false);
 
-// Legendre stage, Ozaki INT8 slices on tcgen05 (legendre_oz.cu).
-size_t oz_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir);
+// Legendre stage, Ozaki INT8 slices on tcgen05 (legendre_oz.cu). slices: 7
+// (the FP64-class form) or 4 (the ~1e-7 form, first 4 table slices).
+size_t oz_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir,
+                        int slices = kTableSlices);
 gsht_status legendre_inverse_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
                                 int count, const double* coef, void* operand, double* spec,
-                                cudaStream_t s);
+                                cudaStream_t s, int slices = kTableSlices);
 // The spectra buffer is reused for the kernel's result rows.
 gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
                                 int count, double* spec, void* operand, double* coef,
-                                cudaStream_t s);
+                                cudaStream_t s, int slices = kTableSlices);
 // Legendre stage, FP64 with the Wigner values generated by the l-recurrence
 // inside the contraction (legendre_rec.cu); no stored table.
 size_t rec_forward_bytes(const gsht_grid* g, const Table* t, int is_real, int count);

@@ -29,18 +29,24 @@ namespace {
 using namespace tc;
 
 constexpr int kBM = 128;  // tile rows (TMEM lanes)
-constexpr int kN = 64;    // field rows per tile
 constexpr int kBK = 64;   // K (bytes) per stage
-constexpr int kS = kTableSlices;            // 7 slices per operand
-constexpr int kNDiag = kS;                  // diagonals d = 0..6
-constexpr int kTileA = kBM * kBK;           // 8 KB per slice
-constexpr int kTileB = kN * kBK;            // 4 KB per slice
-constexpr int kStageBytes = kS * (kTileA + kTileB);  // 84 KB
-constexpr int kStages = 2;
 constexpr int kTmemCols = 512;
-constexpr int kMaxMerge = 4;  // B slices per MMA: N = 4 x 64 = 256, the largest N
-constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + 1024 + 256;
-static_assert(kNDiag * kN <= kTmemCols, "diagonal accumulators exceed the TMEM allocation");
+
+// Per-form configuration: kS slices per operand (7: the FP64-class form; 4:
+// the ~1e-7 form, products i + j <= 3) and kN field rows per tile. One TMEM
+// accumulator of kN columns per diagonal d = i + j.
+template <int kS_, int kN_>
+struct OzCfg {
+  static constexpr int kNDiag = kS_;
+  static constexpr int kTileA = kBM * kBK;  // 8 KB per slice
+  static constexpr int kTileB = kN_ * kBK;  // 4 or 8 KB per slice
+  static constexpr int kStageBytes = kS_ * (kTileA + kTileB);
+  static constexpr int kStages = kS_ == 7 ? 2 : 3;
+  static constexpr int kMaxMerge = 256 / kN_;  // B slices per MMA (N <= 256)
+  static constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + 1024 + 256;
+  static_assert(kNDiag * kN_ <= kTmemCols, "diagonal accumulators exceed the TMEM allocation");
+  static_assert(kSmemBytes <= 227 * 1024, "stages exceed shared memory");
+};
 
 struct OzArgs {
   int L, lmax, n, na, count, Q, R, nTheta, thetaPad, isReal;
@@ -69,11 +75,14 @@ __device__ __forceinline__ double i32_to_f64(uint32_t v) {
 // Persistent kernel over the tile list (see legendre_tc.cu for the protocol):
 // the epilogue sums the 7 diagonal accumulators of its 32 columns in FP64,
 // releases TMEM, then writes.
-template <int kDir>
+template <int kDir, int kS, int kN>
 __global__ void __launch_bounds__(kThreads, 1)
     k_legendre_oz(const __grid_constant__ CUtensorMap mapA,
                   const __grid_constant__ CUtensorMap mapB, OzArgs p,
                   const int4* __restrict__ tiles, int numTiles) {
+  using C = OzCfg<kS, kN>;
+  constexpr int kNDiag = C::kNDiag, kTileA = C::kTileA, kTileB = C::kTileB;
+  constexpr int kStageBytes = C::kStageBytes, kStages = C::kStages, kMaxMerge = C::kMaxMerge;
   extern __shared__ __align__(1024) unsigned char oz_smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(oz_smem_raw) + 1023) & ~uintptr_t(1023));
@@ -138,10 +147,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t id1 = idesc(2, 1, kDir == 0 ? 1 : 0, 0, kN, kBM);
-      constexpr uint32_t id2 = idesc(2, 1, kDir == 0 ? 1 : 0, 0, 2 * kN, kBM);
-      constexpr uint32_t id3 = idesc(2, 1, kDir == 0 ? 1 : 0, 0, 3 * kN, kBM);
-      constexpr uint32_t id4 = idesc(2, 1, kDir == 0 ? 1 : 0, 0, 4 * kN, kBM);
+
       int it = 0, tc = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < numTiles && ok; t += gridDim.x, tc++) {
@@ -167,7 +173,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int j0 = 0; i + j0 < kS; j0 += kMaxMerge) {
               const int nb = (kS - i - j0) < kMaxMerge ? (kS - i - j0) : kMaxMerge;
-              const uint32_t idn = nb == 4 ? id4 : (nb == 3 ? id3 : (nb == 2 ? id2 : id1));
+              const uint32_t idn = idesc(2, 1, kDir == 0 ? 1 : 0, 0, nb * kN, kBM);
               const uint32_t aBase = st + i * kTileA;
               const uint32_t bBase = st + kS * kTileA + j0 * kTileB;
               const uint32_t d = tmem + (uint32_t)((i + j0) * kN);
@@ -276,9 +282,10 @@ __device__ __forceinline__ unsigned long long digits49(double x, int sc) {
   return sh >= 64 ? 0ull : (sh <= 0 ? 0ull : m >> sh);
 }
 
-// Four values y_t = x_t 2^{sc_t} (|y_t| < 1) -> seven slice quads, s-th quad
+// Four values y_t = x_t 2^{sc_t} (|y_t| < 1) -> kS slice quads, s-th quad
 // to dst + s * plane (4-byte aligned): y = sum_s S_s 2^{-7(s+1)} with signed
 // 7-bit truncation digits S_s, taken from the integer floor(|y| 2^49).
+template <int kS>
 __device__ __forceinline__ void write_slices4(const double (&x)[4], const int (&sc)[4],
                                               int8_t* dst, size_t plane) {
   unsigned long long Y[4];
@@ -313,6 +320,7 @@ __device__ __forceinline__ int warp_max_int(int v) {
 // Six 256-thread blocks per SM (40 registers): the strided coefficient
 // gathers need warps in flight more than registers (1.01 -> 0.85 ms at lmax
 // 1024, 64 fields, against 76 registers and three blocks).
+template <int kS>
 __global__ void __launch_bounds__(256, 6) k_prep_inverse_oz(int lmax, int n, int na, int count, int Q, int R, int isReal,
                                   long coefSize, int pitch, size_t plane,
                                   const double2* __restrict__ coef, int8_t* __restrict__ op,
@@ -361,8 +369,8 @@ __global__ void __launch_bounds__(256, 6) k_prep_inverse_oz(int lmax, int n, int
       re[t] = v.x;
       im[t] = v.y;
     }
-    write_slices4(re, sre, op + r0 + k4, plane);
-    write_slices4(im, sim, op + r0 + pitch + k4, plane);
+    write_slices4<kS>(re, sre, op + r0 + k4, plane);
+    write_slices4<kS>(im, sim, op + r0 + pitch + k4, plane);
   }
 }
 
@@ -370,6 +378,7 @@ __global__ void __launch_bounds__(256, 6) k_prep_inverse_oz(int lmax, int n, int
 // colatitudes (pitch thetaPad, a multiple of 16). One warp per row (m, q),
 // four consecutive colatitudes per lane: a first pass finds the row maxima,
 // the second (reading the row again, now from L2) writes 4-byte slice quads.
+template <int kS>
 __global__ void k_prep_forward_oz(int lmax, int Q, int R, int thetaPad, size_t plane,
                                   const double2* __restrict__ spec,
                                   const int* __restrict__ tabExp, int8_t* __restrict__ op,
@@ -416,8 +425,8 @@ __global__ void k_prep_forward_oz(int lmax, int Q, int R, int thetaPad, size_t p
       sre[t] = ev[t] - ere;
       sim[t] = ev[t] - eim;
     }
-    write_slices4(re, sre, op + r0 + 4 * j4, plane);
-    write_slices4(im, sim, op + r0 + thetaPad + 4 * j4, plane);
+    write_slices4<kS>(re, sre, op + r0 + 4 * j4, plane);
+    write_slices4<kS>(im, sim, op + r0 + thetaPad + 4 * j4, plane);
   }
 }
 
@@ -439,7 +448,7 @@ gsht_status make_map_i8(CUtensorMap* map, const void* base, uint64_t inner, uint
   return GSHT_OK;
 }
 
-template <int kDir>
+template <int kDir, int kS, int kN>
 gsht_status launch_oz(const gsht_grid* g, const OzArgs& a, const CUtensorMap& mapA,
                       const CUtensorMap& mapB, cudaStream_t s) {
   gsht_status st;
@@ -447,26 +456,30 @@ gsht_status launch_oz(const gsht_grid* g, const OzArgs& a, const CUtensorMap& ma
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
   const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kN, kBK, &st);
   if (!tl) return st;
-  auto kern = k_legendre_oz<kDir>;
-  GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kSmemBytes));
+  auto kern = k_legendre_oz<kDir, kS, kN>;
+  constexpr size_t kSmem = OzCfg<kS, kN>::kSmemBytes;
+  GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
   const int blocks = tl->count < sms ? tl->count : sms;
-  kern<<<blocks, kThreads, kSmemBytes, s>>>(mapA, mapB, a, tl->d_tiles, tl->count);
+  kern<<<blocks, kThreads, kSmem, s>>>(mapA, mapB, a, tl->d_tiles, tl->count);
   GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_oz<inverse>" : "k_legendre_oz<forward>");
   return GSHT_OK;
 }
 
 }  // namespace
 
-size_t oz_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir) {
+size_t oz_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir,
+                        int slices) {
+  const int kS = slices;
   const int R = 2 * (is_real ? 1 : 2) * count;
   const long long pitch = dir == 0 ? g->theta_pad : round_up(lmax + 1, kBK);
   return (size_t)kS * (lmax + 1) * R * pitch + sizeof(int) * (size_t)(lmax + 1) * R + 256;
 }
 
-gsht_status legendre_inverse_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
-                                int count, const double* coef, void* operand, double* spec,
-                                cudaStream_t s) {
+namespace {
+
+template <int kS, int kN>
+gsht_status inverse_oz(const gsht_grid* g, const Table* t, int lmax, int is_real, int count,
+                       const double* coef, void* operand, double* spec, cudaStream_t s) {
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
   const int pitch = (int)round_up(lmax + 1, kBK);
@@ -476,7 +489,7 @@ gsht_status legendre_inverse_oz(const gsht_grid* g, const Table* t, int lmax, in
   {
     StageTimer tm(GSHT_STAGE_PREP_INVERSE, s);
     const long long warps = (long long)(lmax + 1) * Q;
-    k_prep_inverse_oz<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
+    k_prep_inverse_oz<kS><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
         lmax, t->n, na, count, Q, R, is_real, coef_size(lmax, t->n, is_real), pitch, plane,
         reinterpret_cast<const double2*>(coef), op, rowExp);
     GSHT_LAUNCH_CHECK("k_prep_inverse_oz");
@@ -496,12 +509,12 @@ gsht_status legendre_inverse_oz(const gsht_grid* g, const Table* t, int lmax, in
   a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
-  return launch_oz<0>(g, a, mapA, mapB, s);
+  return launch_oz<0, kS, kN>(g, a, mapA, mapB, s);
 }
 
-gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
-                                int count, double* spec, void* operand, double* coef,
-                                cudaStream_t s) {
+template <int kS, int kN>
+gsht_status forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real, int count,
+                       double* spec, void* operand, double* coef, cudaStream_t s) {
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
   const int tp = g->theta_pad;
@@ -511,7 +524,7 @@ gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, in
   {
     StageTimer tm(GSHT_STAGE_PREP_FORWARD, s);
     const long long warps = (long long)(lmax + 1) * Q;
-    k_prep_forward_oz<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
+    k_prep_forward_oz<kS><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
         lmax, Q, R, tp, plane, reinterpret_cast<const double2*>(spec), t->i8_exp, op, rowExp);
     GSHT_LAUNCH_CHECK("k_prep_forward_oz");
   }
@@ -532,9 +545,27 @@ gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, in
   a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
-  st = launch_oz<1>(g, a, mapA, mapB, s);
+  st = launch_oz<1, kS, kN>(g, a, mapA, mapB, s);
   if (st != GSHT_OK) return st;
   return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, tp, spec, coef, s);
+}
+
+}  // namespace
+
+// Slices 7 (FP64-class) run on 64-row field tiles, 4 (~1e-7) on 128-row ones
+// (4 diagonals x 128 TMEM columns).
+gsht_status legendre_inverse_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                                int count, const double* coef, void* operand, double* spec,
+                                cudaStream_t s, int slices) {
+  if (slices == 4) return inverse_oz<4, 128>(g, t, lmax, is_real, count, coef, operand, spec, s);
+  return inverse_oz<7, 64>(g, t, lmax, is_real, count, coef, operand, spec, s);
+}
+
+gsht_status legendre_forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                                int count, double* spec, void* operand, double* coef,
+                                cudaStream_t s, int slices) {
+  if (slices == 4) return forward_oz<4, 128>(g, t, lmax, is_real, count, spec, operand, coef, s);
+  return forward_oz<7, 64>(g, t, lmax, is_real, count, spec, operand, coef, s);
 }
 
 }  // namespace gsht

@@ -54,9 +54,12 @@ enum {
   GSHT_FP64 = 0,   /* FP64 tensor-core (DMMA) contraction: the drop-in path   */
   GSHT_BF16X3 = 1, /* hi/mid/lo BF16 split products, FP32 accumulation       */
   GSHT_OZAKI = 2,  /* Ozaki INT8 slices, exact INT32 accumulation, FP64 sum   */
-  GSHT_RECURRENCE = 3 /* FP64 with d^l_mn(theta) generated by the l-recurrence
-                         inside the contraction kernels (no stored table); the
-                         path GSHT_FP64 takes on grids built without FP64 table */
+  GSHT_RECURRENCE = 3, /* FP64 with d^l_mn(theta) generated by the l-recurrence
+                          inside the contraction kernels (no stored table); the
+                          path GSHT_FP64 takes on grids built without FP64 table */
+  GSHT_OZAKI4 = 4     /* Ozaki INT8 with 4 slices (products i + j <= 3): ~1e-7,
+                          for the same tier as BF16X3; uses the first 4 planes of
+                          the GSHT_FORM_OZAKI table */
 };
 
 /* Table forms built by gsht_grid_create (bit mask). GSHT_FORM_RECURRENCE

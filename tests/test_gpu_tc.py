@@ -133,6 +133,44 @@ def test_bf16x3_fp32_spectra_every_ring_length(gsht, L):
             assert relerr(res["bf16x3"][1], res["fp64"][1]) < 2 * tol, (L, is_real)
 
 
+# --- Ozaki INT8 with 4 slices: the ~1e-7 form (same tier as BF16x3) -------
+
+@pytest.mark.parametrize("seed", range(4))
+def test_ozaki4_random_sizes_vs_fp64(gsht, seed):
+    rng = np.random.default_rng(7000 + seed)
+    L = int(rng.integers(8, 300))
+    lmax = int(rng.integers(4, L + 1))
+    n = int(rng.integers(-min(lmax, 2), min(lmax, 2) + 1))
+    with gsht.GaussLegendreGrid(L, 2, forms=("ozaki4",)) as g:
+        for is_real in (False, True):
+            c = oracle.random_coefficients(rng, L, lmax, n, is_real, 1.0)
+            f64, c64 = _both(g, lmax, n, is_real, c, "fp64")
+            f4, c4 = _both(g, lmax, n, is_real, c, "ozaki4")
+            assert relerr(f4, f64) < TOL_BF16, (L, lmax, n, is_real)
+            assert relerr(c4, c64) < 2 * TOL_BF16, (L, lmax, n, is_real)
+
+
+@pytest.mark.parametrize("n,is_real", [(0, False), (2, True), (-2, False)])
+def test_ozaki4_L1024_batched(gsht, n, is_real):
+    import torch
+
+    L, B = 1024, 4
+    rng = np.random.default_rng(91 + n)
+    c = np.stack([oracle.random_coefficients(rng, L, L, n, is_real, 1.5) for _ in range(B)])
+    with gsht.GaussLegendreGrid(L, abs(n), forms=("ozaki",)) as g:
+        dc = torch.from_numpy(c).cuda()
+        res = {}
+        for prec in ("fp64", "ozaki4"):
+            f = torch.zeros((B, g.FieldSize()), dtype=torch.float64 if is_real else torch.complex128, device="cuda")
+            g.inverse_batch(L, n, dc, f, prec)
+            back = torch.zeros_like(dc)
+            g.forward_batch(L, n, f, back, prec)
+            g.device_status()
+            res[prec] = (f.cpu().numpy(), back.cpu().numpy())
+    assert relerr(res["ozaki4"][0], res["fp64"][0]) < TOL_BF16
+    assert relerr(res["ozaki4"][1], res["fp64"][1]) < 2 * TOL_BF16
+
+
 # --- Ozaki INT8 slices (tcgen05 kind::i8, exact INT32 accumulation) --------
 
 TOL_OZ = 1e-12
