@@ -395,35 +395,47 @@ __global__ void __launch_bounds__(256) k_accumulate_forward(
 
 // Forward: weighted spectra (FP64, or FP32 with unmirrored -m rows) ->
 // B[split][m*R + 2q + part][j]; column j of a -m row is the spectrum at the
-// mirrored colatitude nTheta-1-j (zero in the padding).
+// mirrored colatitude nTheta-1-j (zero in the padding). Two colatitudes per
+// thread, written as BF16 pairs (thetaPad is even).
 template <typename SpecT>
 __global__ void k_prep_forward_bf16(int lmax, int Q, int R, int count, int nTheta, int thetaPad,
                                     size_t plane, const SpecT* __restrict__ spec,
                                     __nv_bfloat16* __restrict__ op) {
   const int m = blockIdx.y;
   const int q = blockIdx.z;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   if (j >= thetaPad) return;
-  double2 v = make_double2(0.0, 0.0);
+  const size_t row = ((size_t)m * Q + q) * thetaPad;
+  double2 v[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
   if constexpr (std::is_same<SpecT, double2>::value) {
-    v = spec[((size_t)m * Q + q) * thetaPad + j];
+    v[0] = spec[row + j];
+    v[1] = spec[row + j + 1];
+  } else if (q < count) {
+    const float4 f = *reinterpret_cast<const float4*>(spec + row + j);
+    v[0] = make_double2(f.x, f.y);
+    v[1] = make_double2(f.z, f.w);
   } else {
-    const int col = q >= count ? nTheta - 1 - j : j;
-    if (col >= 0 && col < nTheta) {
-      const float2 f = spec[((size_t)m * Q + q) * thetaPad + col];
-      v = make_double2(f.x, f.y);
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const int col = nTheta - 1 - (j + t);
+      if (col >= 0) {
+        const float2 f = spec[row + col];
+        v[t] = make_double2(f.x, f.y);
+      }
     }
   }
   const size_t r0 = ((size_t)m * R + 2 * q) * thetaPad + j;
-  __nv_bfloat16 h, md, lo;
-  split3(v.x, h, md, lo);
-  op[r0] = h;
-  op[plane + r0] = md;
-  op[2 * plane + r0] = lo;
-  split3(v.y, h, md, lo);
-  op[r0 + thetaPad] = h;
-  op[plane + r0 + thetaPad] = md;
-  op[2 * plane + r0 + thetaPad] = lo;
+  __nv_bfloat162 h, md, lo;
+  split3(v[0].x, h.x, md.x, lo.x);
+  split3(v[1].x, h.y, md.y, lo.y);
+  *reinterpret_cast<__nv_bfloat162*>(op + r0) = h;
+  *reinterpret_cast<__nv_bfloat162*>(op + plane + r0) = md;
+  *reinterpret_cast<__nv_bfloat162*>(op + 2 * plane + r0) = lo;
+  split3(v[0].y, h.x, md.x, lo.x);
+  split3(v[1].y, h.y, md.y, lo.y);
+  *reinterpret_cast<__nv_bfloat162*>(op + r0 + thetaPad) = h;
+  *reinterpret_cast<__nv_bfloat162*>(op + plane + r0 + thetaPad) = md;
+  *reinterpret_cast<__nv_bfloat162*>(op + 2 * plane + r0 + thetaPad) = lo;
 }
 
 // ---------------------------------------------------------------------------
@@ -568,7 +580,7 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
   auto* op = static_cast<__nv_bfloat16*>(operand);
   {
     StageTimer tm(GSHT_STAGE_PREP_FORWARD, s);
-    dim3 pg((tp + 127) / 128, lmax + 1, Q);
+    dim3 pg((tp / 2 + 127) / 128, lmax + 1, Q);
     if (spec32)
       k_prep_forward_bf16<float2><<<pg, 128, 0, s>>>(lmax, Q, R, count, g->n_theta, tp, plane,
                                                      reinterpret_cast<const float2*>(spec), op);
