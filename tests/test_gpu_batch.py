@@ -38,7 +38,7 @@ SPECS = [(32, 0, False), (32, 0, False), (32, -1, True), (64, 2, False), (64, 2,
          (48, 0, False), (96, -1, True)]
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-14), ("bf16x3", 1e-12), ("ozaki", 1e-14)])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-14), ("bf16x3", 1e-12), ("ozaki", 1e-14), ("ozaki4", 1e-14)])
 def test_batch_matches_single_field_calls(gsht, precision, tol):
     import torch
 
