@@ -100,3 +100,20 @@ def test_plan_batch_validates_without_a_device():
     assert g.library.gsht_plan_batch(arr, 1, 7, 1, ctypes.byref(h)) == 5       # precision
     assert g.library.gsht_plan_batch(arr, 1, 1, 1, ctypes.byref(h)) == 6       # no device
     assert g.library.gsht_batch_execute(None, 0, None) == 1
+
+
+def test_python_constants_match_the_header():
+    # The Python mirror's precision and form constants are the C ABI's.
+    import gshtrans_b200 as g
+
+    text = open(os.path.join(ROOT, "include", "gsht.h")).read()
+    values = {k: int(v) for k, v in re.findall(r"\b(GSHT_[A-Z0-9_]+)\s*=\s*(\d+)", text)}
+    for name in ("FP64", "BF16X3", "OZAKI", "RECURRENCE", "OZAKI4"):
+        assert getattr(g, name) == values[f"GSHT_{name}"], name
+    forms = {"FP64": "GSHT_FORM_FP64", "BF16X3": "GSHT_FORM_BF16X3", "OZAKI": "GSHT_FORM_OZAKI",
+             "RECURRENCE": "GSHT_FORM_RECURRENCE", "OZAKI4": "GSHT_FORM_OZAKI"}
+    for name, form in forms.items():
+        assert g._FORM_BIT[getattr(g, name)] == values[form], name
+    for name, code in (("All", "GSHT_RANGE_ALL"), ("NonNegative", "GSHT_RANGE_NONNEGATIVE"),
+                       ("Single", "GSHT_RANGE_SINGLE")):
+        assert getattr(g, name) == values[code], name
