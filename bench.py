@@ -40,7 +40,7 @@ FIELDS = 64
 ENVELOPE = 1.5
 DTYPE = {"fp64": "f64", "bf16x3": "bf16", "ozaki": "int8", "ozaki4": "int8"}
 STAGES = ["prep_inverse", "legendre_inverse", "fft_inverse", "fft_forward",
-          "prep_forward", "legendre_forward"]
+          "prep_forward", "legendre_forward", "accumulate_forward"]
 
 
 def parse():
@@ -271,16 +271,17 @@ def measure_mode(gsht, grid, torch, dev, coef, field, back, precision, args, wor
         dist.barrier()
     ms = e0.elapsed_time(e1)
     launches = gsht.launch_count() - launches0
-    stage_ms = (ctypes.c_double * 6)()
-    stage_n = (ctypes.c_long * 6)()
+    ns = len(STAGES)
+    stage_ms = (ctypes.c_double * ns)()
+    stage_n = (ctypes.c_long * ns)()
     lib.gsht_profile_read(ctypes.cast(stage_ms, ctypes.c_void_p),
-                          ctypes.cast(stage_n, ctypes.c_void_p), 6)
+                          ctypes.cast(stage_n, ctypes.c_void_p), ns)
     lib.gsht_profile_enable(0)
     grid.device_status()
     if world > 1:
         ms = reduce_max_ms(ms, dist, dev)
     stages = {STAGES[i]: {"ms_per_step": stage_ms[i] / args.steps,
-                          "launches_per_step": stage_n[i] / args.steps} for i in range(6)}
+                          "launches_per_step": stage_n[i] / args.steps} for i in range(ns)}
     return {"ms": ms, "launches": launches, "stages": stages, "clocks": clk.summary(),
             "round_trip_rel_err": rt_err,
             "legendre_ms": (stage_ms[1] + stage_ms[5]) / args.steps,

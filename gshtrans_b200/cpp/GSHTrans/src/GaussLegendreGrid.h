@@ -22,11 +22,14 @@ namespace GSHTrans {
 // reference interface): FP64 is the drop-in default. Recurrence is FP64 with
 // no stored table: the grid keeps only the l-recurrence's start values and
 // coefficients, and the transforms generate the Wigner values as they go.
+// BF16x3 and Ozaki4 are the ~1e-6 tensor-core forms, Ozaki the FP64-class
+// one; Ozaki4 reads the first four slices of the Ozaki table.
 enum class Precision {
   FP64 = GSHT_FP64,
   BF16x3 = GSHT_BF16X3,
   Ozaki = GSHT_OZAKI,
-  Recurrence = GSHT_RECURRENCE
+  Recurrence = GSHT_RECURRENCE,
+  Ozaki4 = GSHT_OZAKI4
 };
 
 template <RealFloatingPoint _Real, OrderIndexRange _MRange, IndexRange _NRange>
@@ -53,7 +56,7 @@ class GaussLegendreGrid : public GridBase<GaussLegendreGrid<_Real, _MRange, _NRa
   GaussLegendreGrid(int lMax, int nMax, Precision precision) : _lMax{lMax}, _nMax{nMax}, _prec{precision} {
     unsigned forms = GSHT_FORM_FP64;
     if (precision == Precision::BF16x3) forms |= GSHT_FORM_BF16X3;
-    if (precision == Precision::Ozaki) forms |= GSHT_FORM_OZAKI;
+    if (precision == Precision::Ozaki || precision == Precision::Ozaki4) forms |= GSHT_FORM_OZAKI;
     if (precision == Precision::Recurrence) forms = GSHT_FORM_RECURRENCE;
     gsht_grid* g = nullptr;
     Backend::Check(gsht_grid_create(lMax, nMax, Backend::RangeCode<MRange>(),

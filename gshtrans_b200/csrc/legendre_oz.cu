@@ -544,8 +544,10 @@ gsht_status forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real
   // go into their buffer and are then added into the coefficients.
   a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
-  StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
-  st = launch_oz<1, kS, kN>(g, a, mapA, mapB, s);
+  {
+    StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
+    st = launch_oz<1, kS, kN>(g, a, mapA, mapB, s);
+  }
   if (st != GSHT_OK) return st;
   return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, tp, spec, coef, s);
 }

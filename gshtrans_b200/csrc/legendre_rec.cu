@@ -417,9 +417,9 @@ gsht_status legendre_forward_rec(const gsht_grid* g, const Table* t, int lmax, i
                                          t->rec_sc, static_cast<const double2*>(partial),
                                          reinterpret_cast<double2*>(spec));
     GSHT_LAUNCH_CHECK("k_rec_forward_sum");
-    return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real,
-                              coef_size(lmax, t->n, is_real), g->theta_pad, spec, coef, s);
   }
+  return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real,
+                            coef_size(lmax, t->n, is_real), g->theta_pad, spec, coef, s);
 }
 
 }  // namespace gsht

@@ -604,8 +604,10 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
   // buffer holds the kernel's order-major result rows (keff <= thetaPad).
   a.rowOff = t->d_row_off; a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
-  StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
-  st = launch_bf16<1>(g, ntile, a, mapA, mapB, s);
+  {
+    StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
+    st = launch_bf16<1>(g, ntile, a, mapA, mapB, s);
+  }
   if (st != GSHT_OK) return st;
   return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, tp, spec, coef, s);
 }
@@ -613,6 +615,7 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
 gsht_status accumulate_forward(int L, int lmax, int n, int na, int count, int Q, int is_real,
                                long coefSize, int pitch, const double* rows, double* coef,
                                cudaStream_t s) {
+  StageTimer tm(GSHT_STAGE_ACCUMULATE_FORWARD, s);
   dim3 ag((lmax + 32) / 32, (lmax + 32) / 32, Q);
   k_accumulate_forward<<<ag, 256, 0, s>>>(L, lmax, n, na, count, Q, is_real, coefSize, pitch,
                                           reinterpret_cast<const double2*>(rows),

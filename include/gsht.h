@@ -240,7 +240,10 @@ enum {
   GSHT_STAGE_FFT_FORWARD = 3,      /* ring FFTs, forward                       */
   GSHT_STAGE_PREP_FORWARD = 4,     /* spectra -> per-order operand rows        */
   GSHT_STAGE_LEGENDRE_FORWARD = 5, /* order-wise contraction, forward          */
-  GSHT_STAGE_COUNT = 6
+  GSHT_STAGE_ACCUMULATE_FORWARD = 6, /* forward result rows added into the packed
+                                        coefficients (tensor-core and recurrence
+                                        forms)                                  */
+  GSHT_STAGE_COUNT = 7
 };
 gsht_status gsht_profile_enable(int on);
 gsht_status gsht_profile_read(double* ms, long* launches, int nstages);

@@ -183,6 +183,12 @@ int main() {
     Report("Coeff2Coeff C2C <All,All> recurrence" + tag, e < 1e-12, e);
     e = Coeff2Coeff<double, All, All>(lg, l, Precision::Recurrence);
     Report("Coeff2Coeff R2C <All,All> recurrence" + tag, e < 1e-12, e);
+    // Extension: the tensor-core forms selected through the C++ grid
+    // (max-abs error relative to the largest coefficient).
+    e = Coeff2Coeff<std::complex<double>, All, All>(lg, l, Precision::Ozaki);
+    Report("Coeff2Coeff C2C <All,All> Ozaki" + tag, e < 1e-12, e);
+    e = Coeff2Coeff<std::complex<double>, All, All>(lg, l, Precision::Ozaki4);
+    Report("Coeff2Coeff C2C <All,All> Ozaki4" + tag, e < 1e-5, e);
   }
   std::uniform_real_distribution<double> angle(0.0, std::numbers::pi);
   for (int trial = 0; trial < 3; trial++) {
