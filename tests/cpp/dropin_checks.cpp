@@ -165,6 +165,73 @@ static double ExpansionRoundTrip(Int L) {
   return err / ref;
 }
 
+// Vector fields (GSHTrans/Vector): the pointwise products and compound
+// operators against the same formulas on the host, and the three-component
+// expansion -> field -> expansion round trip.
+static void Vectors() {
+  using Grid = GaussLegendreGrid<double, All, All>;
+  using Complex = std::complex<double>;
+  Grid grid(40, 1);
+  ComplexVectorField<Grid> u(grid), v(grid);
+  std::normal_distribution<double> nd;
+  for (auto alpha : u.CanonicalIndices())
+    for (auto [i, j] : u.Component<0>().PointIndices()) {
+      u[alpha, i, j] = {nd(g_gen), nd(g_gen)};
+      v[alpha, i, j] = {nd(g_gen), nd(g_gen)};
+    }
+  const auto ip = InnerProduct(u, v);
+  const auto dp = DualityProduct(u, v);
+  double eip = 0, edp = 0, ref = 0;
+  for (auto [i, j] : ip.PointIndices()) {
+    Complex h = 0;
+    for (auto a : u.CanonicalIndices()) h += std::conj(u[a, i, j]) * v[a, i, j];
+    const Complex d = -u[-1, i, j] * v[1, i, j] + u[0, i, j] * v[0, i, j] - u[1, i, j] * v[-1, i, j];
+    eip = std::max(eip, std::abs(ip[i, j] - h));
+    edp = std::max(edp, std::abs(dp[i, j] - d));
+    ref = std::max(ref, std::max(std::abs(h), std::abs(d)));
+  }
+  const double tol = 16 * std::numeric_limits<double>::epsilon();
+  Report("vector InnerProduct", eip / ref < tol, eip / ref);
+  Report("vector DualityProduct", edp / ref < tol, edp / ref);
+
+  ComplexScalarField<Grid> s(grid, [](double th, double ph) { return Complex(1.5 + std::sin(th), std::cos(ph)); });
+  ComplexVectorField<Grid> w = u;
+  w += v;
+  w *= s;
+  w *= Complex(0.5, -1.0);
+  double ew = 0, rw = 0;
+  for (auto a : u.CanonicalIndices())
+    for (auto [i, j] : s.PointIndices()) {
+      const Complex h = (u[a, i, j] + v[a, i, j]) * s[i, j] * Complex(0.5, -1.0);
+      ew = std::max(ew, std::abs(w[a, i, j] - h));
+      rw = std::max(rw, std::abs(h));
+    }
+  Report("vector compound += *= (field, scalar)", ew / rw < tol, ew / rw);
+
+  ComplexVectorExpansion<Grid> e(grid);
+  const Int L = grid.MaxDegree();
+  auto fill = [&](auto& c) {
+    for (auto [l, m] : c.Indices()) c[l, m] = {nd(g_gen), nd(g_gen)};
+    c[L, L] = 0;  // alias of (L, -L)
+  };
+  fill(e.Component<-1>());
+  fill(e.Component<0>());
+  fill(e.Component<1>());
+  const auto f = e.ToField();
+  ComplexVectorExpansion<Grid> back(f);
+  double err = 0, rc = 0;
+  auto diff = [&](const auto& a, const auto& b) {
+    for (auto [l, m] : a.Indices()) {
+      err = std::max(err, std::abs(a[l, m] - b[l, m]));
+      rc = std::max(rc, std::abs(a[l, m]));
+    }
+  };
+  diff(e.Component<-1>(), back.Component<-1>());
+  diff(e.Component<0>(), back.Component<0>());
+  diff(e.Component<1>(), back.Component<1>());
+  Report("vector expansion -> field -> expansion", err / rc < 1e-12, err / rc);
+}
+
 int main() {
   for (int trial = 0; trial < 3; trial++) {
     const Int lg = Uniform(4, 256), l = Uniform(4, lg);
@@ -199,6 +266,7 @@ int main() {
     Report("addition theorem (FourPi, All, All)", e2 <= 1000 * std::numeric_limits<double>::epsilon(), e2);
   }
   Fields();
+  Vectors();
   for (Int L : {31, 96}) {
     const double ec = ExpansionRoundTrip<ComplexValued>(L);
     Report("expansion -> field -> expansion (complex) L=" + std::to_string(L), ec < 1e-12, ec);
