@@ -14,6 +14,10 @@
 // MMAs per K step instead of 28), which cuts the shared-memory operand reads
 // that bound the kernel by 43%.
 //
+// The 4-slice form (GSHT_OZAKI4, ~1e-7) keeps the first four table slices
+// and the products i + j <= 3: 10 products in 4 MMAs per K step on 128-row
+// field tiles, 4 diagonal accumulators x 128 columns.
+//
 // Table scale folding: in the inverse the table scale belongs to an output
 // row (colatitude) and is applied in the epilogue; in the forward it runs
 // along the contraction and is folded into the field-side rows before they

@@ -11,8 +11,8 @@
 // planes and six split products (hi.hi, hi.mid, mid.hi, hi.lo, lo.hi,
 // mid.mid) accumulate in FP32 in TMEM.
 //
-// Warp roles (192 threads): warp 0 issues TMA loads, warp 1 owns TMEM and
-// issues MMAs from one lane, warps 2-5 drain TMEM in the epilogue. Every
+// Warp roles (320 threads): warp 0 issues TMA loads, warp 1 owns TMEM and
+// issues MMAs from one lane, warps 2-9 drain TMEM in the epilogue. Every
 // mbarrier wait is bounded (tc_common.cuh) and reports a timeout through
 // the grid's device error word instead of hanging.
 #include <cstdio>
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   } else {
-    // Epilogue warps 2..17: lane quarter warp % 4, column group (warp - 2) / 4.
+    // Epilogue warps 2..9: lane quarter warp % 4, column group (warp - 2) / 4.
     const int quarter = warp & 3;
     const int group = (warp - 2) >> 2;
     const int row = quarter * 32 + lane;
