@@ -1,9 +1,10 @@
 /*
  * CPU restatement of the reference's Gauss-Legendre GSHT path, in plain C.
  *
- * TEST INFRASTRUCTURE ONLY. This file is the oracle: tests, the smoke check
- * and the CPU-baseline leg of the benchmark call it as the checker. The
- * product (libgsht_cuda.so) never links, loads or calls it.
+ * TEST INFRASTRUCTURE ONLY. This file is the oracle: tests and the smoke
+ * check compare the GPU results against it, and the CPU-baseline leg of the
+ * benchmark times it. The product (libgsht_cuda.so) never links, loads or
+ * calls it.
  *
  * It restates, function by function, the reference's algorithm:
  *   orc_gl_nodes      GaussQuad::LegendrePolynomial::GaussQuadrature (the
