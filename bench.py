@@ -87,24 +87,95 @@ def coefficients(lmax, fields, seed=0):
 # Clock sampling during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock, its maximum and the clock-event (throttle) reasons, sampled
+    while the timed region runs: through NVML every 10 ms where the driver's
+    library loads (pynvml; the same counters nvidia-smi prints), otherwise by
+    running nvidia-smi every 200 ms. The device is found by its PCI bus id
+    when one is given (CUDA and NVML may number GPUs differently), else by
+    index."""
     FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap,power.draw")
+    # NVML clock-event reason bits, in the order of FIELDS' reason columns.
+    REASON_BITS = (0x8, 0x40, 0x20, 0x4)
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, bus_id: str | None = None, nvml=None, period_s: float = 0.01):
         self.index = index
+        self.bus_id = bus_id
+        self.period_s = period_s
         self.samples = []
+        self.source = None
+        self._nvml = nvml
         self._stop = threading.Event()
         self._t = None
 
+    def _open_nvml(self):
+        nv = self._nvml
+        if nv is None:
+            import pynvml as nv
+        nv.nvmlInit()
+        h = None
+        if self.bus_id:
+            try:
+                h = nv.nvmlDeviceGetHandleByPciBusId(self.bus_id)
+            except Exception:
+                h = None
+        if h is None:
+            h = nv.nvmlDeviceGetHandleByIndex(self.index)
+        # Every call is tried once here, so that a driver without one of them
+        # falls back to nvidia-smi before the timed region starts.
+        reasons = None
+        for name in ("nvmlDeviceGetCurrentClocksEventReasons",
+                     "nvmlDeviceGetCurrentClocksThrottleReasons"):
+            fn = getattr(nv, name, None)
+            try:
+                if fn is not None:
+                    int(fn(h))
+                    reasons = fn
+                    break
+            except Exception:
+                continue
+        if reasons is None:
+            raise RuntimeError("NVML reports no clock-event reasons")
+        nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        return nv, h, reasons, nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+    def _run_nvml(self, nv, h, reasons, mx):
+        self.source = "nvml"
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = int(reasons(h))
+                self.samples.append([str(sm), str(mx)] +
+                                    ["Active" if r & bit else "Not Active" for bit in self.REASON_BITS])
+            except Exception:
+                pass
+            self._stop.wait(self.period_s)
+        try:
+            nv.nvmlShutdown()
+        except Exception:
+            pass
+
     def _run(self):
+        try:
+            opened = self._open_nvml()
+        except Exception:
+            opened = None
+        if opened is not None:
+            self._run_nvml(*opened)
+            return
+        self.source = "nvidia-smi"
+        dev = self.bus_id or str(self.index)
         while not self._stop.is_set():
             try:
                 out = subprocess.run(
-                    ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                    ["nvidia-smi", "-i", dev, f"--query-gpu={self.FIELDS}",
                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
                 if out.returncode == 0 and out.stdout.strip():
                     self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+                elif dev != str(self.index):
+                    dev = str(self.index)  # bus id not accepted: by index
+                    continue
             except Exception:
                 pass
             self._stop.wait(0.2)
@@ -129,7 +200,16 @@ class ClockSampler:
                           if len(s) > 2 + i and s[2 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.samples)}
+                "samples": len(self.samples), "source": self.source}
+
+
+def pci_bus_id(torch, index: int):
+    """domain:bus:device.0 of a CUDA device, as NVML and nvidia-smi -i take it."""
+    try:
+        p = torch.cuda.get_device_properties(index)
+        return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+    except Exception:
+        return None
 
 
 # ---------------------------------------------------------------------------
@@ -261,7 +341,8 @@ def measure_mode(gsht, grid, torch, dev, coef, field, back, precision, args, wor
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(torch.cuda.current_device()) as clk:
+    cur = torch.cuda.current_device()
+    with ClockSampler(cur, pci_bus_id(torch, cur)) as clk:
         e0.record()
         for _ in range(args.steps):
             step()
