@@ -84,3 +84,13 @@ def test_fallback_when_nvml_does_not_load():
     s = clk.summary()
     if not clk.samples:  # no nvidia-smi on this host
         assert s["reasons"] == ["nvidia-smi unavailable"]
+
+
+def test_stage_names_cover_the_header_stages():
+    import re
+
+    text = open(os.path.join(os.path.dirname(bench.__file__), "include", "gsht.h")).read()
+    stages = dict((k, int(v)) for k, v in re.findall(r"\b(GSHT_STAGE_[A-Z_]+)\s*=\s*(\d+)", text))
+    assert len(bench.STAGES) == stages["GSHT_STAGE_COUNT"]
+    for i, name in enumerate(bench.STAGES):
+        assert stages[f"GSHT_STAGE_{name.upper()}"] == i, name
