@@ -7,6 +7,8 @@
 #include <cstring>
 #include <new>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "gsht_internal.cuh"
 
 namespace gsht {
@@ -40,7 +42,15 @@ std::vector<ProfRecord> g_prof;
 
 }  // namespace
 
+// NVTX range names of the stages (gsht.h GSHT_STAGE_*), for profilers that
+// filter or group by range (ncu --nvtx, nsys); the ranges are pushed and
+// popped whether or not stage timing is enabled.
+const char* const kStageRangeNames[GSHT_STAGE_COUNT] = {
+    "gsht:prep_inverse", "gsht:legendre_inverse", "gsht:fft_inverse", "gsht:fft_forward",
+    "gsht:prep_forward", "gsht:legendre_forward", "gsht:accumulate_forward"};
+
 StageTimer::StageTimer(int stage, cudaStream_t s) : stage_(stage), s_(s) {
+  nvtxRangePushA(stage >= 0 && stage < GSHT_STAGE_COUNT ? kStageRangeNames[stage] : "gsht:stage");
   std::lock_guard<std::mutex> lk(g_prof_mu);
   if (!g_prof_on) return;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -58,6 +68,7 @@ StageTimer::StageTimer(int stage, cudaStream_t s) : stage_(stage), s_(s) {
 }
 
 StageTimer::~StageTimer() {
+  nvtxRangePop();
   if (!a_) return;
   cudaEventRecord(b_, s_);
   std::lock_guard<std::mutex> lk(g_prof_mu);
