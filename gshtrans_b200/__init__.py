@@ -22,6 +22,7 @@ import numpy as np
 
 __all__ = [
     "All", "NonNegative", "Single", "FP64", "BF16X3", "OZAKI", "RECURRENCE", "OZAKI4",
+    "STAGES", "StageProfile",
     "GaussLegendreGrid", "GSHTError", "BadArgument", "library", "launch_count",
     "coefficient_size", "wigner", "Batch", "random_coefficients", "degree_order",
 ]
@@ -87,6 +88,35 @@ library = _load()
 def launch_count() -> int:
     """Kernels launched by libgsht_cuda.so in this process."""
     return int(library.gsht_launch_count())
+
+
+STAGES = ("prep_inverse", "legendre_inverse", "fft_inverse", "fft_forward",
+          "prep_forward", "legendre_forward", "accumulate_forward")
+
+
+class StageProfile:
+    """Per-stage device time of the transform calls made inside a ``with``
+    block (gsht_profile_enable / gsht_profile_read: CUDA events around every
+    stage of direct calls; captured graphs are not timed). After the block,
+    ``stages`` maps each stage name to ``(milliseconds, kernel launches)``.
+    No counterpart in the reference, which has no tracing."""
+
+    def __enter__(self):
+        _check(library.gsht_profile_enable(1))
+        self.stages = {}
+        return self
+
+    def __exit__(self, *exc):
+        n = len(STAGES)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_long * n)()
+        try:
+            _check(library.gsht_profile_read(ctypes.cast(ms, ctypes.c_void_p),
+                                             ctypes.cast(cnt, ctypes.c_void_p), n))
+        finally:
+            library.gsht_profile_enable(0)
+        self.stages = {name: (ms[i], int(cnt[i])) for i, name in enumerate(STAGES)}
+        return False
 
 
 def _check(status: int):

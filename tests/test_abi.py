@@ -117,3 +117,13 @@ def test_python_constants_match_the_header():
     for name, code in (("All", "GSHT_RANGE_ALL"), ("NonNegative", "GSHT_RANGE_NONNEGATIVE"),
                        ("Single", "GSHT_RANGE_SINGLE")):
         assert getattr(g, name) == values[code], name
+
+
+def test_stage_profile_without_calls():
+    # No transform inside the block: every stage reads zero (no device needed).
+    import gshtrans_b200 as g
+
+    with g.StageProfile() as p:
+        pass
+    assert tuple(p.stages) == g.STAGES
+    assert all(v == (0.0, 0) for v in p.stages.values())

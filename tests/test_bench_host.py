@@ -94,3 +94,9 @@ def test_stage_names_cover_the_header_stages():
     assert len(bench.STAGES) == stages["GSHT_STAGE_COUNT"]
     for i, name in enumerate(bench.STAGES):
         assert stages[f"GSHT_STAGE_{name.upper()}"] == i, name
+
+
+def test_bench_stages_are_the_package_stages():
+    import gshtrans_b200 as g
+
+    assert tuple(bench.STAGES) == g.STAGES

@@ -290,3 +290,21 @@ def test_fp64_accuracy_at_least_the_references(gsht, reference):
     finally:
         rd.close()
         rl.close()
+
+
+def test_stage_profile_records_the_stages_of_a_call(gsht):
+    # One FP64 inverse + forward of a complex field: the preparation,
+    # contraction and ring-FFT stages each record time and launches.
+    rng = np.random.default_rng(5)
+    with gsht.GaussLegendreGrid(64, 0) as g:
+        c = oracle.random_coefficients(rng, 64, 64, 0, False, 1.0)
+        f = np.zeros(g.FieldSize(), np.complex128)
+        back = np.zeros_like(c)
+        with gsht.StageProfile() as p:
+            g.InverseTransformation(64, 0, c, f)
+            g.ForwardTransformation(64, 0, f, back)
+        for name in ("prep_inverse", "legendre_inverse", "fft_inverse", "fft_forward",
+                     "legendre_forward"):
+            ms, launches = p.stages[name]
+            assert ms > 0.0 and launches >= 1, name
+        assert relerr(back, c) < 1e-12
