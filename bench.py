@@ -75,12 +75,22 @@ def workload(args):
     }
 
 
-def coefficients(lmax, fields, seed=0):
-    import gshtrans_b200 as gsht
+def coefficients(lmax, fields, seed=0, generator=None):
+    """Seeded coefficients of the headline workload. ``generator`` is a
+    random_coefficients function (the package's, or the oracle's for the
+    reference arm, which must not load the CUDA library)."""
+    if generator is None:
+        import gshtrans_b200 as gsht
 
+        generator = gsht.random_coefficients
     rng = np.random.default_rng(seed)
-    return np.stack([gsht.random_coefficients(rng, lmax, lmax, N_UPPER, False, ENVELOPE)
+    return np.stack([generator(rng, lmax, lmax, N_UPPER, False, ENVELOPE)
                      for _ in range(fields)])
+
+
+def run_config(args):
+    """The config dict both arms print (identical for the same arguments)."""
+    return workload(args) | {"parallelism": f"replicas x{args.gpus}"}
 
 
 # ---------------------------------------------------------------------------
@@ -235,7 +245,7 @@ def reference_run(lmax, steps, warmup, log=None):
     t0 = time.perf_counter()
     g = ref.grid(lmax, N_UPPER, 0, 2)  # NRange = Single: one host table
     build_s = time.perf_counter() - t0
-    coefs = coefficients(lmax, cores, seed=1)
+    coefs = coefficients(lmax, cores, seed=1, generator=oracle.random_coefficients)
     for _ in range(warmup):
         g.roundtrip_batch(lmax, N_UPPER, False, coefs, cores)
     t0 = time.perf_counter()
@@ -272,7 +282,8 @@ def impl_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * res["seconds"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload(args) | {"fields_per_step": res["cores"]},
+        "config": run_config(args), "precision": "fp64",
+        "fields_per_step": res["cores"],
         "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample",
                                              "single_core_value")},
         "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -390,8 +401,9 @@ def legendre_roofline(precision, res, args, peaks):
         peak, src = peaks.get("int8"), "2 x MEASURED_PEAKS.json bf16_tflops (dense INT8 = 2x BF16 rate)"
         unit = "TOP/s"
     # DRAM bytes (read + write) per launch, mean of the inverse and forward
-    # launches, from one ncu capture of this workload (lmax 1024, 64 complex
-    # fields, n = 0; profiles/traffic_legendre_lmax1024.md); None elsewhere.
+    # launches: a constant taken from an earlier ncu capture of this shape
+    # (lmax 1024, 64 complex fields, n = 0), not a measurement of this run;
+    # None for any other shape.
     traffic = None
     if L == L_MAX and B == 64 and N_UPPER == 0:
         traffic = {"fp64": (7.575e9 + 8.788e9) / 2, "bf16x3": (5.384e9 + 6.302e9) / 2,
@@ -405,6 +417,9 @@ def legendre_roofline(precision, res, args, peaks):
         "algorithmic_flops_per_launch": flops_per_dir,
         "tensor_ops_per_launch": pipe * flops_per_dir,
         "avg_launch_ms": 1e3 * t, "traffic": traffic,
+        "traffic_source": ("constant from an earlier ncu capture of this shape "
+                           "(dram__bytes_read.sum + dram__bytes_write.sum per launch), "
+                           "not measured in this run") if traffic is not None else None,
     }
 
 
@@ -492,7 +507,7 @@ def impl_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": DTYPE[headline], "data": "synthetic",
-            "config": workload(args) | {"precision": headline, "parallelism": f"replicas x{world}"},
+            "config": run_config(args), "precision": headline,
             "roofline": mode_lines[headline]["roofline"], "cpu_baseline": cpu, "e2e": e2e,
             "clocks": res["clocks"], "gpu_launches": res["launches"],
             "round_trip_rel_err": res["round_trip_rel_err"], "modes": mode_lines,
@@ -777,9 +792,24 @@ def impl_pipeline(args):
         del out[prec]["result"]
     for prec in out:
         out[prec]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out[prec]["ms_per_step"]
+    # The fused expression kernel alone (k_field_eval): reads u and v once,
+    # writes w once; 3 x 16 B per grid point, the 64 x 1.18 M points (3.6 GB
+    # per launch) far larger than L2.
+    ms_eval = _event_time(torch, lambda: w.assign(expr), max(args.steps, 10), max(args.warmup, 3))
+    bytes_eval = 3 * 16 * B * fs
+    hbm = None
+    mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(mp):
+        hbm = json.load(open(mp)).get("hbm_gbs")
+    gbs = bytes_eval / (ms_eval * 1e-3) / 1e9
+    field_eval = {"kernel": "k_field_eval", "ms": ms_eval, "algorithmic_bytes": bytes_eval,
+                  "achieved_gbs": gbs, "peak_gbs": hbm,
+                  "frac": gbs / hbm if hbm else None,
+                  "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
     print(json.dumps({
         "metric": "field-product pipeline pairs/s (2 inverses, fused u*v + conj(u)*u, 1 forward)",
         "unit": "pairs/s", "value": out["ozaki"]["pairs_per_s"], "modes": out,
+        "field_eval": field_eval,
         "config": {"workload": "64 pairs, lmax 768 (nTheta 769, nPhi 1536), u n=+1, v n=-1, "
                                "envelope (l+1)^-1.5", "steps": args.steps, "warmup": args.warmup},
     }))
