@@ -137,6 +137,13 @@ class Reference:
             [ctypes.c_void_p] + [ctypes.c_int] * 4 + [_dp, _dp, _dp] + [ctypes.c_long] * 2 + [ctypes.c_int]
         )
         L.ref_max_threads.restype = ctypes.c_int
+        L.ref_chunked_nodes.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.ref_chunked_nodes.restype = None
+        _ip = ctypes.POINTER(ctypes.c_int)
+        L.ref_chunked_inverse_rings.argtypes = [ctypes.c_int] * 4 + [_dp, ctypes.c_int, _ip, _dp]
+        L.ref_chunked_inverse_rings.restype = ctypes.c_int
+        L.ref_chunked_forward_orders.argtypes = ([ctypes.c_int] * 4 + [_dp, ctypes.c_int, _ip, ctypes.c_int, _dp])
+        L.ref_chunked_forward_orders.restype = ctypes.c_int
 
     def grid(self, lmax, nmax, mrange=0, nrange=0, long_double=False):
         return RefGrid(self, lmax, nmax, mrange, nrange, long_double)
@@ -149,6 +156,46 @@ class Reference:
 
     def max_threads(self) -> int:
         return self.lib.ref_max_threads()
+
+    # Transforms at any degree with the reference's Wigner table built on
+    # chunks of colatitudes (ref_harness.cpp: ref_chunked_*); long double is
+    # the accuracy yardstick, double the reference's own FP64 values.
+    def chunked_nodes(self, lmax, long_double=True):
+        th = np.zeros(lmax + 1)
+        w = np.zeros(lmax + 1)
+        self.lib.ref_chunked_nodes(lmax, int(long_double), _ptr(th), _ptr(w))
+        return th, w
+
+    def chunked_inverse_rings(self, lmax, n, is_real, coef, rings, long_double=True):
+        """InverseTransformation on the listed rings only: array
+        [len(rings), 2 lmax] (real or complex)."""
+        c = np.ascontiguousarray(coef, dtype=np.complex128)
+        r = np.ascontiguousarray(rings, dtype=np.int32)
+        out = np.zeros((r.size, 2 * lmax), np.float64 if is_real else np.complex128)
+        rc = self.lib.ref_chunked_inverse_rings(
+            lmax, n, int(is_real), int(long_double), _ptr(c.view(np.float64)), r.size,
+            r.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _ptr(out.view(np.float64).reshape(-1)))
+        if rc:
+            raise ValueError(f"reference chunked inverse rejected (rc={rc})")
+        return out
+
+    def chunked_forward_orders(self, lmax, n, is_real, grid, orders, chunk=64, long_double=True):
+        """ForwardTransformation restricted to the listed orders:
+        {m: c_{l,m} for l = max(|m|,|n|)..lmax}."""
+        g = np.ascontiguousarray(grid, dtype=np.float64 if is_real else np.complex128)
+        o = np.ascontiguousarray(orders, dtype=np.int32)
+        sizes = [lmax - max(abs(int(m)), abs(n)) + 1 for m in o]
+        out = np.zeros(sum(sizes), np.complex128)
+        rc = self.lib.ref_chunked_forward_orders(
+            lmax, n, int(is_real), int(long_double), _ptr(g.view(np.float64).reshape(-1)), o.size,
+            o.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), chunk, _ptr(out.view(np.float64)))
+        if rc:
+            raise ValueError(f"reference chunked forward rejected (rc={rc})")
+        res, k = {}, 0
+        for m, s in zip(o, sizes):
+            res[int(m)] = out[k:k + s]
+            k += s
+        return res
 
 
 class RefGrid:

@@ -15,10 +15,12 @@
 #include <GSHTrans/Core>
 #include <omp.h>
 
+#include <algorithm>
 #include <complex>
 #include <cstdint>
 #include <memory>
 #include <mutex>
+#include <numbers>
 #include <span>
 #include <vector>
 
@@ -276,5 +278,232 @@ int ref_roundtrip_batch(void* h, int lmax, int n, int isReal, int nfields,
 }
 
 int ref_max_threads() { return omp_get_max_threads(); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Transforms at degrees whose whole table does not fit in host memory (lmax
+// 2048: 68.8 GB in double, twice that in long double). The reference's own
+// Wigner<Real, Ortho, All, Single, Multiple, ColumnMajor> is built on chunks
+// of colatitudes and the loops of InverseTransformation
+// (GaussLegendreGrid.h:281-320) and ForwardTransformation
+// (GaussLegendreGrid.h:163-216) are restated per chunk, in the reference's
+// order of operations, so that the results equal those of a whole
+// GaussLegendreGrid<Real, All, Single> bit for bit (checked at small
+// degrees). The grid's colatitudes and weights come from the same quadrature
+// and map as its constructor (GaussLegendreGrid.h:47-49). Real = long double
+// is the accuracy yardstick; Real = double reproduces the reference's FP64
+// values where the whole grid cannot be built. Both transforms take lmax
+// equal to the grid's degree (the whole field) and one upper index n.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename Real>
+GaussQuad::Quadrature1D<Real> ChunkedQuadrature(int lmax) {
+  auto q = GaussQuad::LegendrePolynomial<Real>{}.GaussQuadrature(lmax + 1);
+  q.Transform([](auto x) { return std::acos(-x); },
+              [](auto) -> Real { return 1; });
+  return q;
+}
+
+template <typename Real>
+int ChunkedInverseRings(int lmax, int n, int isReal, const double* coef,
+                        int nRings, const int* rings, double* out) {
+  using Complex = std::complex<Real>;
+  using ChunkTable = Wigner<Real, Ortho, All, Single, Multiple, ColumnMajor>;
+  if (lmax < 1 || std::abs(n) > lmax || nRings < 1) return 1;
+  const auto quad = ChunkedQuadrature<Real>(lmax);
+  std::vector<Real> theta(nRings);
+  for (int i = 0; i < nRings; i++) {
+    if (rings[i] < 0 || rings[i] > lmax) return 1;
+    theta[i] = quad.Points()[rings[i]];
+  }
+  const ChunkTable table(lmax, lmax, n, theta);
+  const int nPhi = 2 * lmax;
+  const auto size = static_cast<std::size_t>(
+      isReal ? GSHIndices<NonNegative>(lmax, lmax, n).Size()
+             : GSHIndices<All>(lmax, lmax, n).Size());
+  std::vector<Complex> in(size);
+  for (std::size_t i = 0; i < size; i++)
+    in[i] = Complex(coef[2 * i], coef[2 * i + 1]);
+
+  if (isReal) {
+    auto inWork = FFTWpp::vector<Complex>(nPhi / 2 + 1);
+    auto outWork = FFTWpp::vector<Real>(nPhi);
+    auto plan = FFTWpp::Ranges::Plan(FFTWpp::Ranges::View(inWork),
+                                     FFTWpp::Ranges::View(outWork),
+                                     FFTWpp::Estimate);
+    for (int i = 0; i < nRings; i++) {
+      std::ranges::fill(inWork, Complex(0));
+      auto d = table[n, i];
+      auto inIter = in.begin();
+      auto wigIter = d.begin();
+      for (auto l : d.Degrees()) {
+        auto dl = d[l];
+        auto workIter = inWork.begin();
+        std::advance(wigIter, l);
+        for ([[maybe_unused]] auto m : dl.NonNegativeOrders()) {
+          *workIter++ += *inIter++ * *wigIter++;
+        }
+      }
+      plan.Execute();
+      for (int k = 0; k < nPhi; k++)
+        out[static_cast<std::size_t>(i) * nPhi + k] =
+            static_cast<double>(outWork[k]);
+    }
+    return 0;
+  }
+  auto inWork = FFTWpp::vector<Complex>(nPhi);
+  auto outWork = FFTWpp::vector<Complex>(nPhi);
+  auto plan = FFTWpp::Ranges::Plan(FFTWpp::Ranges::View(inWork),
+                                   FFTWpp::Ranges::View(outWork),
+                                   FFTWpp::Estimate, FFTWpp::Backward);
+  for (int i = 0; i < nRings; i++) {
+    std::ranges::fill(inWork, Complex(0));
+    auto d = table[n, i];
+    auto inIter = in.begin();
+    auto wigIter = d.begin();
+    for (auto l : d.Degrees()) {
+      auto dl = d[l];
+      auto workIter = std::prev(inWork.end(), l);
+      for ([[maybe_unused]] auto m : dl.NegativeOrders()) {
+        *workIter++ += *inIter++ * *wigIter++;
+      }
+      workIter = inWork.begin();
+      for ([[maybe_unused]] auto m : dl.NonNegativeOrders()) {
+        *workIter++ += *inIter++ * *wigIter++;
+      }
+    }
+    plan.Execute();
+    for (int k = 0; k < nPhi; k++) {
+      const auto o = 2 * (static_cast<std::size_t>(i) * nPhi + k);
+      out[o] = static_cast<double>(outWork[k].real());
+      out[o + 1] = static_cast<double>(outWork[k].imag());
+    }
+  }
+  return 0;
+}
+
+template <typename Real>
+int ChunkedForwardOrders(int lmax, int n, int isReal, const double* grid,
+                         int nOrders, const int* orders, int chunk,
+                         double* out) {
+  using Complex = std::complex<Real>;
+  using ChunkTable = Wigner<Real, Ortho, All, Single, Multiple, ColumnMajor>;
+  if (lmax < 1 || std::abs(n) > lmax || nOrders < 1 || chunk < 1) return 1;
+  std::vector<std::size_t> start(nOrders + 1, 0);
+  for (int k = 0; k < nOrders; k++) {
+    const int m = orders[k];
+    if (std::abs(m) > lmax || (isReal && m < 0)) return 1;
+    const int l0 = std::max(std::abs(m), std::abs(n));
+    start[k + 1] = start[k] + static_cast<std::size_t>(lmax - l0 + 1);
+  }
+  std::vector<Complex> acc(start[nOrders], Complex(0));
+  const auto quad = ChunkedQuadrature<Real>(lmax);
+  const int nTheta = lmax + 1;
+  const int nPhi = 2 * lmax;
+  const Real scaleFactor = static_cast<Real>(2) * std::numbers::pi_v<Real> /
+                           static_cast<Real>(nPhi);
+
+  auto inReal = FFTWpp::vector<Real>(nPhi);
+  auto inCplx = FFTWpp::vector<Complex>(nPhi);
+  auto outWork = FFTWpp::vector<Complex>(isReal ? nPhi / 2 + 1 : nPhi);
+  auto planReal = FFTWpp::Ranges::Plan(FFTWpp::Ranges::View(inReal),
+                                       FFTWpp::Ranges::View(outWork),
+                                       FFTWpp::Estimate);
+  auto planCplx = FFTWpp::Ranges::Plan(FFTWpp::Ranges::View(inCplx),
+                                       FFTWpp::Ranges::View(outWork),
+                                       FFTWpp::Estimate, FFTWpp::Forward);
+
+  for (int c0 = 0; c0 < nTheta; c0 += chunk) {
+    const int cn = std::min(chunk, nTheta - c0);
+    std::vector<Real> theta(quad.Points().begin() + c0,
+                            quad.Points().begin() + c0 + cn);
+    const ChunkTable table(lmax, lmax, n, theta);
+    for (int i = 0; i < cn; i++) {
+      const int iTheta = c0 + i;
+      const auto ring = static_cast<std::size_t>(iTheta) * nPhi;
+      if (isReal) {
+        for (int k = 0; k < nPhi; k++) inReal[k] = grid[ring + k];
+        planReal.Execute();
+      } else {
+        for (int k = 0; k < nPhi; k++)
+          inCplx[k] = Complex(grid[2 * (ring + k)], grid[2 * (ring + k) + 1]);
+        planCplx.Execute();
+      }
+      auto d = table[n, i];
+      const Real w = quad.W(iTheta) * scaleFactor;
+      for (int k = 0; k < nOrders; k++) {
+        const int m = orders[k];
+        const int l0 = std::max(std::abs(m), std::abs(n));
+        const auto bin = m < 0 ? nPhi + m : m;
+        for (int l = l0; l <= lmax; l++) {
+          acc[start[k] + (l - l0)] += d[l][m] * outWork[bin] * w;
+        }
+      }
+      if (!isReal) {
+        for (int k = 0; k < nOrders; k++)
+          if (orders[k] == lmax) acc[start[k + 1] - 1] = 0;
+      }
+    }
+  }
+  for (std::size_t i = 0; i < acc.size(); i++) {
+    out[2 * i] = static_cast<double>(acc[i].real());
+    out[2 * i + 1] = static_cast<double>(acc[i].imag());
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Colatitudes and weights of the grid of degree lmax (nTheta = lmax + 1
+// values each), computed in long double or double and returned as double.
+void ref_chunked_nodes(int lmax, int longDouble, double* theta, double* w) {
+  auto run = [&](auto q) {
+    for (int i = 0; i <= lmax; i++) {
+      theta[i] = static_cast<double>(q.Points()[i]);
+      w[i] = static_cast<double>(q.W(i));
+    }
+  };
+  if (longDouble) {
+    run(ChunkedQuadrature<long double>(lmax));
+  } else {
+    run(ChunkedQuadrature<double>(lmax));
+  }
+}
+
+// InverseTransformation on the rings listed in `rings` only
+// (GaussLegendreGrid.h:281-320 for each listed iTheta). coef: the packed
+// coefficients (GSHIndices<All> for a complex field, <NonNegative> for a real
+// one), complex interleaved. out: nRings rings of nPhi = 2 lmax values (real,
+// or complex interleaved), in the order of `rings`. Returns 0 on success.
+int ref_chunked_inverse_rings(int lmax, int n, int isReal, int longDouble,
+                              const double* coef, int nRings, const int* rings,
+                              double* out) {
+  return longDouble ? ChunkedInverseRings<long double>(lmax, n, isReal, coef,
+                                                       nRings, rings, out)
+                    : ChunkedInverseRings<double>(lmax, n, isReal, coef,
+                                                  nRings, rings, out);
+}
+
+// ForwardTransformation restricted to the orders listed in `orders`
+// (GaussLegendreGrid.h:163-216: every ring's FFT, weight and table block,
+// accumulated over iTheta in ascending order; the table is rebuilt for each
+// chunk of `chunk` colatitudes). grid: nTheta x nPhi values (real, or complex
+// interleaved). out: for each listed order m in turn, the coefficients
+// c_{l,m} for l = max(|m|, |n|)..lmax, complex interleaved; c_{lmax,lmax} is
+// zeroed as the reference does for complex fields. Real fields take orders
+// m >= 0 only. Returns 0 on success.
+int ref_chunked_forward_orders(int lmax, int n, int isReal, int longDouble,
+                               const double* grid, int nOrders,
+                               const int* orders, int chunk, double* out) {
+  return longDouble
+             ? ChunkedForwardOrders<long double>(lmax, n, isReal, grid,
+                                                 nOrders, orders, chunk, out)
+             : ChunkedForwardOrders<double>(lmax, n, isReal, grid, nOrders,
+                                            orders, chunk, out);
+}
 
 }  // extern "C"

@@ -37,7 +37,7 @@ def relerr(a, b) -> float:
 def golden():
     return {
         name: np.load(os.path.join(GOLDEN, f"{name}.npz"))
-        for name in ("nodes", "wigner", "transforms", "wigner_single")
+        for name in ("nodes", "wigner", "transforms", "wigner_single", "lmax2048")
     }
 
 

@@ -164,3 +164,65 @@ def test_package_coefficient_generator_matches_the_oracle():
         lb, mb = oracle.degree_order(lmax, n, is_real)
         np.testing.assert_array_equal(la, lb)
         np.testing.assert_array_equal(ma, mb)
+
+
+@pytest.mark.parametrize("long_double", [True, False])
+def test_chunked_reference_equals_the_whole_grid(reference, long_double):
+    # The chunked transforms (the reference's Wigner built on chunks of
+    # colatitudes, the loops of GaussLegendreGrid.h:163-216 / 281-320 per
+    # chunk) reproduce a whole GaussLegendreGrid<Real, All, Single> bit for bit.
+    for L, n in ((40, 1), (33, 2), (64, 0)):
+        g = reference.grid(L, n, 0, 2, long_double=long_double)
+        try:
+            rng = np.random.default_rng(L + n)
+            for is_real in (False, True):
+                c = oracle.random_coefficients(rng, L, L, n, is_real, 2.0)
+                full = g.inverse(L, n, is_real, c).reshape(L + 1, 2 * L)
+                rings = [0, 1, L // 2, L - 1, L]
+                part = reference.chunked_inverse_rings(L, n, is_real, c, rings, long_double=long_double)
+                np.testing.assert_array_equal(part, full[rings])
+                grid = rng.standard_normal(full.shape)
+                if not is_real:
+                    grid = grid + 1j * rng.standard_normal(full.shape)
+                whole = g.forward(L, n, is_real, grid.ravel())
+                _, ms = oracle.degree_order(L, n, is_real)
+                orders = [0, 1, 2, L] + ([] if is_real else [-1, -(L - 1), -L])
+                got = reference.chunked_forward_orders(L, n, is_real, grid, orders, chunk=5,
+                                                       long_double=long_double)
+                for m in orders:
+                    np.testing.assert_array_equal(got[m], whole[ms == m])
+            th, w = g.nodes()
+            th2, w2 = reference.chunked_nodes(L, long_double)
+            np.testing.assert_array_equal(th, th2)
+            np.testing.assert_array_equal(w, w2)
+        finally:
+            g.close()
+
+
+def test_lmax2048_fixture_is_consistent(golden):
+    # The seeded inputs regenerate to the stored checksums, the nodes are the
+    # mirrored Gauss-Legendre colatitudes, and the reference's own double
+    # build misses the long-double values by far more than 1e-12 at this
+    # degree (its start values underflow, Wigner.h:77-79).
+    import importlib.util
+    import os
+
+    from conftest import GOLDEN
+
+    fx = np.load(os.path.join(GOLDEN, "lmax2048.npz"))
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    L, n = (int(v) for v in fx["meta"])
+    assert (L, n) == (2048, 1)
+    th = fx["theta"]
+    assert np.all(np.diff(th) > 0) and np.max(np.abs(th + th[::-1] - np.pi)) < 1e-14
+    assert abs(fx["weight"].sum() - 2.0) < 1e-13
+    for is_real in (False, True):
+        k = "real" if is_real else "complex"
+        c, grid = mg.lmax2048_inputs(is_real)
+        np.testing.assert_array_equal(np.concatenate([c[:8], c[-8:]]), fx[f"{k}_coef_head"])
+        assert abs(c.sum() - fx[f"{k}_coef_sum"][()]) <= 1e-9 * abs(fx[f"{k}_coef_sum"][()])
+        assert abs(grid.sum() - fx[f"{k}_grid_sum"][()]) <= 1e-9 * abs(fx[f"{k}_grid_sum"][()])
+        assert fx[f"{k}_inverse_rings"].shape == (16, 2 * L)
+        assert float(fx[f"{k}_ref64_inverse_relerr"]) > 1e-8
