@@ -25,6 +25,7 @@ __all__ = [
     "STAGES", "StageProfile",
     "GaussLegendreGrid", "GSHTError", "BadArgument", "library", "launch_count",
     "coefficient_size", "wigner", "Batch", "random_coefficients", "degree_order",
+    "set_allocator", "use_torch_allocator", "alloc_stats",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -79,7 +80,15 @@ def _load() -> ctypes.CDLL:
     lib.gsht_profile_read.argtypes = [vp, vp, ip]
     lib.gsht_last_error.restype = ctypes.c_char_p
     lib.gsht_launch_count.restype = ctypes.c_ulonglong
+    lib.gsht_check_bounded_wait.argtypes = [vp, vp]
+    lib.gsht_set_allocator.argtypes = [_ALLOC_FN, _FREE_FN, vp]
+    lib.gsht_alloc_stats.argtypes = [ctypes.POINTER(ctypes.c_ulonglong)] * 2 + [ctypes.POINTER(ctypes.c_size_t)]
     return lib
+
+
+# gsht_alloc_fn / gsht_free_fn (include/gsht.h)
+_ALLOC_FN = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
+_FREE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p)
 
 
 library = _load()
@@ -88,6 +97,62 @@ library = _load()
 def launch_count() -> int:
     """Kernels launched by libgsht_cuda.so in this process."""
     return int(library.gsht_launch_count())
+
+
+_allocator_refs = None  # keeps the ctypes callbacks of the current hook alive
+
+
+def set_allocator(alloc=None, free=None):
+    """Routes every device allocation of the library through ``alloc(bytes)
+    -> int pointer (0 on failure)`` and ``free(pointer)`` (gsht_set_allocator;
+    no counterpart in the reference). ``set_allocator()`` restores
+    cudaMalloc / cudaFree. A pointer is released by the hook that made it, so
+    the callables of an earlier hook stay referenced here while it may still
+    own memory."""
+    global _allocator_refs
+    if (alloc is None) != (free is None):
+        raise BadArgument(1, "give both alloc and free, or neither")
+    if alloc is None:
+        _check(library.gsht_set_allocator(_ALLOC_FN(), _FREE_FN(), None))
+        return
+
+    def _alloc(nbytes, _ctx):
+        try:
+            return int(alloc(int(nbytes)) or 0)
+        except Exception:
+            return 0
+
+    def _free(ptr, _ctx):
+        try:
+            free(int(ptr))
+        except Exception:
+            pass
+
+    refs = (_ALLOC_FN(_alloc), _FREE_FN(_free))
+    _check(library.gsht_set_allocator(refs[0], refs[1], None))
+    _old_allocators.append(_allocator_refs)
+    _allocator_refs = refs
+
+
+_old_allocators = []
+
+
+def use_torch_allocator():
+    """Draws the library's device memory from PyTorch's caching allocator on
+    the current device (torch.cuda.caching_allocator_alloc / _delete)."""
+    import torch
+
+    set_allocator(lambda n: torch.cuda.caching_allocator_alloc(n),
+                  lambda p: torch.cuda.caching_allocator_delete(p))
+
+
+def alloc_stats():
+    """(allocations, releases, live bytes) of the library's device memory in
+    this process (gsht_alloc_stats)."""
+    a, r = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+    b = ctypes.c_size_t()
+    _check(library.gsht_alloc_stats(ctypes.byref(a), ctypes.byref(r), ctypes.byref(b)))
+    return int(a.value), int(r.value), int(b.value)
 
 
 STAGES = ("prep_inverse", "legendre_inverse", "fft_inverse", "fft_forward",
@@ -333,6 +398,12 @@ class GaussLegendreGrid:
     def device_status(self):
         """Synchronises and raises GSHTError(TIMEOUT) if a kernel gave up a bounded wait."""
         _check(library.gsht_device_status(self._h))
+
+    def check_bounded_wait(self, stream=None):
+        """Enqueues gsht_check_bounded_wait: a wait that nothing completes runs
+        to its limit (about half a second) and raises this grid's device error
+        word; the next device_status() raises GSHTError(TIMEOUT)."""
+        _check(library.gsht_check_bounded_wait(self._h, stream))
 
     # ---- transforms (GaussLegendreGrid.h:108-321) ----
     def ForwardTransformation(self, lmax: int, n: int, in_, out, precision="fp64"):

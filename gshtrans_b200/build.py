@@ -39,14 +39,35 @@ def needs_build() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every translation unit to an object in parallel (they share
+    no device symbols), then links the shared library."""
     if not force and not needs_build():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [
-        nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17",
-        "-Xcompiler", "-fPIC", "-shared", "-I", os.path.join(ROOT, "include"),
-        *sources(), "-o", LIB + ".tmp",
-    ]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+             "-I", os.path.join(ROOT, "include")]
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        cmd = [nvcc, *flags, "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, obj, r
+
+    jobs = max(1, min(len(sources()), os.cpu_count() or 1))
+    with ThreadPoolExecutor(jobs) as ex:
+        results = list(ex.map(compile_one, sources()))
+    failed = [(src, r) for src, _, r in results if r.returncode != 0]
+    for src, r in failed:
+        sys.stderr.write(r.stdout + r.stderr)
+    if failed:
+        raise subprocess.CalledProcessError(failed[0][1].returncode, f"nvcc {failed[0][0]}")
+    cmd = [nvcc, *ARCH, "-shared", *[o for _, o, _ in results], "-o", LIB + ".tmp"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

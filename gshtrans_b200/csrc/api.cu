@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <unordered_map>
 
 #include <nvtx3/nvToolsExt.h>
 
@@ -14,6 +15,7 @@
 namespace gsht {
 
 std::atomic<unsigned long long> g_launches{0};
+thread_local unsigned long long t_launches = 0;
 static thread_local char t_error[512] = "";
 
 gsht_status fail(gsht_status s, const char* fmt, ...) {
@@ -29,6 +31,75 @@ gsht_status cuda_fail(cudaError_t e, const char* what) {
               "%s: %s", what, cudaGetErrorString(e));
 }
 
+PtrKind pointer_kind(const void* p, int device) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return kHostPtr;
+  }
+  if (a.type == cudaMemoryTypeManaged) return kDevicePtr;
+  if (a.type == cudaMemoryTypeDevice) return a.device == device ? kDevicePtr : kOtherDevicePtr;
+  return kHostPtr;
+}
+
+namespace {
+
+// The allocator hook (gsht_set_allocator) and the allocations it made.
+struct Hook {
+  gsht_alloc_fn alloc = nullptr;
+  gsht_free_fn free = nullptr;
+  void* ctx = nullptr;
+};
+std::mutex g_alloc_mu;
+Hook g_hook;
+std::unordered_map<void*, Hook> g_hooked;  // pointer -> the hook that made it
+unsigned long long g_alloc_calls = 0, g_free_calls = 0;
+size_t g_live_bytes = 0;
+std::unordered_map<void*, size_t> g_live;  // pointer -> bytes, every allocation
+
+}  // namespace
+
+cudaError_t dev_malloc_bytes(void** p, size_t bytes) {
+  *p = nullptr;
+  std::lock_guard<std::mutex> lk(g_alloc_mu);
+  if (g_hook.alloc) {
+    void* q = g_hook.alloc(bytes, g_hook.ctx);
+    if (!q) return cudaErrorMemoryAllocation;
+    g_hooked[q] = g_hook;
+    *p = q;
+  } else {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      *p = nullptr;
+      return e;
+    }
+  }
+  g_alloc_calls++;
+  g_live[*p] = bytes;
+  g_live_bytes += bytes;
+  return cudaSuccess;
+}
+
+void dev_free(void* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_alloc_mu);
+  auto l = g_live.find(p);
+  if (l != g_live.end()) {
+    g_live_bytes -= l->second;
+    g_live.erase(l);
+  }
+  g_free_calls++;
+  auto h = g_hooked.find(p);
+  if (h != g_hooked.end()) {
+    const Hook hook = h->second;
+    g_hooked.erase(h);
+    hook.free(p, hook.ctx);
+  } else {
+    cudaFree(p);
+  }
+}
+
 namespace {
 
 struct ProfRecord {
@@ -39,6 +110,33 @@ struct ProfRecord {
 std::mutex g_prof_mu;
 bool g_prof_on = false;
 std::vector<ProfRecord> g_prof;
+// Records whose events have completed are folded into these per-stage
+// totals once more than kProfFold are pending, so that a long profiled loop
+// keeps a bounded number of events.
+constexpr size_t kProfFold = 1024;
+double g_prof_ms[GSHT_STAGE_COUNT] = {};
+long g_prof_launches[GSHT_STAGE_COUNT] = {};
+
+// Folds every record whose end event has completed (the caller holds g_prof_mu).
+void fold_completed() {
+  size_t keep = 0;
+  for (auto& r : g_prof) {
+    if (cudaEventQuery(r.b) == cudaSuccess) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess && r.stage >= 0 &&
+          r.stage < GSHT_STAGE_COUNT) {
+        g_prof_ms[r.stage] += t;
+        g_prof_launches[r.stage] += (long)r.launches;
+      }
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    } else {
+      g_prof[keep++] = r;
+    }
+  }
+  cudaGetLastError();
+  g_prof.resize(keep);
+}
 
 }  // namespace
 
@@ -64,7 +162,7 @@ StageTimer::StageTimer(int stage, cudaStream_t s) : stage_(stage), s_(s) {
     return;
   }
   cudaEventRecord(a_, s_);
-  launches0_ = g_launches.load();
+  launches0_ = t_launches;
 }
 
 StageTimer::~StageTimer() {
@@ -72,7 +170,8 @@ StageTimer::~StageTimer() {
   if (!a_) return;
   cudaEventRecord(b_, s_);
   std::lock_guard<std::mutex> lk(g_prof_mu);
-  g_prof.push_back({stage_, a_, b_, g_launches.load() - launches0_});
+  g_prof.push_back({stage_, a_, b_, t_launches - launches0_});
+  if (g_prof.size() > kProfFold) fold_completed();
 }
 
 namespace {
@@ -99,24 +198,15 @@ __global__ void k_lmax0(int dir, int isReal, int count, long fieldSize,
   }
 }
 
-bool is_device_ptr(const void* p) {
-  cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
 gsht_status ensure_workspace(gsht_grid* g, size_t bytes) {
   if (g->ws_bytes >= bytes) return GSHT_OK;
   if (g->ws) {
     GSHT_CUDA(cudaDeviceSynchronize());
-    cudaFree(g->ws);
+    dev_free(g->ws);
     g->ws = nullptr;
     g->ws_bytes = 0;
   }
-  cudaError_t e = cudaMalloc(&g->ws, bytes);
+  cudaError_t e = dev_malloc(&g->ws, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return fail(GSHT_ERR_OOM, "workspace allocation of %zu bytes failed", bytes);
@@ -185,7 +275,10 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
   const size_t gridBytes = sizeof(double) * (is_real ? 1 : 2) * fs * (size_t)count;
   const size_t inBytes = dir == 0 ? gridBytes : coefBytes;
   const size_t outBytes = dir == 0 ? coefBytes : gridBytes;
-  const bool inDev = is_device_ptr(in), outDev = is_device_ptr(out);
+  const PtrKind inKind = pointer_kind(in, g->device), outKind = pointer_kind(out, g->device);
+  if (inKind == kOtherDevicePtr || outKind == kOtherDevicePtr)
+    return fail(GSHT_ERR_BAD_ARG, "a buffer lives on another GPU than the grid (device %d)", g->device);
+  const bool inDev = inKind == kDevicePtr, outDev = outKind == kDevicePtr;
 
   // Inside a stream capture (batch graphs) nothing may be allocated, the
   // calls are serial on one stream, and events recorded outside the capture
@@ -220,8 +313,12 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
       opBytes = bf16_operand_bytes(g, lmax, is_real, chunk, dir);
     else if (precision == GSHT_OZAKI || precision == GSHT_OZAKI4)
       opBytes = oz_operand_bytes(g, lmax, is_real, chunk, dir, precision == GSHT_OZAKI4 ? 4 : 7);
-    else if (dir == 1)
-      opBytes = sizeof(double) * 2 * fp64_operand_elems(g, t, lmax, is_real, chunk);
+    else if (dir == 1) {
+      size_t elems = 0;
+      st = fp64_operand_elems(g, t, lmax, is_real, chunk, &elems);
+      if (st != GSHT_OK) return st;
+      opBytes = sizeof(double) * 2 * elems;
+    }
     else if (rec)
       opBytes = rec_forward_bytes(g, t, is_real, chunk);
   }
@@ -394,7 +491,7 @@ gsht_status gsht_grid_create(int lmax, int nmax, int mrange, int nrange,
   g->n_phi = 2 * lmax;
   g->theta_pad = (int)round_up(g->n_theta, kThetaPad);
   gsht_status st = build_nodes(g);
-  if (st == GSHT_OK && (cudaMalloc(&g->d_err, sizeof(int)) != cudaSuccess ||
+  if (st == GSHT_OK && (dev_malloc(&g->d_err, sizeof(int)) != cudaSuccess ||
                         cudaMemset(g->d_err, 0, sizeof(int)) != cudaSuccess)) {
     cudaGetLastError();
     st = fail(GSHT_ERR_OOM, "error word allocation failed");
@@ -408,7 +505,7 @@ gsht_status gsht_grid_create(int lmax, int nmax, int mrange, int nrange,
       tw[2 * t] = (double)cosl(a);
       tw[2 * t + 1] = (double)-sinl(a);
     }
-    if (cudaMalloc(&g->d_twiddle, sizeof(double) * tw.size()) != cudaSuccess ||
+    if (dev_malloc(&g->d_twiddle, sizeof(double) * tw.size()) != cudaSuccess ||
         cudaMemcpy(g->d_twiddle, tw.data(), sizeof(double) * tw.size(),
                    cudaMemcpyHostToDevice) != cudaSuccess) {
       cudaGetLastError();
@@ -442,11 +539,11 @@ gsht_status gsht_grid_destroy(gsht_grid* g) {
   cudaDeviceSynchronize();
   for (auto& t : g->tables) free_table(&t);
   free_layouts(g);
-  cudaFree(g->d_theta);
-  cudaFree(g->d_weight);
-  cudaFree(g->d_twiddle);
-  cudaFree(g->d_err);
-  cudaFree(g->ws);
+  dev_free(g->d_theta);
+  dev_free(g->d_weight);
+  dev_free(g->d_twiddle);
+  dev_free(g->d_err);
+  dev_free(g->ws);
   if (g->ws_done) cudaEventDestroy(g->ws_done);
   for (cudaEvent_t e : g->xfer_ev) cudaEventDestroy(e);
   if (g->h2d) cudaStreamDestroy(g->h2d);
@@ -549,6 +646,108 @@ gsht_status gsht_inverse(const gsht_grid* g, int lmax, int n, int is_real,
                        precision, 1, in, out, stream);
 }
 
+// ---- Stages of a transform sharded over ranks (include/gsht.h) ----
+
+gsht_status gsht_spectra_layout(const gsht_grid* g, int lmax, int is_real, int count,
+                                long* elems, int* pitch) {
+  if (!g) return fail(GSHT_ERR_BAD_ARG, "grid is NULL");
+  if (lmax < 1 || lmax > g->L) return fail(GSHT_ERR_BAD_ARG, "lmax %d outside [1, %d]", lmax, g->L);
+  if (count < 1) return fail(GSHT_ERR_BAD_ARG, "count %d < 1", count);
+  if (elems) *elems = (long)spec_elems(g, lmax, is_real, count);
+  if (pitch) *pitch = g->theta_pad;
+  return GSHT_OK;
+}
+
+namespace {
+
+// Common checks of the stage entry points: FP64 table form, device buffers
+// of the grid's device, a range inside [0, limit).
+gsht_status stage_check(const gsht_grid* g, int lmax, int n, int is_real, int count, int begin,
+                        int end, int limit, const void* a, const void* b) {
+  gsht_status st = validate(g, lmax, n, is_real, GSHT_FP64, count);
+  if (st != GSHT_OK) return st;
+  if (lmax < 1) return fail(GSHT_ERR_BAD_ARG, "the stages need lmax >= 1");
+  if (begin < 0 || end > limit || begin > end)
+    return fail(GSHT_ERR_BAD_ARG, "range [%d, %d) outside [0, %d)", begin, end, limit);
+  if (!a || !b) return fail(GSHT_ERR_BAD_ARG, "NULL buffer");
+  if (pointer_kind(a, g->device) != kDevicePtr || pointer_kind(b, g->device) != kDevicePtr)
+    return fail(GSHT_ERR_BAD_ARG, "the stages take device buffers of the grid's device (%d)",
+                g->device);
+  return GSHT_OK;
+}
+
+}  // namespace
+
+gsht_status gsht_forward_rings(const gsht_grid* g, int lmax, int is_real, int count,
+                               int ring_begin, int ring_end, const void* grid_values,
+                               void* spectra, void* stream) {
+  const int n = g ? g->min_n : 0;
+  gsht_status st = stage_check(g, lmax, n, is_real, count, ring_begin, ring_end,
+                               g ? g->n_theta : 0, grid_values, spectra);
+  if (st != GSHT_OK) return st;
+  GSHT_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  StageTimer tm(GSHT_STAGE_FFT_FORWARD, s);
+  return fft_forward(g, lmax, is_real, count, static_cast<const double*>(grid_values),
+                     static_cast<double*>(spectra), s, RingRange{ring_begin, ring_end});
+}
+
+gsht_status gsht_inverse_rings(const gsht_grid* g, int lmax, int is_real, int count,
+                               int ring_begin, int ring_end, const void* spectra,
+                               void* grid_values, void* stream) {
+  const int n = g ? g->min_n : 0;
+  gsht_status st = stage_check(g, lmax, n, is_real, count, ring_begin, ring_end,
+                               g ? g->n_theta : 0, spectra, grid_values);
+  if (st != GSHT_OK) return st;
+  GSHT_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  StageTimer tm(GSHT_STAGE_FFT_INVERSE, s);
+  return fft_inverse(g, lmax, is_real, count, static_cast<const double*>(spectra),
+                     static_cast<double*>(grid_values), s, RingRange{ring_begin, ring_end});
+}
+
+gsht_status gsht_forward_orders(const gsht_grid* g, int lmax, int n, int is_real, int count,
+                                int m_begin, int m_end, const void* spectra, void* coef_out,
+                                void* stream) {
+  gsht_status st = stage_check(g, lmax, n, is_real, count, m_begin, m_end, lmax + 1, spectra,
+                               coef_out);
+  if (st != GSHT_OK) return st;
+  const Table* t = g->table(n);
+  if (!t->t64) return fail(GSHT_ERR_UNSUPPORTED, "the order stages need the stored FP64 table");
+  GSHT_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
+  return legendre_forward_fp64(g, t, lmax, is_real, count, static_cast<const double*>(spectra),
+                               static_cast<double*>(coef_out), s, m_begin, m_end);
+}
+
+gsht_status gsht_inverse_orders(const gsht_grid* g, int lmax, int n, int is_real, int count,
+                                int m_begin, int m_end, const void* coef_in, void* spectra,
+                                void* stream) {
+  gsht_status st = stage_check(g, lmax, n, is_real, count, m_begin, m_end, lmax + 1, coef_in,
+                               spectra);
+  if (st != GSHT_OK) return st;
+  const Table* t = g->table(n);
+  if (!t->t64) return fail(GSHT_ERR_UNSUPPORTED, "the order stages need the stored FP64 table");
+  GSHT_CUDA(cudaSetDevice(g->device));
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  gsht_grid* gm = const_cast<gsht_grid*>(g);
+  CallScope scope(gm, s);
+  size_t elems = 0;
+  st = fp64_operand_elems(g, t, lmax, is_real, count, &elems);
+  if (st != GSHT_OK) return st;
+  st = ensure_workspace(gm, sizeof(double) * 2 * elems + 256);
+  if (st != GSHT_OK) return st;
+  if (g->ws_done) GSHT_CUDA(cudaStreamWaitEvent(s, g->ws_done, 0));
+  st = legendre_inverse_fp64(g, t, lmax, is_real, count, static_cast<const double*>(coef_in),
+                             static_cast<double*>(g->ws), static_cast<double*>(spectra), s,
+                             m_begin, m_end);
+  if (st != GSHT_OK) return st;
+  if (!gm->ws_done) GSHT_CUDA(cudaEventCreateWithFlags(&gm->ws_done, cudaEventDisableTiming));
+  GSHT_CUDA(cudaEventRecord(gm->ws_done, s));
+  return GSHT_OK;
+}
+
 gsht_status gsht_forward_batch(const gsht_grid* g, int lmax, int n,
                                int is_real, int precision, int count,
                                const void* in, void* out, void* stream) {
@@ -570,6 +769,10 @@ gsht_status gsht_profile_enable(int on) {
     cudaEventDestroy(r.b);
   }
   g_prof.clear();
+  for (int i = 0; i < GSHT_STAGE_COUNT; i++) {
+    g_prof_ms[i] = 0.0;
+    g_prof_launches[i] = 0;
+  }
   g_prof_on = on != 0;
   return GSHT_OK;
 }
@@ -581,6 +784,10 @@ gsht_status gsht_profile_read(double* ms, long* launches, int nstages) {
     if (launches) launches[i] = 0;
   }
   std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (int i = 0; i < nstages && i < GSHT_STAGE_COUNT; i++) {
+    if (ms) ms[i] = g_prof_ms[i];
+    if (launches) launches[i] = g_prof_launches[i];
+  }
   for (auto& r : g_prof) {
     GSHT_CUDA(cudaEventSynchronize(r.b));
     float t = 0.f;
@@ -609,5 +816,24 @@ gsht_status gsht_device_status(const gsht_grid* g) {
 const char* gsht_last_error(void) { return t_error; }
 
 unsigned long long gsht_launch_count(void) { return g_launches.load(); }
+
+gsht_status gsht_set_allocator(gsht_alloc_fn alloc, gsht_free_fn free_fn, void* ctx) {
+  if ((alloc == nullptr) != (free_fn == nullptr))
+    return fail(GSHT_ERR_BAD_ARG, "give both an allocation and a release function, or neither");
+  std::lock_guard<std::mutex> lk(g_alloc_mu);
+  g_hook.alloc = alloc;
+  g_hook.free = free_fn;
+  g_hook.ctx = ctx;
+  return GSHT_OK;
+}
+
+gsht_status gsht_alloc_stats(unsigned long long* allocations, unsigned long long* releases,
+                             size_t* live_bytes) {
+  std::lock_guard<std::mutex> lk(g_alloc_mu);
+  if (allocations) *allocations = g_alloc_calls;
+  if (releases) *releases = g_free_calls;
+  if (live_bytes) *live_bytes = g_live_bytes;
+  return GSHT_OK;
+}
 
 }  // extern "C"

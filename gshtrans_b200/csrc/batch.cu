@@ -149,12 +149,12 @@ void free_batch(gsht_batch* b) {
     if (b->graph[i]) cudaGraphDestroy(b->graph[i]);
   }
   for (auto& gr : b->groups) {
-    cudaFree(gr.coefIn);
-    cudaFree(gr.gridBuf);
-    cudaFree(gr.coefOut);
-    cudaFree(gr.coefInPtrs);
-    cudaFree(gr.gridPtrs);
-    cudaFree(gr.coefOutPtrs);
+    dev_free(gr.coefIn);
+    dev_free(gr.gridBuf);
+    dev_free(gr.coefOut);
+    dev_free(gr.coefInPtrs);
+    dev_free(gr.gridPtrs);
+    dev_free(gr.coefOutPtrs);
   }
   for (auto& kv : b->grids) gsht_grid_destroy(kv.second);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -162,19 +162,11 @@ void free_batch(gsht_batch* b) {
 }
 
 gsht_status upload_ptrs(double2*** dst, const std::vector<const void*>& host) {
-  GSHT_CUDA(cudaMalloc(dst, sizeof(double2*) * host.size()));
+  GSHT_CUDA(dev_malloc(dst, sizeof(double2*) * host.size()));
   GSHT_CUDA(cudaMemcpy(*dst, host.data(), sizeof(double2*) * host.size(), cudaMemcpyHostToDevice));
   return GSHT_OK;
 }
 
-bool on_device(const void* p) {
-  cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
 
 // Times one round trip of a group (after a warm-up) on the plan's stream.
 gsht_status time_group(gsht_batch* b, Group& gr, float* ms) {
@@ -234,9 +226,9 @@ gsht_status plan(const gsht_field_desc* fields, int count, int precision, int au
     gr.coefElems = coef_size(gr.lmax, gr.n, gr.isReal);
     const long points = (long)(gr.lmax + 1) * 2 * gr.lmax;
     gr.gridElems = gr.isReal ? points / 2 : points;
-    GSHT_CUDA(cudaMalloc(&gr.coefIn, sizeof(double2) * gr.coefElems * k));
-    GSHT_CUDA(cudaMalloc(&gr.gridBuf, sizeof(double2) * gr.gridElems * k));
-    GSHT_CUDA(cudaMalloc(&gr.coefOut, sizeof(double2) * gr.coefElems * k));
+    GSHT_CUDA(dev_malloc(&gr.coefIn, sizeof(double2) * gr.coefElems * k));
+    GSHT_CUDA(dev_malloc(&gr.gridBuf, sizeof(double2) * gr.gridElems * k));
+    GSHT_CUDA(dev_malloc(&gr.coefOut, sizeof(double2) * gr.coefElems * k));
     std::vector<const void*> ci, gp, co;
     for (int i : gr.fields) {
       ci.push_back(b->fields[i].coef_in);
@@ -324,10 +316,13 @@ gsht_status gsht_plan_batch(const gsht_field_desc* fields, int count, int precis
     cudaGetLastError();
     return fail(GSHT_ERR_NO_DEVICE, "no CUDA device visible");
   }
+  int dev = 0;
+  GSHT_CUDA(cudaGetDevice(&dev));
   for (int i = 0; i < count; i++)
-    if (!on_device(fields[i].coef_in) || !on_device(fields[i].grid) ||
-        !on_device(fields[i].coef_out))
-      return fail(GSHT_ERR_BAD_ARG, "field %d: batch buffers must be device memory", i);
+    if (pointer_kind(fields[i].coef_in, dev) != kDevicePtr ||
+        pointer_kind(fields[i].grid, dev) != kDevicePtr ||
+        pointer_kind(fields[i].coef_out, dev) != kDevicePtr)
+      return fail(GSHT_ERR_BAD_ARG, "field %d: batch buffers must be memory of the current device", i);
   auto* b = new gsht_batch();
   const gsht_status st = plan(fields, count, precision, autotune, b);
   if (st != GSHT_OK) {

@@ -149,9 +149,9 @@ template <bool kReal>
 __global__ void __launch_bounds__(256) k_fft_inverse(
     FftPlan plan, int L, int lmax, int nTheta, int thetaPad, int count,
     const double2* __restrict__ spec, const double2* __restrict__ tw,
-    double* __restrict__ out) {
+    double* __restrict__ out, RingRange rr) {
   extern __shared__ double2 smem[];
-  const int j = blockIdx.x, f = blockIdx.y;
+  const int j = blockIdx.x + rr.jBegin, f = blockIdx.y;
   const int nPhi = 2 * L;
   const int sgnCount = kReal ? 1 : 2;
   double2* a = smem;
@@ -197,9 +197,9 @@ template <bool kReal>
 __global__ void __launch_bounds__(256) k_fft_forward(
     FftPlan plan, int L, int lmax, int nTheta, int thetaPad, int count,
     const double* __restrict__ in, const double* __restrict__ weight,
-    const double2* __restrict__ tw, double2* __restrict__ spec) {
+    const double2* __restrict__ tw, double2* __restrict__ spec, RingRange rr) {
   extern __shared__ double2 smem[];
-  const int j = blockIdx.x, f = blockIdx.y;
+  const int j = blockIdx.x + rr.jBegin, f = blockIdx.y;
   const int nPhi = 2 * L;
   const int sgnCount = kReal ? 1 : 2;
   double2* a = smem;
@@ -403,9 +403,9 @@ template <bool kReal, int kVPT>
 __global__ void __launch_bounds__(256) k_fft_inverse_reg(
     FftPlan plan, int R, int L, int lmax, int nTheta, int thetaPad, int count,
     const double2* __restrict__ spec, const double2* __restrict__ tw,
-    double* __restrict__ out) {
+    double* __restrict__ out, RingRange rr) {
   extern __shared__ double2 smem[];
-  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int j0 = (blockIdx.x + rr.jBegin / R) * R, f = blockIdx.y;
   const int nPhi = 2 * L, n = plan.n;
   const int sgnCount = kReal ? 1 : 2;
   auto S = [&](int m, int sgn, int jj) {
@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(256) k_fft_inverse_reg(
   for (int e = threadIdx.x; e < R * n; e += 256) {
     const int r = e / n, k = e - r * n;
     const int j = j0 + r;
-    if (j >= nTheta) continue;
+    if (!rr.has(j)) continue;
     if (!kReal) {
       reinterpret_cast<double2*>(out)[((size_t)f * nTheta + j) * nPhi + k] = smem[pad8(e)];
     } else {
@@ -460,9 +460,9 @@ template <bool kReal, int kVPT>
 __global__ void __launch_bounds__(256) k_fft_forward_reg(
     FftPlan plan, int R, int L, int lmax, int nTheta, int thetaPad, int count,
     const double* __restrict__ in, const double* __restrict__ weight,
-    const double2* __restrict__ tw, double2* __restrict__ spec) {
+    const double2* __restrict__ tw, double2* __restrict__ spec, RingRange rr) {
   extern __shared__ double2 smem[];
-  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int j0 = (blockIdx.x + rr.jBegin / R) * R, f = blockIdx.y;
   const int nPhi = 2 * L, n = plan.n;
   const int sgnCount = kReal ? 1 : 2;
   auto S = [&](int m, int sgn, int jj) -> double2& {
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(256) k_fft_forward_reg(
   for (int e = threadIdx.x; e < R * (lmax + 1); e += 256) {
     const int r = e % R, m = e / R;
     const int j = j0 + r;
-    if (j >= nTheta) continue;
+    if (!rr.has(j)) continue;
     const double scale = weight[j] * twoPiOverN;
     auto X = [&](int b) { return smem[pad8(r * n + b)]; };
     if (!kReal) {
@@ -583,10 +583,10 @@ __device__ __forceinline__ void p2_fft(double2* buf, const double2* __restrict__
 template <bool kReal, int N>
 __global__ void __launch_bounds__(256) k_fft_inverse_p2(
     int L, int lmax, int nTheta, int thetaPad, int count, const double2* __restrict__ spec,
-    const double2* __restrict__ tw, double* __restrict__ out) {
+    const double2* __restrict__ tw, double* __restrict__ out, RingRange rr) {
   extern __shared__ double2 smem[];
   constexpr int R = P2<N>::R;
-  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int j0 = (blockIdx.x + rr.jBegin / R) * R, f = blockIdx.y;
   const int nPhi = 2 * L;
   const int sgnCount = kReal ? 1 : 2;
   const int twStride = nPhi / N;
@@ -628,7 +628,7 @@ __global__ void __launch_bounds__(256) k_fft_inverse_p2(
   for (int e = threadIdx.x; e < R * N; e += 256) {
     const int r = e >> ilog2(N), k = e & (N - 1);
     const int j = j0 + r;
-    if (j >= nTheta) continue;
+    if (!rr.has(j)) continue;
     if (!kReal) {
       reinterpret_cast<double2*>(out)[((size_t)f * nTheta + j) * nPhi + k] = smem[P2<N>::at(r, k)];
     } else {
@@ -641,10 +641,10 @@ template <bool kReal, int N>
 __global__ void __launch_bounds__(256) k_fft_forward_p2(
     int L, int lmax, int nTheta, int thetaPad, int count, const double* __restrict__ in,
     const double* __restrict__ weight, const double2* __restrict__ tw,
-    double2* __restrict__ spec) {
+    double2* __restrict__ spec, RingRange rr) {
   extern __shared__ double2 smem[];
   constexpr int R = P2<N>::R;
-  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int j0 = (blockIdx.x + rr.jBegin / R) * R, f = blockIdx.y;
   const int nPhi = 2 * L;
   const int sgnCount = kReal ? 1 : 2;
   const int twStride = nPhi / N;
@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(256) k_fft_forward_p2(
   for (int e = threadIdx.x; e < R * (lmax + 1); e += 256) {
     const int r = e & (R - 1), m = e >> ilog2(R);
     const int j = j0 + r;
-    if (j >= nTheta) continue;
+    if (!rr.has(j)) continue;
     const double scale = weight[j] * twoPiOverN;
     auto X = [&](int b) { return smem[P2<N>::at(r, b)]; };
     if (!kReal) {
@@ -827,7 +827,7 @@ template <bool kReal, int N, bool kTma, int kPts, typename SpecT>
 __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
     const __grid_constant__ CUtensorMap specMap, int L, int lmax, int nTheta, int thetaPad,
     int count, const SpecT* __restrict__ spec, const double2* __restrict__ tw,
-    double* __restrict__ out, int* err, int smemElems) {
+    double* __restrict__ out, int* err, int smemElems, RingRange rr) {
   constexpr bool kMir = std::is_same<SpecT, double2>::value;
   // TMA destinations want 128-byte alignment: round the dynamic base up (the
   // launch adds 128 bytes of slack plus the barrier word after the buffer).
@@ -836,7 +836,7 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
       (reinterpret_cast<uintptr_t>(p3_raw) + 127) & ~uintptr_t(127));
   uint64_t& bar = *reinterpret_cast<uint64_t*>(smem + smemElems);
   constexpr int R = P3<N, kPts>::R;
-  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int j0 = (blockIdx.x + rr.jBegin / R) * R, f = blockIdx.y;
   const int nPhi = 2 * L;
   const int sgnCount = kReal ? 1 : 2;
   const int twStride = nPhi / N;
@@ -922,7 +922,7 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
     for (int q = 0; q < P; q++) v[q] = smem[P3<N, kPts>::at(ring, k + q * M)];
     dft_reg<P>(v, +1);
     const int th = j0 + ring;
-    if (th < nTheta) {
+    if (rr.has(th)) {
       double2* row = kReal ? reinterpret_cast<double2*>(out + ((size_t)f * nTheta + th) * nPhi)
                            : reinterpret_cast<double2*>(out) + ((size_t)f * nTheta + th) * nPhi;
 #pragma unroll
@@ -936,11 +936,11 @@ template <bool kReal, int N, int kPts, typename SpecT>
 __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
     int L, int lmax, int nTheta, int thetaPad, int count, const double* __restrict__ in,
     const double* __restrict__ weight, const double2* __restrict__ tw,
-    SpecT* __restrict__ spec) {
+    SpecT* __restrict__ spec, RingRange rr) {
   constexpr bool kMir = std::is_same<SpecT, double2>::value;
   extern __shared__ double2 smem[];
   constexpr int R = P3<N, kPts>::R;
-  const int j0 = blockIdx.x * R, f = blockIdx.y;
+  const int j0 = (blockIdx.x + rr.jBegin / R) * R, f = blockIdx.y;
   const int nPhi = 2 * L;
   const int sgnCount = kReal ? 1 : 2;
   const int twStride = nPhi / N;
@@ -987,7 +987,7 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
       for (int q = 0; q < P; q++) v[q] = smem[P3<N, kPts>::at(ring, k + q * M)];
       dft_reg<P>(v, -1);
       const int th = j0 + ring;
-      if (th < nTheta) {
+      if (rr.has(th)) {
         const double scale = weight[th] * twoPiOverN;
 #pragma unroll
         for (int r = 0; r < P; r++) {
@@ -1024,7 +1024,7 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
     for (int e = threadIdx.x; e < R * (lmax + 1); e += P3<N, kPts>::kThreads) {
       const int r = e & (R - 1), m = e >> ilog2(R);
       const int th = j0 + r;
-      if (th >= nTheta) continue;
+      if (!rr.has(th)) continue;
       const double scale = weight[th] * twoPiOverN;
       const int Mh = L;
       const double2 z0 = smem[P3<N, kPts>::at(r, m == Mh ? 0 : m)];
@@ -1058,13 +1058,18 @@ bool spec_map(CUtensorMap* map, const SpecT* spec, int thetaPad, int count, int 
             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Blocks of R rings covering the colatitudes of rr.
+inline unsigned ring_blocks(RingRange rr, int R) {
+  return (unsigned)((rr.jEnd + R - 1) / R - rr.jBegin / R);
+}
+
 template <int N, int kPts, typename SpecT>
 gsht_status launch_p3_dir(const gsht_grid* g, int dir, int lmax, int is_real, int count,
-                          const void* src, void* dst, cudaStream_t s) {
+                          const void* src, void* dst, cudaStream_t s, RingRange rr) {
   constexpr int kThr = P3<N, kPts>::kThreads;
   size_t shmem = sizeof(double2) * P3<N, kPts>::kSmem;
   constexpr int R = P3<N, kPts>::R;
-  dim3 grid((g->n_theta + R - 1) / R, count);
+  dim3 grid(ring_blocks(rr, R), count);
   const double2* tw = reinterpret_cast<const double2*>(g->d_twiddle);
   if (dir == 1) {
     const SpecT* spec = static_cast<const SpecT*>(src);
@@ -1087,13 +1092,13 @@ gsht_status launch_p3_dir(const gsht_grid* g, int dir, int lmax, int is_real, in
                        : k_fft_inverse_p3<false, N, true, kPts, SpecT>;
       GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
       k<<<grid, kThr, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count, spec, tw, out,
-                                  g->d_err, smemElems);
+                                  g->d_err, smemElems, rr);
     } else {
       auto k = is_real ? k_fft_inverse_p3<true, N, false, kPts, SpecT>
                        : k_fft_inverse_p3<false, N, false, kPts, SpecT>;
       GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
       k<<<grid, kThr, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count, spec, tw, out,
-                                  g->d_err, smemElems);
+                                  g->d_err, smemElems, rr);
     }
     GSHT_LAUNCH_CHECK("k_fft_inverse_p3");
   } else {
@@ -1101,7 +1106,7 @@ gsht_status launch_p3_dir(const gsht_grid* g, int dir, int lmax, int is_real, in
     GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
     k<<<grid, kThr, shmem, s>>>(g->L, lmax, g->n_theta, g->theta_pad, count,
                                 static_cast<const double*>(src), g->d_weight, tw,
-                                static_cast<SpecT*>(dst));
+                                static_cast<SpecT*>(dst), rr);
     GSHT_LAUNCH_CHECK("k_fft_forward_p3");
   }
   return GSHT_OK;
@@ -1121,29 +1126,31 @@ constexpr int p3_points() {
 
 template <int N, typename SpecT = double2>
 gsht_status launch_p3(const gsht_grid* g, int dir, int lmax, int is_real, int count,
-                      const void* src, void* dst, cudaStream_t s) {
+                      const void* src, void* dst, cudaStream_t s, RingRange rr) {
   if (dir == 0)
-    return launch_p3_dir<N, p3_points<N, true>(), SpecT>(g, dir, lmax, is_real, count, src, dst, s);
-  return launch_p3_dir<N, p3_points<N, false>(), SpecT>(g, dir, lmax, is_real, count, src, dst, s);
+    return launch_p3_dir<N, p3_points<N, true>(), SpecT>(g, dir, lmax, is_real, count, src, dst, s,
+                                                         rr);
+  return launch_p3_dir<N, p3_points<N, false>(), SpecT>(g, dir, lmax, is_real, count, src, dst, s,
+                                                        rr);
 }
 
 template <int N>
 gsht_status launch_p2(const gsht_grid* g, int dir, int lmax, int is_real, int count,
-                      const double* src, double* dst, cudaStream_t s) {
+                      const double* src, double* dst, cudaStream_t s, RingRange rr) {
   const size_t shmem = sizeof(double2) * P2<N>::kSmem;
-  dim3 grid((g->n_theta + P2<N>::R - 1) / P2<N>::R, count);
+  dim3 grid(ring_blocks(rr, P2<N>::R), count);
   const double2* tw = reinterpret_cast<const double2*>(g->d_twiddle);
   if (dir == 1) {
     auto k = is_real ? k_fft_inverse_p2<true, N> : k_fft_inverse_p2<false, N>;
     GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
     k<<<grid, 256, shmem, s>>>(g->L, lmax, g->n_theta, g->theta_pad, count,
-                               reinterpret_cast<const double2*>(src), tw, dst);
+                               reinterpret_cast<const double2*>(src), tw, dst, rr);
     GSHT_LAUNCH_CHECK("k_fft_inverse_p2");
   } else {
     auto k = is_real ? k_fft_forward_p2<true, N> : k_fft_forward_p2<false, N>;
     GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
     k<<<grid, 256, shmem, s>>>(g->L, lmax, g->n_theta, g->theta_pad, count, src, g->d_weight,
-                               tw, reinterpret_cast<double2*>(dst));
+                               tw, reinterpret_cast<double2*>(dst), rr);
     GSHT_LAUNCH_CHECK("k_fft_forward_p2");
   }
   return GSHT_OK;
@@ -1151,17 +1158,17 @@ gsht_status launch_p2(const gsht_grid* g, int dir, int lmax, int is_real, int co
 
 // Power-of-two paths if n is one of the compiled lengths; *used = false otherwise.
 gsht_status fft_p2(const gsht_grid* g, int n, int dir, int lmax, int is_real, int count,
-                   const double* src, double* dst, cudaStream_t s, bool* used) {
+                   const double* src, double* dst, cudaStream_t s, bool* used, RingRange rr) {
   *used = true;
   switch (n) {
-    case 32: return launch_p2<32>(g, dir, lmax, is_real, count, src, dst, s);
-    case 64: return launch_p2<64>(g, dir, lmax, is_real, count, src, dst, s);
-    case 128: return launch_p2<128>(g, dir, lmax, is_real, count, src, dst, s);
-    case 256: return launch_p3<256>(g, dir, lmax, is_real, count, src, dst, s);
-    case 512: return launch_p3<512>(g, dir, lmax, is_real, count, src, dst, s);
-    case 1024: return launch_p3<1024>(g, dir, lmax, is_real, count, src, dst, s);
-    case 2048: return launch_p3<2048>(g, dir, lmax, is_real, count, src, dst, s);
-    case 4096: return launch_p3<4096>(g, dir, lmax, is_real, count, src, dst, s);
+    case 32: return launch_p2<32>(g, dir, lmax, is_real, count, src, dst, s, rr);
+    case 64: return launch_p2<64>(g, dir, lmax, is_real, count, src, dst, s, rr);
+    case 128: return launch_p2<128>(g, dir, lmax, is_real, count, src, dst, s, rr);
+    case 256: return launch_p3<256>(g, dir, lmax, is_real, count, src, dst, s, rr);
+    case 512: return launch_p3<512>(g, dir, lmax, is_real, count, src, dst, s, rr);
+    case 1024: return launch_p3<1024>(g, dir, lmax, is_real, count, src, dst, s, rr);
+    case 2048: return launch_p3<2048>(g, dir, lmax, is_real, count, src, dst, s, rr);
+    case 4096: return launch_p3<4096>(g, dir, lmax, is_real, count, src, dst, s, rr);
     default: *used = false; return GSHT_OK;
   }
 }
@@ -1201,28 +1208,30 @@ RegConfig reg_config(int n, int tableLen) {
 
 template <int kVPT>
 gsht_status launch_inverse_reg(const gsht_grid* g, const RegConfig& c, int lmax, int is_real,
-                               int count, const double* spec, double* out, cudaStream_t s) {
+                               int count, const double* spec, double* out, cudaStream_t s,
+                               RingRange rr) {
   const size_t shmem = sizeof(double2) * (kVPT * 256 + kVPT * 32);
-  dim3 grid((g->n_theta + c.rings - 1) / c.rings, count);
+  dim3 grid(ring_blocks(rr, c.rings), count);
   auto kr = is_real ? k_fft_inverse_reg<true, kVPT> : k_fft_inverse_reg<false, kVPT>;
   GSHT_CUDA(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
   kr<<<grid, 256, shmem, s>>>(c.plan, c.rings, g->L, lmax, g->n_theta, g->theta_pad, count,
                               reinterpret_cast<const double2*>(spec),
-                              reinterpret_cast<const double2*>(g->d_twiddle), out);
+                              reinterpret_cast<const double2*>(g->d_twiddle), out, rr);
   GSHT_LAUNCH_CHECK("k_fft_inverse_reg");
   return GSHT_OK;
 }
 
 template <int kVPT>
 gsht_status launch_forward_reg(const gsht_grid* g, const RegConfig& c, int lmax, int is_real,
-                               int count, const double* in, double* spec, cudaStream_t s) {
+                               int count, const double* in, double* spec, cudaStream_t s,
+                               RingRange rr) {
   const size_t shmem = sizeof(double2) * (kVPT * 256 + kVPT * 32);
-  dim3 grid((g->n_theta + c.rings - 1) / c.rings, count);
+  dim3 grid(ring_blocks(rr, c.rings), count);
   auto kf = is_real ? k_fft_forward_reg<true, kVPT> : k_fft_forward_reg<false, kVPT>;
   GSHT_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
   kf<<<grid, 256, shmem, s>>>(c.plan, c.rings, g->L, lmax, g->n_theta, g->theta_pad, count,
                               in, g->d_weight, reinterpret_cast<const double2*>(g->d_twiddle),
-                              reinterpret_cast<double2*>(spec));
+                              reinterpret_cast<double2*>(spec), rr);
   GSHT_LAUNCH_CHECK("k_fft_forward_reg");
   return GSHT_OK;
 }
@@ -1230,64 +1239,69 @@ gsht_status launch_forward_reg(const gsht_grid* g, const RegConfig& c, int lmax,
 }  // namespace
 
 gsht_status fft_inverse(const gsht_grid* g, int lmax, int is_real, int count,
-                        const double* spec, double* out, cudaStream_t s) {
+                        const double* spec, double* out, cudaStream_t s, RingRange rr) {
+  rr = resolve(rr, g->n_theta);
+  if (rr.jBegin >= rr.jEnd) return GSHT_OK;
   const int N = g->n_phi;
   bool used = false;
-  gsht_status st = fft_p2(g, is_real ? N / 2 : N, 1, lmax, is_real, count, spec, out, s, &used);
+  gsht_status st =
+      fft_p2(g, is_real ? N / 2 : N, 1, lmax, is_real, count, spec, out, s, &used, rr);
   if (used) return st;
   const RegConfig rc = reg_config(is_real ? N / 2 : N, N);
-  if (rc.vpt == 16) return launch_inverse_reg<16>(g, rc, lmax, is_real, count, spec, out, s);
-  if (rc.vpt == 24) return launch_inverse_reg<24>(g, rc, lmax, is_real, count, spec, out, s);
-  if (rc.vpt == 32) return launch_inverse_reg<32>(g, rc, lmax, is_real, count, spec, out, s);
+  if (rc.vpt == 16) return launch_inverse_reg<16>(g, rc, lmax, is_real, count, spec, out, s, rr);
+  if (rc.vpt == 24) return launch_inverse_reg<24>(g, rc, lmax, is_real, count, spec, out, s, rr);
+  if (rc.vpt == 32) return launch_inverse_reg<32>(g, rc, lmax, is_real, count, spec, out, s, rr);
   const FftPlan plan = make_plan(is_real ? N / 2 : N, N);
   const size_t shmem = sizeof(double2) * 2 * plan.n;
-  dim3 grid(g->n_theta, count);
+  dim3 grid(rr.jEnd - rr.jBegin, count);
   if (is_real) {
     if (shmem > 48 * 1024)
       GSHT_CUDA(cudaFuncSetAttribute(k_fft_inverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
     k_fft_inverse<true><<<grid, 256, shmem, s>>>(
         plan, g->L, lmax, g->n_theta, g->theta_pad, count,
         reinterpret_cast<const double2*>(spec),
-        reinterpret_cast<const double2*>(g->d_twiddle), out);
+        reinterpret_cast<const double2*>(g->d_twiddle), out, rr);
   } else {
     if (shmem > 48 * 1024)
       GSHT_CUDA(cudaFuncSetAttribute(k_fft_inverse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
     k_fft_inverse<false><<<grid, 256, shmem, s>>>(
         plan, g->L, lmax, g->n_theta, g->theta_pad, count,
         reinterpret_cast<const double2*>(spec),
-        reinterpret_cast<const double2*>(g->d_twiddle), out);
+        reinterpret_cast<const double2*>(g->d_twiddle), out, rr);
   }
   GSHT_LAUNCH_CHECK("k_fft_inverse");
   return GSHT_OK;
 }
 
 gsht_status fft_forward(const gsht_grid* g, int lmax, int is_real, int count,
-                        const double* in, double* spec, cudaStream_t s) {
+                        const double* in, double* spec, cudaStream_t s, RingRange rr) {
+  rr = resolve(rr, g->n_theta);
+  if (rr.jBegin >= rr.jEnd) return GSHT_OK;
   const int N = g->n_phi;
   bool used = false;
-  gsht_status st = fft_p2(g, is_real ? N / 2 : N, 0, lmax, is_real, count, in, spec, s, &used);
+  gsht_status st = fft_p2(g, is_real ? N / 2 : N, 0, lmax, is_real, count, in, spec, s, &used, rr);
   if (used) return st;
   const RegConfig rc = reg_config(is_real ? N / 2 : N, N);
-  if (rc.vpt == 16) return launch_forward_reg<16>(g, rc, lmax, is_real, count, in, spec, s);
-  if (rc.vpt == 24) return launch_forward_reg<24>(g, rc, lmax, is_real, count, in, spec, s);
-  if (rc.vpt == 32) return launch_forward_reg<32>(g, rc, lmax, is_real, count, in, spec, s);
+  if (rc.vpt == 16) return launch_forward_reg<16>(g, rc, lmax, is_real, count, in, spec, s, rr);
+  if (rc.vpt == 24) return launch_forward_reg<24>(g, rc, lmax, is_real, count, in, spec, s, rr);
+  if (rc.vpt == 32) return launch_forward_reg<32>(g, rc, lmax, is_real, count, in, spec, s, rr);
   const FftPlan plan = make_plan(is_real ? N / 2 : N, N);
   const size_t shmem = sizeof(double2) * 2 * plan.n;
-  dim3 grid(g->n_theta, count);
+  dim3 grid(rr.jEnd - rr.jBegin, count);
   if (is_real) {
     if (shmem > 48 * 1024)
       GSHT_CUDA(cudaFuncSetAttribute(k_fft_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
     k_fft_forward<true><<<grid, 256, shmem, s>>>(
         plan, g->L, lmax, g->n_theta, g->theta_pad, count, in, g->d_weight,
         reinterpret_cast<const double2*>(g->d_twiddle),
-        reinterpret_cast<double2*>(spec));
+        reinterpret_cast<double2*>(spec), rr);
   } else {
     if (shmem > 48 * 1024)
       GSHT_CUDA(cudaFuncSetAttribute(k_fft_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
     k_fft_forward<false><<<grid, 256, shmem, s>>>(
         plan, g->L, lmax, g->n_theta, g->theta_pad, count, in, g->d_weight,
         reinterpret_cast<const double2*>(g->d_twiddle),
-        reinterpret_cast<double2*>(spec));
+        reinterpret_cast<double2*>(spec), rr);
   }
   GSHT_LAUNCH_CHECK("k_fft_forward");
   return GSHT_OK;
@@ -1302,12 +1316,13 @@ bool fft_spec32_supported(const gsht_grid* g, int is_real) {
 // ring lengths fft_spec32_supported accepts.
 gsht_status fft_spec32(const gsht_grid* g, int dir, int lmax, int is_real, int count,
                        const void* src, void* dst, cudaStream_t s) {
+  const RingRange rr = resolve(RingRange{}, g->n_theta);
   switch (is_real ? g->n_phi / 2 : g->n_phi) {
-    case 256: return launch_p3<256, float2>(g, dir, lmax, is_real, count, src, dst, s);
-    case 512: return launch_p3<512, float2>(g, dir, lmax, is_real, count, src, dst, s);
-    case 1024: return launch_p3<1024, float2>(g, dir, lmax, is_real, count, src, dst, s);
-    case 2048: return launch_p3<2048, float2>(g, dir, lmax, is_real, count, src, dst, s);
-    case 4096: return launch_p3<4096, float2>(g, dir, lmax, is_real, count, src, dst, s);
+    case 256: return launch_p3<256, float2>(g, dir, lmax, is_real, count, src, dst, s, rr);
+    case 512: return launch_p3<512, float2>(g, dir, lmax, is_real, count, src, dst, s, rr);
+    case 1024: return launch_p3<1024, float2>(g, dir, lmax, is_real, count, src, dst, s, rr);
+    case 2048: return launch_p3<2048, float2>(g, dir, lmax, is_real, count, src, dst, s, rr);
+    case 4096: return launch_p3<4096, float2>(g, dir, lmax, is_real, count, src, dst, s, rr);
     default: return fail(GSHT_ERR_UNSUPPORTED, "no FP32-spectrum FFT for this ring length");
   }
 }

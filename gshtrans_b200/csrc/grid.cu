@@ -337,8 +337,8 @@ __global__ void k_slice_i8(int L, int n, int thetaPad,
 
 gsht_status build_nodes(gsht_grid* g) {
   const int nt = g->n_theta;
-  GSHT_CUDA(cudaMalloc(&g->d_theta, sizeof(double) * g->theta_pad));
-  GSHT_CUDA(cudaMalloc(&g->d_weight, sizeof(double) * g->theta_pad));
+  GSHT_CUDA(dev_malloc(&g->d_theta, sizeof(double) * g->theta_pad));
+  GSHT_CUDA(dev_malloc(&g->d_weight, sizeof(double) * g->theta_pad));
   GSHT_CUDA(cudaMemset(g->d_theta, 0, sizeof(double) * g->theta_pad));
   GSHT_CUDA(cudaMemset(g->d_weight, 0, sizeof(double) * g->theta_pad));
   const int pairs = (nt + 1) / 2;
@@ -364,22 +364,22 @@ static gsht_status compute_table(int L, int nTheta, int thetaPad, const double* 
     t->row_off[m + 1] = t->row_off[m] + (L - l0 + 1);
   }
   t->rows = t->row_off[L + 1];
-  GSHT_CUDA(cudaMalloc(&t->d_row_off, sizeof(long long) * (L + 2)));
+  GSHT_CUDA(dev_malloc(&t->d_row_off, sizeof(long long) * (L + 2)));
   GSHT_CUDA(cudaMemcpy(t->d_row_off, t->row_off.data(),
                        sizeof(long long) * (L + 2), cudaMemcpyHostToDevice));
   const size_t elems = (size_t)(t->rows + kTablePadRows) * tp;
-  if (cudaMalloc(&t->t64, sizeof(double) * elems) != cudaSuccess) {
+  if (dev_malloc(&t->t64, sizeof(double) * elems) != cudaSuccess) {
     cudaGetLastError();
     return fail(GSHT_ERR_OOM, "table allocation of %zu bytes failed",
                 sizeof(double) * elems);
   }
   GSHT_CUDA(cudaMemsetAsync(t->t64, 0, sizeof(double) * elems, s));
-  double* start_f = nullptr;
-  int* start_e = nullptr;
-  GSHT_CUDA(cudaMalloc(&start_f, sizeof(double) * (size_t)(L + 1) * tp));
-  GSHT_CUDA(cudaMalloc(&start_e, sizeof(int) * (size_t)(L + 1) * tp));
-  k_wigner_start<<<(nTheta + 127) / 128, 128, 0, s>>>(L, t->n, nTheta, tp, d_theta, start_f,
-                                                      start_e);
+  ScopedDev<double> start_f;
+  ScopedDev<int> start_e;
+  GSHT_CUDA(dev_malloc(&start_f.p, sizeof(double) * (size_t)(L + 1) * tp));
+  GSHT_CUDA(dev_malloc(&start_e.p, sizeof(int) * (size_t)(L + 1) * tp));
+  k_wigner_start<<<(nTheta + 127) / 128, 128, 0, s>>>(L, t->n, nTheta, tp, d_theta, start_f.p,
+                                                      start_e.p);
   GSHT_LAUNCH_CHECK("k_wigner_start");
   const size_t shmem = sizeof(double) * 4 * (L + 1);
   if (shmem > 48 * 1024) {
@@ -388,12 +388,10 @@ static gsht_status compute_table(int L, int nTheta, int thetaPad, const double* 
                                    (int)shmem));
   }
   dim3 grid((tp + 127) / 128, L + 1);
-  k_wigner_chain<<<grid, 128, shmem, s>>>(L, t->n, nTheta, tp, ortho, d_theta, start_f,
-                                          start_e, t->d_row_off, t->t64);
+  k_wigner_chain<<<grid, 128, shmem, s>>>(L, t->n, nTheta, tp, ortho, d_theta, start_f.p,
+                                          start_e.p, t->d_row_off, t->t64);
   GSHT_LAUNCH_CHECK("k_wigner_chain");
   GSHT_CUDA(cudaStreamSynchronize(s));
-  cudaFree(start_f);
-  cudaFree(start_e);
   return GSHT_OK;
 }
 
@@ -448,14 +446,14 @@ gsht_status build_recurrence(gsht_grid* g, Table* t, cudaStream_t s) {
       t->row_off[m + 1] = t->row_off[m] + (L - l0 + 1);
     }
     t->rows = t->row_off[L + 1];
-    GSHT_CUDA(cudaMalloc(&t->d_row_off, sizeof(long long) * (L + 2)));
+    GSHT_CUDA(dev_malloc(&t->d_row_off, sizeof(long long) * (L + 2)));
     GSHT_CUDA(cudaMemcpy(t->d_row_off, t->row_off.data(), sizeof(long long) * (L + 2),
                          cudaMemcpyHostToDevice));
   }
-  if (cudaMalloc(&t->rec_f, sizeof(double) * (size_t)(L + 1) * tp) != cudaSuccess ||
-      cudaMalloc(&t->rec_e, sizeof(int) * (size_t)(L + 1) * tp) != cudaSuccess ||
-      cudaMalloc(&t->rec_ab, sizeof(double2) * (size_t)t->rows) != cudaSuccess ||
-      cudaMalloc(&t->rec_sc, sizeof(double) * (size_t)t->rows) != cudaSuccess) {
+  if (dev_malloc(&t->rec_f, sizeof(double) * (size_t)(L + 1) * tp) != cudaSuccess ||
+      dev_malloc(&t->rec_e, sizeof(int) * (size_t)(L + 1) * tp) != cudaSuccess ||
+      dev_malloc(&t->rec_ab, sizeof(double2) * (size_t)t->rows) != cudaSuccess ||
+      dev_malloc(&t->rec_sc, sizeof(double) * (size_t)t->rows) != cudaSuccess) {
     cudaGetLastError();
     return fail(GSHT_ERR_OOM, "recurrence form allocation failed");
   }
@@ -473,7 +471,7 @@ gsht_status build_forms(gsht_grid* g, Table* t, cudaStream_t s) {
   const int L = g->L, tp = g->theta_pad;
   const size_t plane = (size_t)(t->rows + kTablePadRows) * tp;
   if (g->forms & GSHT_FORM_BF16X3) {
-    if (cudaMalloc(&t->tbf, sizeof(__nv_bfloat16) * 3 * plane) != cudaSuccess) {
+    if (dev_malloc(&t->tbf, sizeof(__nv_bfloat16) * 3 * plane) != cudaSuccess) {
       cudaGetLastError();
       return fail(GSHT_ERR_OOM, "BF16 table allocation failed");
     }
@@ -483,12 +481,12 @@ gsht_status build_forms(gsht_grid* g, Table* t, cudaStream_t s) {
     GSHT_LAUNCH_CHECK("k_split_bf16");
   }
   if (g->forms & GSHT_FORM_OZAKI) {
-    if (cudaMalloc(&t->ti8, (size_t)kTableSlices * plane) != cudaSuccess) {
+    if (dev_malloc(&t->ti8, (size_t)kTableSlices * plane) != cudaSuccess) {
       cudaGetLastError();
       return fail(GSHT_ERR_OOM, "INT8 slice allocation failed");
     }
     GSHT_CUDA(cudaMemsetAsync(t->ti8, 0, (size_t)kTableSlices * plane, s));
-    GSHT_CUDA(cudaMalloc(&t->i8_exp, sizeof(int) * (size_t)(L + 1) * tp));
+    GSHT_CUDA(dev_malloc(&t->i8_exp, sizeof(int) * (size_t)(L + 1) * tp));
     dim3 grid((tp + 127) / 128, L + 1);
     k_slice_i8<<<grid, 128, 0, s>>>(L, t->n, tp, t->d_row_off, t->t64, t->ti8,
                                     plane, t->i8_exp);
@@ -519,8 +517,9 @@ gsht_status wigner_compute(int lmax, int mmax, int nmax, int mrange, int nrange,
   if (count) *count = total;
   if (!out) return GSHT_OK;
   const int tp = (int)round_up(ntheta, kThetaPad);
-  double* d_theta = nullptr;
-  GSHT_CUDA(cudaMalloc(&d_theta, sizeof(double) * tp));
+  ScopedDev<double> dTheta;
+  GSHT_CUDA(dev_malloc(&dTheta.p, sizeof(double) * tp));
+  double* d_theta = dTheta.p;
   GSHT_CUDA(cudaMemset(d_theta, 0, sizeof(double) * tp));
   GSHT_CUDA(cudaMemcpy(d_theta, theta, sizeof(double) * ntheta, cudaMemcpyHostToDevice));
   // Negative orders at n come from the table of -n: d^l_{-m,n} = (-1)^{m+n} d^l_{m,-n}.
@@ -563,20 +562,19 @@ gsht_status wigner_compute(int lmax, int mmax, int nmax, int mrange, int nrange,
     }
   }
   for (auto& t : tabs) free_table(&t);
-  cudaFree(d_theta);
   return st;
 }
 
 void free_table(Table* t) {
-  cudaFree(t->d_row_off);
-  cudaFree(t->t64);
-  cudaFree(t->tbf);
-  cudaFree(t->ti8);
-  cudaFree(t->i8_exp);
-  cudaFree(t->rec_f);
-  cudaFree(t->rec_e);
-  cudaFree(t->rec_ab);
-  cudaFree(t->rec_sc);
+  dev_free(t->d_row_off);
+  dev_free(t->t64);
+  dev_free(t->tbf);
+  dev_free(t->ti8);
+  dev_free(t->i8_exp);
+  dev_free(t->rec_f);
+  dev_free(t->rec_e);
+  dev_free(t->rec_ab);
+  dev_free(t->rec_sc);
   *t = Table{};
 }
 

@@ -21,6 +21,9 @@ namespace gsht {
 gsht_status fail(gsht_status s, const char* fmt, ...);
 gsht_status cuda_fail(cudaError_t e, const char* what);
 extern std::atomic<unsigned long long> g_launches;
+// Launches made by this thread (stage launch counts: exact for the calls of
+// one thread, whichever other threads launch meanwhile).
+extern thread_local unsigned long long t_launches;
 
 #define GSHT_CUDA(call)                                   \
   do {                                                    \
@@ -32,11 +35,41 @@ extern std::atomic<unsigned long long> g_launches;
 #define GSHT_LAUNCH_CHECK(name)                                    \
   do {                                                             \
     gsht::g_launches.fetch_add(1, std::memory_order_relaxed);      \
+    gsht::t_launches++;                                            \
     cudaError_t e_ = cudaGetLastError();                           \
     if (e_ != cudaSuccess) return gsht::cuda_fail(e_, name);       \
   } while (0)
 
 inline long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
+
+// Where a caller's buffer lives, seen from `device`: host memory, memory the
+// device uses in place (its own, or managed), or another GPU's memory
+// (rejected by the entry points: the kernels would read it over a peer
+// mapping that need not exist).
+enum PtrKind { kHostPtr = 0, kDevicePtr = 1, kOtherDevicePtr = 2 };
+PtrKind pointer_kind(const void* p, int device);
+
+// Every device allocation of the library goes through these: the hook of
+// gsht_set_allocator when one is set, else cudaMalloc / cudaFree. A pointer
+// is released by the allocator that made it, even if the hook has changed
+// since. A failed hook allocation reads as cudaErrorMemoryAllocation.
+cudaError_t dev_malloc_bytes(void** p, size_t bytes);
+template <typename T>
+inline cudaError_t dev_malloc(T** p, size_t bytes) {
+  return dev_malloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
+void dev_free(void* p);
+
+// Device scratch of one call, released (dev_free) when it leaves scope, so
+// that every early return of the call gives it back.
+template <typename T>
+struct ScopedDev {
+  T* p = nullptr;
+  ScopedDev() = default;
+  ScopedDev(const ScopedDev&) = delete;
+  ScopedDev& operator=(const ScopedDev&) = delete;
+  ~ScopedDev() { dev_free(p); }
+};
 
 // Brackets one stage of a transform call with CUDA events while stage
 // profiling is enabled (gsht_profile_enable); otherwise does nothing.
@@ -166,11 +199,24 @@ gsht_status wigner_compute(int lmax, int mmax, int nmax, int mrange, int nrange,
                            int row_major, const double* theta, int ntheta, double* out,
                            long* count);
 
+// Colatitudes [jBegin, jEnd) a ring-FFT launch transforms: the whole grid,
+// or one rank's slab of a transform sharded over colatitudes (rings outside
+// the range are not written). jEnd < 0 stands for the whole grid.
+struct RingRange {
+  int jBegin = 0, jEnd = -1;
+  __host__ __device__ bool has(int j) const { return j >= jBegin && j < jEnd; }
+};
+inline RingRange resolve(RingRange r, int nTheta) {
+  if (r.jEnd < 0 || r.jEnd > nTheta) r.jEnd = nTheta;
+  if (r.jBegin < 0) r.jBegin = 0;
+  return r;
+}
+
 // FFT stage (fft.cu). spec: spectral buffer [m][sgn][f][j] complex.
 gsht_status fft_inverse(const gsht_grid* g, int lmax, int is_real, int count,
-                        const double* spec, double* out, cudaStream_t s);
+                        const double* spec, double* out, cudaStream_t s, RingRange rr = {});
 gsht_status fft_forward(const gsht_grid* g, int lmax, int is_real, int count,
-                        const double* in, double* spec, cudaStream_t s);
+                        const double* in, double* spec, cudaStream_t s, RingRange rr = {});
 // FP32 spectra (BF16x3 form): the -m rows are stored at their own
 // colatitudes (no mirror). Ring lengths 256..4096 (powers of two) only.
 bool fft_spec32_supported(const gsht_grid* g, int is_real);
@@ -180,19 +226,22 @@ gsht_status fft_forward32(const gsht_grid* g, int lmax, int is_real, int count, 
                           float* spec, cudaStream_t s);
 
 // Legendre stage, FP64 (legendre_fp64.cu).
-size_t fp64_operand_elems(const gsht_grid* g, const Table* t, int lmax,
-                          int is_real, int count);
+gsht_status fp64_operand_elems(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                               int count, size_t* elems);
+// [mBegin, mEnd): the orders contracted (a rank's share of a transform
+// sharded over orders); mEnd < 0 stands for all orders 0..lmax.
 gsht_status legendre_inverse_fp64(const gsht_grid* g, const Table* t, int lmax,
                                   int is_real, int count, const double* coef,
                                   double* operand, double* spec,
-                                  cudaStream_t s);
+                                  cudaStream_t s, int mBegin = 0, int mEnd = -1);
 // Packed coefficients -> FP64 operand rows op[m][q][k] (the inverse's A).
 gsht_status prep_inverse_fp64(const gsht_grid* g, const Table* t, int lmax, int is_real,
                               int count, const double* coef, double* operand,
-                              const OperandLayout** layout, cudaStream_t s);
+                              const OperandLayout** layout, cudaStream_t s, int mBegin = 0,
+                              int mEnd = -1);
 gsht_status legendre_forward_fp64(const gsht_grid* g, const Table* t, int lmax,
                                   int is_real, int count, const double* spec,
-                                  double* coef, cudaStream_t s);
+                                  double* coef, cudaStream_t s, int mBegin = 0, int mEnd = -1);
 gsht_status legendre_inverse_fp64_layout(const gsht_grid* g, const Table* t, int lmax,
                                          int is_real, int count, const double* coef,
                                          const long long* dOff, const int* dPitch, int kpMax,

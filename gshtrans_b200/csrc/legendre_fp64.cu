@@ -50,6 +50,7 @@ struct Fp64Args {
   const double2* A;          // inverse: operand [m][q][Kp_m]; forward: spec [m][q][thetaPad]
   double2* out;              // inverse: spec; forward: packed coefficients
   long coefSize;
+  int mBegin, mCount;        // orders mBegin .. mBegin + mCount - 1 (a rank's share)
 };
 
 // kDir = 0: inverse (K = degree, N = colatitude; B tile [k][n] from the
@@ -69,7 +70,7 @@ __global__ void __launch_bounds__(256, 2) k_legendre_fp64(Fp64Args p) {
   auto Bs = reinterpret_cast<double(*)[kBTile<kDir>]>(
       fp64_smem + sizeof(double2) * STAGES * BMC * PA);
 
-  const int m = blockIdx.z;
+  const int m = blockIdx.z + p.mBegin;
   const int l0 = m > p.na ? m : p.na;
   const int Keff = p.lmax - l0 + 1;            // degrees l0..lmax
   const int q0 = blockIdx.y * BMC;
@@ -230,7 +231,7 @@ constexpr int kStreamRows = 4;
 template <int kQ>
 __global__ void __launch_bounds__(256) k_legendre_fp64_stream_inv(Fp64Args p) {
   __shared__ double2 As[kQ][256];
-  const int m = blockIdx.y;
+  const int m = blockIdx.y + p.mBegin;
   const int l0 = m > p.na ? m : p.na;
   const int K = p.lmax - l0 + 1;
   const int kp = p.opPitch[m];
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(256) k_legendre_fp64_stream_fwd(Fp64Args p) {
   constexpr int kChunk = 2048 / kQ;  // 32 KB of spectra per block
   __shared__ double2 Fs[kQ][kChunk];
   constexpr int kRowsPerWarp = kFwdRowsPerWarp;
-  const int m = blockIdx.y;
+  const int m = blockIdx.y + p.mBegin;
   const int l0 = m > p.na ? m : p.na;
   const int K = p.lmax - l0 + 1;
   const int kBlock = blockIdx.x * 8 * kRowsPerWarp;
@@ -361,14 +362,14 @@ __global__ void __launch_bounds__(256) k_legendre_fp64_stream_fwd(Fp64Args p) {
 // the DMMA tiles otherwise.
 gsht_status launch_inverse_fp64(const gsht_grid* g, const Fp64Args& a, cudaStream_t s) {
   if (a.Q <= kStreamRows) {
-    dim3 grid((g->n_theta + 255) / 256, a.lmax + 1);
+    dim3 grid((g->n_theta + 255) / 256, a.mCount);
     if (a.Q <= 1) k_legendre_fp64_stream_inv<1><<<grid, 256, 0, s>>>(a);
     else if (a.Q <= 2) k_legendre_fp64_stream_inv<2><<<grid, 256, 0, s>>>(a);
     else k_legendre_fp64_stream_inv<4><<<grid, 256, 0, s>>>(a);
     GSHT_LAUNCH_CHECK("k_legendre_fp64_stream_inv");
     return GSHT_OK;
   }
-  dim3 grid((g->n_theta + BN - 1) / BN, (a.Q + BMC - 1) / BMC, a.lmax + 1);
+  dim3 grid((g->n_theta + BN - 1) / BN, (a.Q + BMC - 1) / BMC, a.mCount);
   GSHT_CUDA(cudaFuncSetAttribute(k_legendre_fp64<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)fp64_smem_bytes<0>()));
   k_legendre_fp64<0><<<grid, 256, fp64_smem_bytes<0>(), s>>>(a);
@@ -384,8 +385,8 @@ __global__ void k_prep_inverse_fp64(int lmax, int n, int na, int count,
                                     const double2* __restrict__ coef,
                                     const long long* __restrict__ opOff,
                                     const int* __restrict__ opPitch,
-                                    double2* __restrict__ op) {
-  const int m = blockIdx.y;
+                                    double2* __restrict__ op, int mBegin) {
+  const int m = blockIdx.y + mBegin;
   const int q = blockIdx.z;
   const int sgn = q / count, f = q - sgn * count;
   const int l0 = m > na ? m : na;
@@ -428,15 +429,15 @@ const OperandLayout* operand_layout(const gsht_grid* g, int lmax, int na,
   }
   o->off[lmax + 1] = acc;
   o->total = acc;
-  if (cudaMalloc(&o->d_off, sizeof(long long) * o->off.size()) != cudaSuccess ||
-      cudaMalloc(&o->d_pitch, sizeof(int) * o->pitch.size()) != cudaSuccess ||
+  if (dev_malloc(&o->d_off, sizeof(long long) * o->off.size()) != cudaSuccess ||
+      dev_malloc(&o->d_pitch, sizeof(int) * o->pitch.size()) != cudaSuccess ||
       cudaMemcpy(o->d_off, o->off.data(), sizeof(long long) * o->off.size(),
                  cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(o->d_pitch, o->pitch.data(), sizeof(int) * o->pitch.size(),
                  cudaMemcpyHostToDevice) != cudaSuccess) {
     cudaGetLastError();
-    cudaFree(o->d_off);
-    cudaFree(o->d_pitch);
+    dev_free(o->d_off);
+    dev_free(o->d_pitch);
     delete o;
     *st = fail(GSHT_ERR_OOM, "operand layout allocation failed");
     return nullptr;
@@ -447,30 +448,33 @@ const OperandLayout* operand_layout(const gsht_grid* g, int lmax, int na,
 
 void free_layouts(gsht_grid* g) {
   for (auto* o : g->layouts) {
-    cudaFree(o->d_off);
-    cudaFree(o->d_pitch);
+    dev_free(o->d_off);
+    dev_free(o->d_pitch);
     delete o;
   }
   g->layouts.clear();
   for (auto* t : g->tile_lists) {
-    cudaFree(t->d_tiles);
+    dev_free(t->d_tiles);
     delete t;
   }
   g->tile_lists.clear();
 }
 
-size_t fp64_operand_elems(const gsht_grid* g, const Table* t, int lmax,
-                          int is_real, int count) {
+gsht_status fp64_operand_elems(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                               int count, size_t* elems) {
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count;
   gsht_status st;
   const OperandLayout* o = operand_layout(g, lmax, na, Q, kDegreePadFp64, &st);
-  return o ? (size_t)o->total : 0;
+  *elems = o ? (size_t)o->total : 0;
+  return st;
 }
 
 gsht_status prep_inverse_fp64(const gsht_grid* g, const Table* t, int lmax, int is_real,
                               int count, const double* coef, double* operand,
-                              const OperandLayout** layout, cudaStream_t s) {
+                              const OperandLayout** layout, cudaStream_t s, int mBegin,
+                              int mEnd) {
+  if (mEnd < 0 || mEnd > lmax + 1) mEnd = lmax + 1;
   const int na = t->n < 0 ? -t->n : t->n;
   const int sgnCount = is_real ? 1 : 2;
   const int Q = sgnCount * count;
@@ -479,11 +483,13 @@ gsht_status prep_inverse_fp64(const gsht_grid* g, const Table* t, int lmax, int 
   if (!lay) return st;
   *layout = lay;
   StageTimer tm(GSHT_STAGE_PREP_INVERSE, s);
-  dim3 pg((lay->pitch_max + 127) / 128, lmax + 1, Q);
+  if (mBegin >= mEnd) return GSHT_OK;
+  dim3 pg((lay->pitch_max + 127) / 128, mEnd - mBegin, Q);
   k_prep_inverse_fp64<<<pg, 128, 0, s>>>(lmax, t->n, na, count, sgnCount, is_real,
                                          coef_size(lmax, t->n, is_real),
                                          reinterpret_cast<const double2*>(coef), lay->d_off,
-                                         lay->d_pitch, reinterpret_cast<double2*>(operand));
+                                         lay->d_pitch, reinterpret_cast<double2*>(operand),
+                                         mBegin);
   GSHT_LAUNCH_CHECK("k_prep_inverse_fp64");
   return GSHT_OK;
 }
@@ -491,12 +497,15 @@ gsht_status prep_inverse_fp64(const gsht_grid* g, const Table* t, int lmax, int 
 gsht_status legendre_inverse_fp64(const gsht_grid* g, const Table* t, int lmax,
                                   int is_real, int count, const double* coef,
                                   double* operand, double* spec,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, int mBegin, int mEnd) {
   const int na = t->n < 0 ? -t->n : t->n;
   const int sgnCount = is_real ? 1 : 2;
   const int Q = sgnCount * count;
+  if (mEnd < 0 || mEnd > lmax + 1) mEnd = lmax + 1;
+  if (mBegin >= mEnd) return GSHT_OK;
   const OperandLayout* lay = nullptr;
-  gsht_status st = prep_inverse_fp64(g, t, lmax, is_real, count, coef, operand, &lay, s);
+  gsht_status st =
+      prep_inverse_fp64(g, t, lmax, is_real, count, coef, operand, &lay, s, mBegin, mEnd);
   if (st != GSHT_OK) return st;
   Fp64Args a{};
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count;
@@ -505,13 +514,17 @@ gsht_status legendre_inverse_fp64(const gsht_grid* g, const Table* t, int lmax,
   a.table = t->t64; a.A = reinterpret_cast<double2*>(operand);
   a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real);
+  a.mBegin = mBegin;
+  a.mCount = mEnd - mBegin;
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
   return launch_inverse_fp64(g, a, s);
 }
 
 gsht_status legendre_forward_fp64(const gsht_grid* g, const Table* t, int lmax,
                                   int is_real, int count, const double* spec,
-                                  double* coef, cudaStream_t s) {
+                                  double* coef, cudaStream_t s, int mBegin, int mEnd) {
+  if (mEnd < 0 || mEnd > lmax + 1) mEnd = lmax + 1;
+  if (mBegin >= mEnd) return GSHT_OK;
   const int na = t->n < 0 ? -t->n : t->n;
   const int sgnCount = is_real ? 1 : 2;
   const int Q = sgnCount * count;
@@ -522,16 +535,18 @@ gsht_status legendre_forward_fp64(const gsht_grid* g, const Table* t, int lmax,
   a.table = t->t64; a.A = reinterpret_cast<const double2*>(spec);
   a.out = reinterpret_cast<double2*>(coef);
   a.coefSize = coef_size(lmax, t->n, is_real);
+  a.mBegin = mBegin;
+  a.mCount = mEnd - mBegin;
   const int kMax = lmax - na + 1;
   if (Q <= kStreamRows) {
-    dim3 sg((kMax + 8 * kFwdRowsPerWarp - 1) / (8 * kFwdRowsPerWarp), lmax + 1);
+    dim3 sg((kMax + 8 * kFwdRowsPerWarp - 1) / (8 * kFwdRowsPerWarp), a.mCount);
     if (Q <= 1) k_legendre_fp64_stream_fwd<1><<<sg, 256, 0, s>>>(a);
     else if (Q <= 2) k_legendre_fp64_stream_fwd<2><<<sg, 256, 0, s>>>(a);
     else k_legendre_fp64_stream_fwd<4><<<sg, 256, 0, s>>>(a);
     GSHT_LAUNCH_CHECK("k_legendre_fp64_stream_fwd");
     return GSHT_OK;
   }
-  dim3 grid((kMax + BN - 1) / BN, (Q + BMC - 1) / BMC, lmax + 1);
+  dim3 grid((kMax + BN - 1) / BN, (Q + BMC - 1) / BMC, a.mCount);
   GSHT_CUDA(cudaFuncSetAttribute(k_legendre_fp64<1>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)fp64_smem_bytes<1>()));
@@ -559,7 +574,7 @@ gsht_status legendre_inverse_fp64_layout(const gsht_grid* g, const Table* t, int
   dim3 pg((kpMax + 127) / 128, lmax + 1, Q);
   k_prep_inverse_fp64<<<pg, 128, 0, s>>>(lmax, t->n, na, count, sgnCount, is_real, cs,
                                          reinterpret_cast<const double2*>(coef), dOff, dPitch,
-                                         op);
+                                         op, 0);
   GSHT_LAUNCH_CHECK("k_prep_inverse_fp64");
   Fp64Args a{};
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count;
@@ -567,6 +582,8 @@ gsht_status legendre_inverse_fp64_layout(const gsht_grid* g, const Table* t, int
   a.isReal = is_real; a.rowOff = t->d_row_off; a.opOff = dOff; a.opPitch = dPitch;
   a.table = t->t64; a.A = op; a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = cs;
+  a.mBegin = 0;
+  a.mCount = lmax + 1;
   return launch_inverse_fp64(g, a, s);
 }
 

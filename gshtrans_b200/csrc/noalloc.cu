@@ -63,14 +63,6 @@ __global__ void k_noalloc_layout(int lmax, int na, int rows, int pad, long long*
   off[lmax + 1] = acc;
 }
 
-bool on_device(const void* p) {
-  cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
 
 }  // namespace
 }  // namespace gsht
@@ -88,8 +80,10 @@ extern "C" gsht_status gsht_inverse_noalloc(const gsht_grid* g, int lmax, int n,
   if (!is_real && g->mrange != GSHT_RANGE_ALL)
     return fail(GSHT_ERR_BAD_ARG, "complex fields need MRange = All");
   GSHT_CUDA(cudaSetDevice(g->device));
-  if (!on_device(in) || !on_device(out))
-    return fail(GSHT_ERR_BAD_ARG, "gsht_inverse_noalloc needs device pointers for in and out");
+  if (pointer_kind(in, g->device) != kDevicePtr || pointer_kind(out, g->device) != kDevicePtr)
+    return fail(GSHT_ERR_BAD_ARG,
+                "gsht_inverse_noalloc needs in and out in the memory of the grid's device (%d)",
+                g->device);
 
   const Table* t = g->table(n);
   if (!t->t64) return fail(GSHT_ERR_UNSUPPORTED, "gsht_inverse_noalloc needs the stored FP64 table");

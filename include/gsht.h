@@ -143,6 +143,46 @@ gsht_status gsht_inverse_batch(const gsht_grid* grid, int lmax, int n,
                                int is_real, int precision, int count,
                                const void* in, void* out, void* stream);
 
+/* Stages of one transform split over several GPUs (ranks): the ring FFTs
+ * shard over colatitudes, the Legendre sums over orders, and the spectra
+ * cross between the two by an all-to-all exchange that the caller runs
+ * (gshtrans_b200.sharded does it over torch.distributed). No counterpart in
+ * the reference, whose transforms loop serially over the rings
+ * (GaussLegendreGrid.h:163, :281). FP64 with the stored table; all buffers
+ * are device memory of the grid's device; work is enqueued on `stream`.
+ *
+ * The spectra buffer (gsht_spectra_layout: `elems` complex doubles, column
+ * pitch `pitch`) is [m][sgn][field][pitch] for m = 0..lmax, sgn = 0 (+m) and,
+ * for complex fields, 1 (-m): column j of a +m row holds ring j, column
+ * nTheta-1-j of a -m row holds ring j (the colatitude mirror); columns
+ * [nTheta, pitch) must hold zeros when gsht_forward_orders reads it.
+ *
+ * gsht_forward_rings: ring FFTs of rings [ring_begin, ring_end) of `count`
+ * fields (full-size grids, other rings not read), weighted by the Gauss
+ * weights and 2 pi / nPhi (GaussLegendreGrid.h:165-178), into their spectra
+ * columns. gsht_forward_orders: the forward Legendre sums of orders
+ * [m_begin, m_end) from complete spectra columns, ADDED into the packed
+ * coefficients like ForwardTransformation (GaussLegendreGrid.h:183-207; the
+ * c_{L,L} = 0 rule is the caller's once the shares are summed).
+ * gsht_inverse_orders: the inverse sums of orders [m_begin, m_end) into the
+ * spectra rows of those orders, every column (GaussLegendreGrid.h:284-312).
+ * gsht_inverse_rings: backward FFTs of rings [ring_begin, ring_end) from
+ * complete spectra rows into those grid rings (GaussLegendreGrid.h:314-319). */
+gsht_status gsht_spectra_layout(const gsht_grid* grid, int lmax, int is_real, int count,
+                                long* elems, int* pitch);
+gsht_status gsht_forward_rings(const gsht_grid* grid, int lmax, int is_real, int count,
+                               int ring_begin, int ring_end, const void* grid_values,
+                               void* spectra, void* stream);
+gsht_status gsht_forward_orders(const gsht_grid* grid, int lmax, int n, int is_real, int count,
+                                int m_begin, int m_end, const void* spectra, void* coef_out,
+                                void* stream);
+gsht_status gsht_inverse_orders(const gsht_grid* grid, int lmax, int n, int is_real, int count,
+                                int m_begin, int m_end, const void* coef_in, void* spectra,
+                                void* stream);
+gsht_status gsht_inverse_rings(const gsht_grid* grid, int lmax, int is_real, int count,
+                               int ring_begin, int ring_end, const void* spectra,
+                               void* grid_values, void* stream);
+
 /* Allocation-free FP64 inverse transform of ONE field. No counterpart in the
  * reference: it serves callers that must not allocate device memory while
  * they transform (an owning arena or caching allocator, a latency-critical
@@ -157,7 +197,10 @@ gsht_status gsht_inverse_batch(const gsht_grid* grid, int lmax, int n,
  * that first call before any stream capture. All calls share the one array
  * and it keeps the last call's contents: calls that overlap on the GPU (on
  * different streams, or different threads) race and corrupt each other;
- * order them. Results equal gsht_inverse with GSHT_FP64. */
+ * order them. CUDA loads the library's device module lazily, so the first
+ * call on a device is also when the 16 MiB are reserved there: make it at
+ * start-up (a failure then reads GSHT_ERR_OOM). The cached address goes
+ * stale after cudaDeviceReset. Results equal gsht_inverse with GSHT_FP64. */
 gsht_status gsht_inverse_noalloc(const gsht_grid* grid, int lmax, int n, int is_real,
                                  const void* in, void* out, void* stream);
 
@@ -174,7 +217,8 @@ gsht_status gsht_inverse_noalloc(const gsht_grid* grid, int lmax, int n, int is_
  * or real doubles; a real output keeps the real part. Runs as one kernel on
  * `stream`: each point reads its inputs once and writes its value once. With
  * device buffers the call only enqueues; host buffers are staged through a
- * library workspace and the call returns with the result in host memory. */
+ * library workspace and the call returns with the result in host memory.
+ * Limits: 64 operations, 16 inputs, a stack 8 values deep. */
 enum {
   GSHT_OP_LOAD = 0, GSHT_OP_CONST = 1, GSHT_OP_ADD = 2, GSHT_OP_SUB = 3,
   GSHT_OP_MUL = 4, GSHT_OP_DIV = 5, GSHT_OP_NEG = 6, GSHT_OP_CONJ = 7,
@@ -232,7 +276,11 @@ gsht_status gsht_batch_destroy(gsht_batch* batch);
  * while enabled, every stage of a transform call is bracketed by CUDA events
  * recorded on the call's stream; gsht_profile_read synchronises those events
  * and returns, per stage, the summed device milliseconds and the number of
- * kernel launches. Enabling clears earlier records. */
+ * kernel launches (counted per calling thread, so exact for each thread's
+ * own calls; a stage's time brackets whatever else runs on its stream
+ * meanwhile). Completed records are folded into per-stage totals, so long
+ * profiled loops hold a bounded number of events. Enabling clears earlier
+ * records. */
 enum {
   GSHT_STAGE_PREP_INVERSE = 0,     /* coefficients -> per-order operand rows   */
   GSHT_STAGE_LEGENDRE_INVERSE = 1, /* order-wise contraction, inverse          */
@@ -253,6 +301,36 @@ gsht_status gsht_profile_read(double* ms, long* launches, int nstages);
  * No counterpart in the reference, which has no device code. Calls with
  * host buffers perform this check themselves. */
 gsht_status gsht_device_status(const gsht_grid* grid);
+
+/* Runs the failure path of the bounded device waits on purpose: one thread
+ * of a one-block kernel waits, with the wait the tensor-core pipelines use,
+ * on an mbarrier phase that nothing completes; after the wait limit (about
+ * half a second) it raises the grid's device error word (code 100) and the
+ * kernel returns. A following gsht_device_status reports GSHT_ERR_TIMEOUT
+ * and clears the word; the context stays usable. No counterpart in the
+ * reference (it has no device code); for checking that a caller's error
+ * handling sees device-side timeouts. Enqueued on `stream`. */
+gsht_status gsht_check_bounded_wait(const gsht_grid* grid, void* stream);
+
+/* Device-memory allocator hook. No counterpart in the reference (its tables
+ * live in host std::vector storage, Wigner.h:126-128). Every device
+ * allocation of the library (grid tables and nodes, workspaces, batch plans,
+ * staging buffers) is made by alloc(bytes, ctx) and released by free_fn(ptr,
+ * ctx) of the hook that made it, even if the hook has been changed since. A
+ * NULL from alloc makes the call that needed the memory return GSHT_ERR_OOM
+ * after releasing what it had taken. For callers whose device memory belongs
+ * to a pool (a caching allocator, an arena). Both NULL restores cudaMalloc /
+ * cudaFree. Change it only while no other thread is inside the library; the
+ * hook is called with the library's allocation lock held, so it must not
+ * call back into the library. */
+typedef void* (*gsht_alloc_fn)(size_t bytes, void* ctx);
+typedef void (*gsht_free_fn)(void* ptr, void* ctx);
+gsht_status gsht_set_allocator(gsht_alloc_fn alloc, gsht_free_fn free_fn, void* ctx);
+
+/* Device allocations and releases the library has made in this process, and
+ * the bytes it holds now (any of the pointers may be NULL). */
+gsht_status gsht_alloc_stats(unsigned long long* allocations, unsigned long long* releases,
+                             size_t* live_bytes);
 
 /* Message describing the last non-OK status returned on this thread. */
 const char* gsht_last_error(void);

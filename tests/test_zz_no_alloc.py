@@ -71,3 +71,38 @@ def test_noalloc_rejects_sizes_beyond_its_scratch_and_host_pointers():
         h = np.zeros(gsht.coefficient_size(64, 0, False), np.complex128)
         st = noalloc(g._h, 64, 0, 0, h.ctypes.data, f.data_ptr(), None)
         assert st == 1
+
+
+def test_noalloc_makes_no_device_allocation_on_a_fresh_grid():
+    # Called first on a grid no other transform has touched (no operand
+    # layout or workspace cached), then three times more: the library's own
+    # allocation counter does not move, and after the first call (which on a
+    # fresh process loads the library's device module and with it the
+    # 16 MiB array) the device's free memory does not change either.
+    import torch
+
+    import gshtrans_b200 as gsht
+
+    noalloc = _entry(gsht.library)
+    rng = np.random.default_rng(77)
+    L, n = 128, 1
+    with gsht.GaussLegendreGrid(L, 1) as g:
+        c = oracle.random_coefficients(rng, L, L, n, False, 1.0)
+        dc = torch.from_numpy(c).cuda()
+        outs = [torch.zeros(g.FieldSize(), dtype=torch.complex128, device="cuda") for _ in range(4)]
+        torch.cuda.synchronize()
+        stats0 = gsht.alloc_stats()
+        s = torch.cuda.current_stream().cuda_stream
+        assert noalloc(g._h, L, n, 0, dc.data_ptr(), outs[0].data_ptr(), s) == 0
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        for k in range(1, 4):
+            assert noalloc(g._h, L, n, 0, dc.data_ptr(), outs[k].data_ptr(), s) == 0
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free0
+        assert gsht.alloc_stats() == stats0
+        g.device_status()
+        want = torch.zeros_like(outs[0])
+        g.InverseTransformation(L, n, dc, want)
+        for k in range(4):
+            assert relerr(outs[k].cpu().numpy(), want.cpu().numpy()) < TOL
