@@ -16,6 +16,7 @@
 // mbarrier wait is bounded (tc_common.cuh) and reports a timeout through
 // the grid's device error word instead of hanging.
 #include <cstdio>
+#include <cstdlib>
 #include <type_traits>
 #include <vector>
 
@@ -54,6 +55,7 @@ struct TcArgs {
 // a separate one, all summed in FP64 in the epilogue (4 x 128 = 512 columns).
 constexpr int kBigAcc = 3;
 constexpr int kAccumulators = kBigAcc + 1;
+constexpr int kNprodTc = 6;  // BF16x3 split products
 
 // Products of the BF16x3 form: (A split, B split).
 __host__ __device__ constexpr int prodA(int p) { return p == 0 ? 0 : p == 1 ? 0 : p == 2 ? 1 : p == 3 ? 0 : p == 4 ? 2 : 1; }
@@ -293,6 +295,271 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // ---------------------------------------------------------------------------
+// CTA-pair form (cta_group::2) for batches of at least 256 field rows. The
+// roles of the operands swap: A is 256 field rows (128 in each CTA of the
+// pair), B a 128-wide tile of the table (64 colatitudes or degrees in each
+// CTA), D = A B^T lands as 128 field rows x 128 table columns in each CTA's
+// TMEM, with the same four accumulators as above (hi.hi by K block, the other
+// five products together). Per tensor-core clock an SM now reads 96 B of
+// operands from shared memory instead of 128 B, and each table tile is
+// fetched once per pair instead of once per 128 field rows.
+//
+// Roles per CTA as in k_legendre_tc: warp 0 loads (TMA into the CTA's own
+// shared memory, counted on the rank-0 CTA's full barrier, no multicast),
+// warp 1 owns TMEM (rank 0 also issues the MMAs for the pair), warps 2-9
+// drain the accumulators. The MMA commits multicast their arrivals to both
+// CTAs' empty / accFull barriers; both CTAs' epilogue warps arrive on the
+// rank-0 accEmpty barriers. Both CTAs of a pair walk the same tiles.
+// ---------------------------------------------------------------------------
+constexpr int kPairM = 256;  // field rows per pair tile
+constexpr int kPairN = 128;  // table columns per pair tile
+
+template <int kDir, int kStages>
+constexpr size_t tc2_smem_bytes() {
+  return (size_t)kStages * 3 * (kBM + kPairN / 2) * bk_of(kDir) * 2 + 1024 + 256;
+}
+
+template <int kDir, int kStages>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_legendre_tc2(const __grid_constant__ CUtensorMap mapT,
+                   const __grid_constant__ CUtensorMap mapF, TcArgs p,
+                   const int4* __restrict__ tiles, int numTiles) {
+  extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
+  constexpr int kBK = bk_of(kDir);
+  constexpr int kTileF = kBM * kBK * 2;          // one split plane of this CTA's field rows
+  constexpr int kTileT = (kPairN / 2) * kBK * 2;  // one split plane of this CTA's table half
+  constexpr int kStageBytes = 3 * kTileF + 3 * kTileT;
+  constexpr int kCols = kPairN / (kEpiWarps / 4);  // 64 accumulator columns per epilogue warp
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* accFull = empty + kStages;
+  uint64_t* accEmptyA = accFull + 1;
+  uint64_t* accEmptyB = accFull + 2;
+  uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(accFull + 3);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  if (pair >= numTiles) return;  // both CTAs of the pair leave together
+
+  if (warp == 0 && lane == 0) {
+    for (int s = 0; s < kStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accFull, 1);
+    mbar_init(accEmptyA, 2 * kEpiWarps);
+    mbar_init(accEmptyB, 2 * kEpiWarps);
+    fence_barrier_init();
+    prefetch_tmap(&mapT);
+    prefetch_tmap(&mapF);
+  }
+  if (warp == 1) tmem_alloc_pair(tmemSlot, kAccumulators * kPairN);
+  tc_fence_before();
+  cluster_sync();  // barriers of both CTAs initialised, TMEM allocated
+  tc_fence_after();
+  const uint32_t tmem = *tmemSlot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      const uint32_t fullRemote0 = cluster_addr(&full[0], 0);
+      int it = 0;
+      bool ok = true;
+      for (int t = pair; t < numTiles && ok; t += npairs) {
+        const int4 tl = tiles[t];  // (m, table tile, field tile, K blocks)
+        const long long tRow = p.rowOff[tl.x];
+        const int fRow = tl.x * p.R + tl.z * kPairM + (int)rank * kBM;
+        for (int kc = 0; kc < tl.w; kc++, it++) {
+          const int s = it % kStages;
+          if (it >= kStages && !mbar_wait(&empty[s], ((it / kStages) - 1) & 1, p.err, 11)) {
+            ok = false;
+            break;
+          }
+          unsigned char* st = smem + s * kStageBytes;
+          const uint32_t fbar = fullRemote0 + (uint32_t)(s * sizeof(uint64_t));
+          // The rank-0 CTA expects the bytes of both CTAs' loads.
+          if (rank == 0) mbar_arrive_expect_tx(&full[s], 2 * kStageBytes);
+          for (int a = 0; a < 3; a++)
+            tma_load_3d_pair(st + a * kTileF, &mapF, fbar, kc * kBK, fRow, a);
+          for (int a = 0; a < 3; a++) {
+            unsigned char* dst = st + 3 * kTileF + a * kTileT;
+            if (kDir == 0) {
+              // MN-major: 64 colatitudes (this CTA's half) x kBK degree rows.
+              tma_load_3d_pair(dst, &mapT, fbar, tl.y * kPairN + (int)rank * (kPairN / 2),
+                               (int)(tRow + kc * kBK), a);
+            } else {
+              // K-major: 64 degree rows (this CTA's half) x kBK colatitudes.
+              tma_load_3d_pair(dst, &mapT, fbar, kc * kBK,
+                               (int)(tRow + tl.y * kPairN + (int)rank * (kPairN / 2)), a);
+            }
+          }
+        }
+      }
+      // Wait until the pair's MMAs have released every stage this CTA
+      // filled, so that no commit arrival is still on its way here when
+      // the CTA leaves.
+      const int pending = it < kStages ? it : kStages;
+      for (int i = it - pending; i < it && ok; i++)
+        if (!mbar_wait(&empty[i % kStages], (i / kStages) & 1, p.err, 16)) ok = false;
+    }
+  } else if (warp == 1) {
+    if (rank == 0 && lane == 0) {
+      constexpr uint32_t id = idesc(1, 1, 0, kDir == 0 ? 1 : 0, kPairN, kPairM);
+      int it = 0, tc = 0;
+      bool ok = true;
+      for (int t = pair; t < numTiles && ok; t += npairs, tc++) {
+        const int nk = tiles[t].w;
+        if (tc > 0 && !mbar_wait(accEmptyA, (tc - 1) & 1, p.err, 14)) break;
+        tc_fence_after();
+        bool haveB = tc == 0;
+        const int nbig = nk < kBigAcc ? nk : kBigAcc;
+        for (int kc = 0; kc < nk; kc++, it++) {
+          const int s = it % kStages;
+          if (!mbar_wait(&full[s], (it / kStages) & 1, p.err, 12)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const int big = 1 + (kc * nbig) / nk;
+          const int bigFirst = ((big - 1) * nk + nbig - 1) / nbig;
+          if (!haveB && big >= 2) {
+            if (!mbar_wait(accEmptyB, (tc - 1) & 1, p.err, 15)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            haveB = true;
+          }
+          const uint32_t st = smem_u32(smem + s * kStageBytes);
+#pragma unroll
+          for (int pr = 0; pr < kNprodTc; pr++) {
+            // A = field rows (split prodB), B = table (split prodA).
+            const uint32_t aBase = st + prodB(pr) * kTileF;
+            const uint32_t bBase = st + 3 * kTileF + prodA(pr) * kTileT;
+            const uint32_t d = tmem + (uint32_t)((pr == 0 ? big : 0) * kPairN);
+#pragma unroll
+            for (int k16 = 0; k16 < kBK / 16; k16++) {
+              uint64_t ad, bd;
+              if constexpr (kDir == 0) {
+                ad = sdesc_sw64(aBase + k16 * 32, 16, 512);
+                bd = sdesc_sw128(bBase + k16 * 2048, kTileT, 1024);
+              } else {
+                ad = sdesc_sw128(aBase + k16 * 32, 16, 1024);
+                bd = sdesc_sw128(bBase + k16 * 32, 16, 1024);
+              }
+              const bool first = pr == 0 ? (kc == bigFirst && k16 == 0)
+                                         : (kc == 0 && k16 == 0 && pr == 1);
+              mma_f16_pair(d, ad, bd, id, first ? 0u : 1u);
+            }
+          }
+          mma_commit_pair(&empty[s], 0x3);
+        }
+        if (ok && !haveB && !mbar_wait(accEmptyB, (tc - 1) & 1, p.err, 15)) ok = false;
+        if (!ok) break;
+        mma_commit_pair(accFull, 0x3);
+      }
+    }
+  } else {
+    // Epilogue warps 2..9: TMEM lane quarter warp % 4 (field rows), column
+    // group (warp - 2) / 4 (64 table columns each).
+    const int quarter = warp & 3;
+    const int group = (warp - 2) >> 2;
+    const int row = quarter * 32 + lane;
+    const uint32_t emptyA0 = cluster_addr(accEmptyA, 0), emptyB0 = cluster_addr(accEmptyB, 0);
+    int tc = 0;
+    for (int t = pair; t < numTiles; t += npairs, tc++) {
+      const int4 tl = tiles[t];
+      const int m = tl.x, nk = tl.w;
+      if (!mbar_wait(accFull, tc & 1, p.err, 13)) break;
+      tc_fence_after();
+      const int nbig = nk < kBigAcc ? nk : kBigAcc;
+      double acc[kCols];
+#pragma unroll
+      for (int i = 0; i < kCols; i++) acc[i] = 0.0;
+      const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + group * kCols;
+      auto drain = [&](int a) {
+#pragma unroll
+        for (int c = 0; c < kCols / 16; c += 2) {
+          uint32_t v0[16], v1[16];
+          tmem_ld16(tbase + a * kPairN + c * 16, v0);
+          tmem_ld16(tbase + a * kPairN + (c + 1) * 16, v1);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; i++) {
+            acc[c * 16 + i] += (double)__uint_as_float(v0[i]);
+            acc[(c + 1) * 16 + i] += (double)__uint_as_float(v1[i]);
+          }
+        }
+      };
+      drain(0);
+      drain(1);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(emptyA0);
+#pragma unroll
+      for (int a = 2; a <= kBigAcc; a++)
+        if (a <= nbig) drain(a);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(emptyB0);
+      // Field row r of this lane, and its partner (the other part of the
+      // same complex row q) in the neighbouring lane.
+      const int r = tl.z * kPairM + (int)rank * kBM + row;
+      const int q = r >> 1, part = r & 1;
+      const int l0 = m > p.na ? m : p.na;
+      const int keff = p.lmax - l0 + 1;
+      const int c0 = tl.y * kPairN + group * kCols;  // first table column of this warp
+      const int limit = kDir == 0 ? p.nTheta : keff;
+      // Even lanes write columns [0, kCols/2), odd lanes [kCols/2, kCols):
+      // at step j the even lane needs the partner's column j, the odd lane
+      // the partner's column kCols/2 + j.
+      constexpr int kHalf = kCols / 2;
+      const bool rowOk = q < p.Q;
+      const int cBase = c0 + (part ? kHalf : 0);
+#pragma unroll
+      for (int j = 0; j < kHalf; j += 2) {
+        double2 v[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const double send = part ? acc[j + u] : acc[kHalf + j + u];
+          const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
+          v[u] = part ? make_double2(recv, acc[kHalf + j + u]) : make_double2(acc[j + u], recv);
+        }
+        if (!rowOk) continue;
+        const int col = cBase + j;
+        if (kDir == 0 && p.out32) {
+          float2* rowp = p.out32 + ((size_t)m * p.Q + q) * p.thetaPad;
+          if (q < p.count && col + 1 < limit) {
+            *reinterpret_cast<float4*>(rowp + col) =
+                make_float4((float)v[0].x, (float)v[0].y, (float)v[1].x, (float)v[1].y);
+          } else {
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+              if (col + u >= limit) continue;
+              const int cc = q >= p.count ? p.nTheta - 1 - (col + u) : col + u;
+              rowp[cc] = make_float2((float)v[u].x, (float)v[u].y);
+            }
+          }
+        } else {
+          double2* rowp = p.out + ((size_t)m * p.Q + q) * p.thetaPad;
+#pragma unroll
+          for (int u = 0; u < 2; u++)
+            if (col + u < limit) rowp[col + u] = v[u];
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  cluster_sync();  // no arrival is still on its way into either CTA
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc_pair(tmem, kAccumulators * kPairN);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Field-side operands: BF16 hi/mid/lo planes of the real rows r = 2q + part.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void split3(double x, __nv_bfloat16& h, __nv_bfloat16& md,
@@ -490,6 +757,56 @@ gsht_status launch_bf16(const gsht_grid* g, int ntile, const TcArgs& a, const CU
   return launch_bf16_n<kDir, 128>(g, a, mapA, mapB, s);
 }
 
+// The CTA-pair kernels serve batches of at least kPairM field rows. By
+// default the forward takes them and the inverse keeps the one-CTA kernel
+// (measured at lmax 1024, 64 fields: forward 1.69 against 1.75 ms, inverse
+// 2.12 against 1.84 ms); GSHT_BF16X3_PAIR=0 / =1 selects the one-CTA / pair
+// kernels for both directions (comparisons and tests).
+bool pair_form(int R, int dir) {
+  if (R < kPairM) return false;
+  const char* e = getenv("GSHT_BF16X3_PAIR");
+  if (e && e[0] == '0') return false;
+  if (e && e[0] == '1') return true;
+  return dir == 1;
+}
+
+template <int kDir>
+gsht_status launch_bf16_pair(const gsht_grid* g, const TcArgs& a, const CUtensorMap& mapT,
+                             const CUtensorMap& mapF, cudaStream_t s) {
+  gsht_status st;
+  // (m, 128-wide table tile, 256-row field tile, K blocks), table tiles innermost.
+  const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kPairM, bk_of(kDir), &st);
+  if (!tl) return st;
+  constexpr int kSt = kDir == 0 ? 5 : 3;
+  auto kern = k_legendre_tc2<kDir, kSt>;
+  const size_t sm = tc2_smem_bytes<kDir, kSt>();
+  GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg{};
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+  cfg.gridDim = dim3(sms & ~1);
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess || clusters < 1) {
+    cudaGetLastError();
+    clusters = sms / 2;
+  }
+  const int pairs = tl->count < clusters ? tl->count : clusters;
+  cfg.gridDim = dim3(2 * pairs);
+  GSHT_CUDA(cudaLaunchKernelEx(&cfg, kern, mapT, mapF, a, (const int4*)tl->d_tiles, tl->count));
+  GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_tc2<inverse,bf16x3>" : "k_legendre_tc2<forward,bf16x3>");
+  return GSHT_OK;
+}
+
 }  // namespace
 
 // Tiles (m, M tile, N tile, K blocks), N tiles innermost: neighbouring
@@ -515,11 +832,11 @@ const TileList* tile_list(const gsht_grid* g, int dir, int lmax, int na, int row
   auto* t = new TileList();
   t->dir = dir; t->lmax = lmax; t->na = na; t->rows = rows; t->ntile = ntile; t->kstep = kstep;
   t->count = (int)v.size();
-  if (cudaMalloc(&t->d_tiles, sizeof(int4) * v.size()) != cudaSuccess ||
+  if (dev_malloc(&t->d_tiles, sizeof(int4) * v.size()) != cudaSuccess ||
       cudaMemcpy(t->d_tiles, v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice) !=
           cudaSuccess) {
     cudaGetLastError();
-    cudaFree(t->d_tiles);
+    dev_free(t->d_tiles);
     delete t;
     *st = fail(GSHT_ERR_OOM, "tile list allocation failed");
     return nullptr;
@@ -556,8 +873,9 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
   gsht_status st = make_map_bf16(&mapA, t->tbf, g->theta_pad, t->rows + kTablePadRows, 3,
                                  g->theta_pad, tplane, 64, kBKInv, CU_TENSOR_MAP_SWIZZLE_128B);
   if (st != GSHT_OK) return st;
-  st = make_map_bf16(&mapB, op, pitch, (uint64_t)(lmax + 1) * R, 3, pitch, plane, kBKInv, ntile,
-                     CU_TENSOR_MAP_SWIZZLE_64B);
+  const bool pairForm = pair_form(R, 0);
+  st = make_map_bf16(&mapB, op, pitch, (uint64_t)(lmax + 1) * R, 3, pitch, plane, kBKInv,
+                     pairForm ? kBM : ntile, CU_TENSOR_MAP_SWIZZLE_64B);
   if (st != GSHT_OK) return st;
   TcArgs a{};
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count; a.Q = Q; a.R = R;
@@ -566,6 +884,7 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
   a.out32 = spec32 ? reinterpret_cast<float2*>(spec) : nullptr;
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
+  if (pairForm) return launch_bf16_pair<0>(g, a, mapA, mapB, s);
   return launch_bf16<0>(g, ntile, a, mapA, mapB, s);
 }
 
@@ -591,11 +910,15 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
   }
   CUtensorMap mapA, mapB;
   const size_t tplane = (size_t)(t->rows + kTablePadRows) * tp;
+  const bool pairForm = pair_form(R, 1);
+  // Table boxes: 128 degree rows (one CTA's M), or 64 (one CTA's half of a
+  // pair's 128-wide table tile).
   gsht_status st = make_map_bf16(&mapA, t->tbf, tp, t->rows + kTablePadRows, 3, tp, tplane,
-                                 bk_of(1), kBM, CU_TENSOR_MAP_SWIZZLE_128B);
+                                 bk_of(1), pairForm ? kPairN / 2 : kBM,
+                                 CU_TENSOR_MAP_SWIZZLE_128B);
   if (st != GSHT_OK) return st;
-  st = make_map_bf16(&mapB, op, tp, (uint64_t)(lmax + 1) * R, 3, tp, plane, bk_of(1), ntile,
-                     CU_TENSOR_MAP_SWIZZLE_128B);
+  st = make_map_bf16(&mapB, op, tp, (uint64_t)(lmax + 1) * R, 3, tp, plane, bk_of(1),
+                     pairForm ? kBM : ntile, CU_TENSOR_MAP_SWIZZLE_128B);
   if (st != GSHT_OK) return st;
   TcArgs a{};
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count; a.Q = Q; a.R = R;
@@ -606,7 +929,8 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   {
     StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
-    st = launch_bf16<1>(g, ntile, a, mapA, mapB, s);
+    st = pairForm ? launch_bf16_pair<1>(g, a, mapA, mapB, s)
+                  : launch_bf16<1>(g, ntile, a, mapA, mapB, s);
   }
   if (st != GSHT_OK) return st;
   return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, tp, spec, coef, s);

@@ -1,0 +1,75 @@
+"""BF16x3 Legendre stage in its CTA-pair form (tcgen05 cta_group::2), the
+form batches of at least 256 field rows take: A = 256 field rows split over
+the two CTAs of a cluster, B = a 128-wide table tile split likewise, four
+TMEM accumulators per CTA. Checked against the FP64 path at the BF16x3
+tier (<= 1e-6 inverse, 2e-6 forward) and against the one-CTA form of the
+same products (GSHT_BF16X3_PAIR=1 forces the pair form in both directions,
+=0 the one-CTA form) on the same inputs: the results are bit-identical. Shapes: 64 complex
+fields (exactly one pair tile of field rows), 65 (a second, mostly empty
+field tile), 128 real fields; odd and even colatitude counts; upper indices
+0 and -2; lmax < L."""
+
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import relerr
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def gsht():
+    import gshtrans_b200
+
+    return gshtrans_b200
+
+
+def _round(g, L, lmax, n, is_real, c, prec):
+    import torch
+
+    dc = torch.from_numpy(c).cuda()
+    B = c.shape[0]
+    f = torch.zeros((B, g.FieldSize()), dtype=torch.float64 if is_real else torch.complex128,
+                    device="cuda")
+    g.inverse_batch(lmax, n, dc, f, prec)
+    back = torch.zeros_like(dc)
+    g.forward_batch(lmax, n, f, back, prec)
+    torch.cuda.synchronize()
+    g.device_status()
+    return f.cpu().numpy(), back.cpu().numpy()
+
+
+@pytest.mark.parametrize("L,lmax,n,is_real,B", [
+    (128, 128, 0, False, 64),
+    (256, 256, -2, False, 65),
+    (200, 200, 0, True, 128),
+    (512, 400, 2, False, 64),
+    (1024, 1024, 0, False, 64),
+])
+def test_pair_form_matches_fp64_and_the_one_cta_form(gsht, L, lmax, n, is_real, B):
+    rng = np.random.default_rng(L + B + int(is_real))
+    c = np.stack([oracle.random_coefficients(rng, L, lmax, n, is_real, 1.5) for _ in range(B)])
+    with gsht.GaussLegendreGrid(L, 2, forms=("bf16x3",)) as g:
+        f64, b64 = _round(g, L, lmax, n, is_real, c, "fp64")
+        try:
+            os.environ["GSHT_BF16X3_PAIR"] = "1"
+            fp, bp = _round(g, L, lmax, n, is_real, c, "bf16x3")
+            os.environ["GSHT_BF16X3_PAIR"] = "0"
+            f1, b1 = _round(g, L, lmax, n, is_real, c, "bf16x3")
+        finally:
+            del os.environ["GSHT_BF16X3_PAIR"]
+    # the forward's input is each form's own inverse, so compare the forward
+    # through the round trip and the inverse directly
+    assert relerr(fp, f64) < TOL, "inverse vs FP64"
+    assert relerr(bp, b64) < 3 * TOL, "round trip vs FP64"
+    assert np.array_equal(fp, f1), "inverse vs one-CTA form"
+    assert np.array_equal(bp, b1), "round trip vs one-CTA form"
+    print(f"L={L} B={B} real={is_real}: pair vs one-CTA inverse {relerr(fp, f1):.2e}, "
+          f"vs FP64 {relerr(fp, f64):.2e} (one-CTA {relerr(f1, f64):.2e})")
