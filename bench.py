@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--lmax", type=int, default=L_MAX)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-secondary", action="store_true",
+                   help="skip the batch / large / pipeline workloads the default run adds")
     p.add_argument("--workload", default="headline",
                    choices=["headline", "batch", "large", "pipeline"],
                    help="headline: 64 fields at lmax 1024 (the metric); batch: 256 fields of "
@@ -512,8 +514,11 @@ def impl_ours(args):
             "clocks": res["clocks"], "gpu_launches": res["launches"],
             "round_trip_rel_err": res["round_trip_rel_err"], "modes": mode_lines,
         }
-        print(json.dumps(result))
     grid.close()
+    if rank == 0:
+        if world == 1 and not args.no_secondary:
+            result["secondary"] = secondary_workloads(args)
+        print(json.dumps(result))
     if world > 1:
         dist.destroy_process_group()
     return 0
@@ -589,7 +594,7 @@ def _event_time(torch, fn, steps, warmup):
     return e0.elapsed_time(e1) / steps
 
 
-def impl_batch(args):
+def impl_batch(args, emit=True):
     """256 fields, lmax uniform in {32, 64, 128, 256, 512}, upper index uniform
     in -2..2, half real; envelope 1/(l+1); each on its own grid. One round
     trip (inverse then forward) of all fields per step: one CUDA graph launch
@@ -646,19 +651,23 @@ def impl_batch(args):
     tiles = {}
     for lm, n, re, cnt, tile in batch.groups():
         tiles[tile] = tiles.get(tile, 0) + 1
-    print(json.dumps({
+    line = {
         "metric": "batched uneven fields, fwd+inv/s (one CUDA graph per step)",
         "value": 256 / (ms_graph * 1e-3), "unit": UNIT, "ms_per_step": ms_graph,
         "per_field_calls": {"value": 256 / (ms_single * 1e-3), "ms_per_step": ms_single},
         "speedup_vs_per_field_calls": ms_single / ms_graph,
         "precision": prec, "round_trip_rel_err_vs_fp64": err,
         "groups": groups, "grids": grids, "graph_nodes_round_trip": nodes[2],
-        "autotuned_tile_widths": tiles, "plan_seconds": plan_s,
+        "autotuned_tile_widths": tiles, "autotuned_streams": batch.streams(),
+        "plan_seconds": plan_s,
         "config": {"workload": "256 fields, lmax in {32,64,128,256,512}, n in -2..2, half real, "
                                "envelope (l+1)^-1, own grid per field", "steps": args.steps,
                    "warmup": args.warmup},
-    }))
+    }
     batch.close()
+    if not emit:
+        return line
+    print(json.dumps(line))
     return 0
 
 
@@ -667,7 +676,7 @@ def table_rows(L, n):
     return sum(L + 1 - max(m, na) for m in range(L + 1))
 
 
-def impl_large(args):
+def impl_large(args, emit=True):
     """One complex field at lmax 2048 (nTheta 2049, nPhi 4096), n = 1,
     envelope (l+1)^-2: table streaming, reported in GB/s of the stored table
     form read per transform; and the same transforms with the Wigner values
@@ -737,19 +746,22 @@ def impl_large(args):
         fo, co = ref[prec]
         res[prec]["inverse_rel_err_vs_fp64"] = float(torch.linalg.norm(fo - f64) / torch.linalg.norm(f64))
         res[prec]["forward_rel_err_vs_fp64"] = float(torch.linalg.norm(co - c64) / torch.linalg.norm(c64))
-    print(json.dumps({
+    line = {
         "metric": f"lmax {L} single field: table streaming GB/s", "unit": "GB/s",
         "value": res["fp64"]["inverse_table_GBps"], "modes": res, "hbm_peak_GBps": hbm,
         "grid_build_seconds": build_s, "fp64_table_bytes": fp64_table_bytes,
         "config": {"workload": f"1 complex field, lmax {L} (nTheta {L + 1}, nPhi {2 * L}), n=1, "
                                "envelope (l+1)^-2", "table_rows": rows, "theta_pad": tp},
-    }))
+    }
     grid.close()
     rgrid.close()
+    if not emit:
+        return line
+    print(json.dumps(line))
     return 0
 
 
-def impl_pipeline(args):
+def impl_pipeline(args, emit=True):
     """64 pairs (u: n = +1, v: n = -1) at lmax 768 (nPhi 1536 = 2^9 x 3):
     inverse both, w = u v + conj(u) u (the conjugate taken with upper index
     -1, so both terms have n = 0) fused in one kernel, forward w."""
@@ -757,7 +769,7 @@ def impl_pipeline(args):
     import gshtrans_b200 as gsht
     from gshtrans_b200 import fields as F
 
-    L, B = 768, 64
+    L, B = 768, args.fields
     rng = np.random.default_rng(768)
     U = torch.from_numpy(np.stack([gsht.random_coefficients(rng, L, L, 1, False, 1.5)
                                    for _ in range(B)])).cuda()
@@ -806,15 +818,38 @@ def impl_pipeline(args):
                   "achieved_gbs": gbs, "peak_gbs": hbm,
                   "frac": gbs / hbm if hbm else None,
                   "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
-    print(json.dumps({
+    line = {
         "metric": "field-product pipeline pairs/s (2 inverses, fused u*v + conj(u)*u, 1 forward)",
         "unit": "pairs/s", "value": out["ozaki"]["pairs_per_s"], "modes": out,
         "field_eval": field_eval,
-        "config": {"workload": "64 pairs, lmax 768 (nTheta 769, nPhi 1536), u n=+1, v n=-1, "
+        "config": {"workload": f"{B} pairs, lmax 768 (nTheta 769, nPhi 1536), u n=+1, v n=-1, "
                                "envelope (l+1)^-1.5", "steps": args.steps, "warmup": args.warmup},
-    }))
+    }
     grid.close()
+    if not emit:
+        return line
+    print(json.dumps(line))
     return 0
+
+
+def secondary_workloads(args):
+    """The other workloads of the task, measured in the same run with a few
+    steps each (their own lines come from --workload batch | large |
+    pipeline): 256 uneven fields in one graph, one field at lmax 2048, the
+    field-product pipeline at lmax 768."""
+    import copy
+
+    out = {}
+    for name, fn in (("batch", impl_batch), ("large", impl_large), ("pipeline", impl_pipeline)):
+        a = copy.copy(args)
+        a.steps, a.warmup = 5, 3
+        a.precision = None
+        a.fields = FIELDS
+        try:
+            out[name] = fn(a, emit=False)
+        except Exception as e:  # report, do not lose the headline line
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+    return out
 
 
 def main():

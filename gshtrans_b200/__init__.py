@@ -466,6 +466,7 @@ library.gsht_batch_execute.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_v
 library.gsht_batch_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_long)]
 library.gsht_batch_group.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.POINTER(ctypes.c_int)] * 5
+library.gsht_batch_schedule.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
 library.gsht_batch_destroy.argtypes = [ctypes.c_void_p]
 
 BATCH_FORWARD, BATCH_INVERSE, BATCH_ROUND_TRIP = 0, 1, 2
@@ -525,6 +526,12 @@ class Batch:
 
     def round_trip(self):
         self._run(BATCH_ROUND_TRIP)
+
+    def streams(self) -> int:
+        """Streams the plan's graphs spread the groups over (gsht_batch_schedule)."""
+        k = ctypes.c_int()
+        _check(library.gsht_batch_schedule(self._h, ctypes.byref(k)))
+        return k.value
 
     def info(self):
         """(groups, grids, graph nodes per mode [forward, inverse, round trip])."""

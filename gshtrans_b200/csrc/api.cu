@@ -260,7 +260,7 @@ struct CallScope {
 
 gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
                           int precision, int count, const void* in, void* out,
-                          void* stream_ptr, int ntile = 128) {
+                          void* stream_ptr, int ntile = 128, PrivateWorkspace* pws = nullptr) {
   gsht_status st = validate(g, lmax, n, is_real, precision, count);
   if (st != GSHT_OK) return st;
   GSHT_CUDA(cudaSetDevice(g->device));
@@ -326,13 +326,25 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
   auto carve = [&](size_t b) { size_t o = off; off += round_up(b, 256); return o; };
   const size_t oSpec = carve(specBytes), oOp = carve(opBytes);
   const size_t oIn = carve(inDev ? 0 : inBytes), oOut = carve(outDev ? 0 : outBytes);
-  if (capturing && g->ws_bytes < (off > 0 ? off : 256))
-    return fail(GSHT_ERR_UNSUPPORTED, "workspace must be sized by an uncaptured call first");
-  st = ensure_workspace(g, off > 0 ? off : 256);
-  if (st != GSHT_OK) return st;
-  char* ws = static_cast<char*>(g->ws);
-  // Calls on other streams may still use the workspace: order after them.
-  if (g->ws_done && !capturing) GSHT_CUDA(cudaStreamWaitEvent(s, g->ws_done, 0));
+  const bool priv = pws != nullptr;
+  if (priv && pws->need) {  // size query only
+    *pws->need = off > 0 ? off : 256;
+    return GSHT_OK;
+  }
+  char* ws = nullptr;
+  if (priv) {
+    if (!pws->ptr || pws->bytes < off)
+      return fail(GSHT_ERR_BAD_ARG, "private workspace of %zu bytes, %zu needed", pws->bytes, off);
+    ws = static_cast<char*>(pws->ptr);
+  } else {
+    if (capturing && g->ws_bytes < (off > 0 ? off : 256))
+      return fail(GSHT_ERR_UNSUPPORTED, "workspace must be sized by an uncaptured call first");
+    st = ensure_workspace(g, off > 0 ? off : 256);
+    if (st != GSHT_OK) return st;
+    ws = static_cast<char*>(g->ws);
+    // Calls on other streams may still use the workspace: order after them.
+    if (g->ws_done && !capturing) GSHT_CUDA(cudaStreamWaitEvent(s, g->ws_done, 0));
+  }
 
   const double* dIn = inDev ? static_cast<const double*>(in) : reinterpret_cast<double*>(ws + oIn);
   double* dOut = outDev ? static_cast<double*>(out) : reinterpret_cast<double*>(ws + oOut);
@@ -432,7 +444,7 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
       return st;
     }
   }
-  if (!capturing) {
+  if (!capturing && !priv) {
     if (!g->ws_done) GSHT_CUDA(cudaEventCreateWithFlags(&g->ws_done, cudaEventDisableTiming));
     GSHT_CUDA(cudaEventRecord(g->ws_done, s));
   }
@@ -451,8 +463,9 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
 }  // namespace
 
 gsht_status transform(gsht_grid* g, int dir, int lmax, int n, int is_real, int precision,
-                      int count, const void* in, void* out, cudaStream_t s, int ntile) {
-  return run_transform(g, dir, lmax, n, is_real, precision, count, in, out, s, ntile);
+                      int count, const void* in, void* out, cudaStream_t s, int ntile,
+                      PrivateWorkspace* pws) {
+  return run_transform(g, dir, lmax, n, is_real, precision, count, in, out, s, ntile, pws);
 }
 
 }  // namespace gsht

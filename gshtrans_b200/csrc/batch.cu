@@ -15,6 +15,11 @@
 //   - autotunes, for the BF16x3 form, the field-row tile width of the
 //     tensor-core kernels per group (32, 64 or 128 columns: small groups
 //     waste fewer MMA columns with narrow tiles) by timing each candidate;
+//   - gives every group its own workspace, so that groups run concurrently
+//     on several streams (groups of the same degree share only read-only
+//     tables), and autotunes that schedule too: the number of streams the
+//     groups are spread over (largest groups first), by timing the captured
+//     round-trip graph of each candidate;
 //   - captures the whole sequence (gathers, transforms, scatters) for each
 //     direction into a CUDA graph, so an execution is one graph launch.
 #include <algorithm>
@@ -27,6 +32,8 @@
 
 namespace gsht {
 namespace {
+
+constexpr int kMaxLanes = 16;  // streams a batch graph spreads its groups over
 
 // Copies `count` vectors of `elems` 16-byte elements between callers'
 // buffers and a contiguous batch buffer; mode 0: gather (dst contiguous),
@@ -66,6 +73,9 @@ struct Group {
   double2** coefInPtrs = nullptr;     // callers' pointers (device arrays)
   double2** gridPtrs = nullptr;
   double2** coefOutPtrs = nullptr;
+  void* ws = nullptr;                 // private workspace of the group's transforms
+  size_t wsBytes = 0;
+  double work = 0.0;                  // estimated cost (fields x lmax^3), for the schedule
 };
 
 }  // namespace
@@ -77,6 +87,9 @@ struct gsht_batch {
   std::map<int, gsht_grid*> grids;  // by degree
   std::vector<gsht::Group> groups;
   cudaStream_t stream = nullptr;
+  std::vector<cudaStream_t> lanes;     // streams the groups are spread over
+  std::vector<cudaEvent_t> laneDone;   // join events (one per lane) and the fork event
+  int nlanes = 1;                      // chosen by the schedule autotuner
   cudaGraph_t graph[3] = {nullptr, nullptr, nullptr};
   cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
   size_t nodes[3] = {0, 0, 0};
@@ -105,8 +118,9 @@ gsht_status run_group(gsht_batch* b, Group& gr, int dir, bool gather, bool scatt
   if (dir == 1) {
     if (gather && (st = copy_group(gr, 0, gr.coefElems, gr.coefInPtrs, gr.coefIn, s)) != GSHT_OK)
       return st;
+    PrivateWorkspace pw{gr.ws, gr.wsBytes, nullptr};
     st = transform(gr.grid, 1, gr.lmax, gr.n, gr.isReal, b->precision, count, gr.coefIn,
-                   gr.gridBuf, s, gr.ntile);
+                   gr.gridBuf, s, gr.ntile, &pw);
     if (st != GSHT_OK) return st;
     if (scatter && (st = copy_group(gr, 1, gr.gridElems, gr.gridPtrs, gr.gridBuf, s)) != GSHT_OK)
       return st;
@@ -114,8 +128,9 @@ gsht_status run_group(gsht_batch* b, Group& gr, int dir, bool gather, bool scatt
     if (gather && (st = copy_group(gr, 0, gr.gridElems, gr.gridPtrs, gr.gridBuf, s)) != GSHT_OK)
       return st;
     GSHT_CUDA(cudaMemsetAsync(gr.coefOut, 0, sizeof(double2) * gr.coefElems * count, s));
+    PrivateWorkspace pw{gr.ws, gr.wsBytes, nullptr};
     st = transform(gr.grid, 0, gr.lmax, gr.n, gr.isReal, b->precision, count, gr.gridBuf,
-                   gr.coefOut, s, gr.ntile);
+                   gr.coefOut, s, gr.ntile, &pw);
     if (st != GSHT_OK) return st;
     // Every field's lmax is its grid's degree, so complex fields get c_{L,L} = 0.
     const int mode = gr.isReal ? 2 : 3;
@@ -125,17 +140,38 @@ gsht_status run_group(gsht_batch* b, Group& gr, int dir, bool gather, bool scatt
   return GSHT_OK;
 }
 
-// Everything one execution of `mode` does (0 forward, 1 inverse, 2 inverse
-// then forward, the grids of the round trip also written back).
-gsht_status run_all(gsht_batch* b, int mode, cudaStream_t s) {
+// userIO: read and write the callers' buffers (false for the tuning runs,
+// which must leave them untouched).
+gsht_status run_one(gsht_batch* b, Group& gr, int mode, cudaStream_t s, bool userIO) {
   gsht_status st;
-  for (auto& gr : b->groups) {
-    if (mode == 2) {
-      if ((st = run_group(b, gr, 1, true, true, s)) != GSHT_OK) return st;
-      if ((st = run_group(b, gr, 0, false, true, s)) != GSHT_OK) return st;
-    } else if ((st = run_group(b, gr, mode, true, true, s)) != GSHT_OK) {
-      return st;
-    }
+  if (mode == 2) {
+    if ((st = run_group(b, gr, 1, userIO, userIO, s)) != GSHT_OK) return st;
+    return run_group(b, gr, 0, false, userIO, s);
+  }
+  return run_group(b, gr, mode, userIO, userIO, s);
+}
+
+// Everything one execution of `mode` does (0 forward, 1 inverse, 2 inverse
+// then forward, the grids of the round trip also written back), with the
+// groups (ordered largest first) dealt round-robin over `lanes` streams
+// forked from and joined back into s.
+gsht_status run_all(gsht_batch* b, int mode, cudaStream_t s, int lanes, bool userIO = true) {
+  gsht_status st;
+  if (lanes <= 1) {
+    for (auto& gr : b->groups)
+      if ((st = run_one(b, gr, mode, s, userIO)) != GSHT_OK) return st;
+    return GSHT_OK;
+  }
+  cudaEvent_t fork = b->laneDone[0];
+  GSHT_CUDA(cudaEventRecord(fork, s));
+  for (int i = 0; i < lanes; i++) GSHT_CUDA(cudaStreamWaitEvent(b->lanes[i], fork, 0));
+  for (size_t gi = 0; gi < b->groups.size(); gi++) {
+    st = run_one(b, b->groups[gi], mode, b->lanes[gi % lanes], userIO);
+    if (st != GSHT_OK) return st;
+  }
+  for (int i = 0; i < lanes; i++) {
+    GSHT_CUDA(cudaEventRecord(b->laneDone[1 + i], b->lanes[i]));
+    GSHT_CUDA(cudaStreamWaitEvent(s, b->laneDone[1 + i], 0));
   }
   return GSHT_OK;
 }
@@ -155,8 +191,11 @@ void free_batch(gsht_batch* b) {
     dev_free(gr.coefInPtrs);
     dev_free(gr.gridPtrs);
     dev_free(gr.coefOutPtrs);
+    dev_free(gr.ws);
   }
   for (auto& kv : b->grids) gsht_grid_destroy(kv.second);
+  for (cudaStream_t l : b->lanes) cudaStreamDestroy(l);
+  for (cudaEvent_t e : b->laneDone) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -242,7 +281,22 @@ gsht_status plan(const gsht_field_desc* fields, int count, int precision, int au
     // Defined batch inputs for the warm-up and tuning runs.
     GSHT_CUDA(cudaMemsetAsync(gr.coefIn, 0, sizeof(double2) * gr.coefElems * k, b->stream));
     GSHT_CUDA(cudaMemsetAsync(gr.gridBuf, 0, sizeof(double2) * gr.gridElems * k, b->stream));
+    // The group's own workspace: the larger of the two directions' needs.
+    size_t needInv = 0, needFwd = 0;
+    PrivateWorkspace qi{nullptr, 0, &needInv}, qf{nullptr, 0, &needFwd};
+    if ((st = transform(gr.grid, 1, gr.lmax, gr.n, gr.isReal, precision, k, gr.coefIn,
+                        gr.gridBuf, b->stream, gr.ntile, &qi)) != GSHT_OK ||
+        (st = transform(gr.grid, 0, gr.lmax, gr.n, gr.isReal, precision, k, gr.gridBuf,
+                        gr.coefOut, b->stream, gr.ntile, &qf)) != GSHT_OK)
+      return st;
+    gr.wsBytes = std::max(needInv, needFwd);
+    GSHT_CUDA(dev_malloc(&gr.ws, gr.wsBytes));
+    gr.work = (double)k * (gr.lmax + 1.0) * (gr.lmax + 1.0) * (gr.lmax + 1.0) * (gr.isReal ? 0.5 : 1.0);
   }
+  // Largest groups first: with the round-robin over streams the long
+  // transforms start early and the small ones fill in behind them.
+  std::stable_sort(b->groups.begin(), b->groups.end(),
+                   [](const Group& x, const Group& y) { return x.work > y.work; });
   // Warm-up (sizes every workspace, builds tile lists and layouts), then
   // the autotuner: per group, the fastest BF16x3 tile width.
   for (auto& gr : b->groups) {
@@ -269,17 +323,76 @@ gsht_status plan(const gsht_field_desc* fields, int count, int precision, int au
     gsht_status st = gsht_device_status(kv.second);
     if (st != GSHT_OK) return st;
   }
-  // One graph per execution mode.
-  for (int mode = 0; mode < 3; mode++) {
+  // Streams for the concurrent schedule and their fork / join events.
+  const int maxLanes = (int)std::min<size_t>(kMaxLanes, b->groups.size());
+  for (int i = 0; i < maxLanes; i++) {
+    cudaStream_t l;
+    GSHT_CUDA(cudaStreamCreateWithFlags(&l, cudaStreamNonBlocking));
+    b->lanes.push_back(l);
+  }
+  for (int i = 0; i <= maxLanes; i++) {
+    cudaEvent_t e;
+    GSHT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->laneDone.push_back(e);
+  }
+  // Schedule autotuner: the round-trip graph for each candidate number of
+  // streams, timed over a few launches; the fastest count is used for all
+  // three modes.
+  auto capture = [&](int mode, int lanes, cudaGraph_t* graph, bool userIO) -> gsht_status {
     GSHT_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
-    gsht_status st = run_all(b, mode, b->stream);
-    cudaGraph_t graph = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+    gsht_status st = run_all(b, mode, b->stream, lanes, userIO);
+    *graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->stream, graph);
     if (st != GSHT_OK) {
-      if (graph) cudaGraphDestroy(graph);
+      if (*graph) cudaGraphDestroy(*graph);
+      *graph = nullptr;
       return st;
     }
     if (e != cudaSuccess) return cuda_fail(e, "batch graph capture");
+    return GSHT_OK;
+  };
+  b->nlanes = 1;
+  if (maxLanes > 1 && autotune) {
+    float best = 3.4e38f;
+    for (int lanes : {1, 2, 4, 8, 16}) {
+      if (lanes > maxLanes) break;
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      // Timed without the callers' buffers (no gathers or scatters).
+      gsht_status st = capture(2, lanes, &graph, false);
+      if (st != GSHT_OK) return st;
+      if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return cuda_fail(cudaGetLastError(), "batch graph instantiation");
+      }
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      cudaGraphLaunch(exec, b->stream);
+      cudaEventRecord(e0, b->stream);
+      for (int r = 0; r < 3; r++) cudaGraphLaunch(exec, b->stream);
+      cudaEventRecord(e1, b->stream);
+      const cudaError_t se = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      cudaGraphExecDestroy(exec);
+      cudaGraphDestroy(graph);
+      if (se != cudaSuccess) return cuda_fail(se, "batch schedule tuning");
+      if (ms < best) {
+        best = ms;
+        b->nlanes = lanes;
+      }
+    }
+  } else if (maxLanes > 1) {
+    b->nlanes = std::min(maxLanes, 8);
+  }
+  // One graph per execution mode.
+  for (int mode = 0; mode < 3; mode++) {
+    cudaGraph_t graph = nullptr;
+    gsht_status st = capture(mode, b->nlanes, &graph, true);
+    if (st != GSHT_OK) return st;
     b->graph[mode] = graph;
     GSHT_CUDA(cudaGraphGetNodes(graph, nullptr, &b->nodes[mode]));
     GSHT_CUDA(cudaGraphInstantiate(&b->exec[mode], graph, 0));
@@ -364,6 +477,12 @@ gsht_status gsht_batch_group(const gsht_batch* b, int index, int* lmax, int* n, 
   if (is_real) *is_real = gr.isReal;
   if (count) *count = (int)gr.fields.size();
   if (ntile) *ntile = gr.ntile;
+  return GSHT_OK;
+}
+
+gsht_status gsht_batch_schedule(const gsht_batch* b, int* streams) {
+  if (!b) return fail(GSHT_ERR_BAD_ARG, "batch is NULL");
+  if (streams) *streams = b->nlanes;
   return GSHT_OK;
 }
 

@@ -22,6 +22,8 @@
 #include <cstring>
 #include <type_traits>
 
+#include <cstdlib>
+
 #include "gsht_internal.cuh"
 #include "tc_common.cuh"
 

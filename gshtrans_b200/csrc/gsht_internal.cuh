@@ -250,10 +250,19 @@ gsht_status legendre_inverse_fp64_layout(const gsht_grid* g, const Table* t, int
 // Legendre stage, BF16x3 on tcgen05 (legendre_tc.cu). dir 0 = forward
 // (operand rows over colatitudes), 1 = inverse (rows over degrees).
 size_t bf16_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir);
+// A workspace owned by the caller of transform() instead of the grid's (so
+// that transforms on one grid can run concurrently on several streams). With
+// `need` set, transform() only stores the bytes it would use there.
+struct PrivateWorkspace {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  size_t* need = nullptr;
+};
 // One batched transform (the body of gsht_forward_batch / gsht_inverse_batch)
 // with an explicit BF16x3 tile width; dir 0 forward, 1 inverse.
 gsht_status transform(gsht_grid* g, int dir, int lmax, int n, int is_real, int precision,
-                      int count, const void* in, void* out, cudaStream_t s, int ntile);
+                      int count, const void* in, void* out, cudaStream_t s, int ntile,
+                      PrivateWorkspace* pws = nullptr);
 // spec32: the spectra are FP32 with unmirrored -m rows (fft_inverse32 /
 // fft_forward32); the buffer is still sized for FP64 spectra.
 gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,

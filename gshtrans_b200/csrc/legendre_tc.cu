@@ -29,14 +29,16 @@ namespace {
 using namespace tc;
 
 constexpr int kBM = 128;       // tile rows (TMEM lanes)
-// K per stage. Inverse: 32 degrees (the MN-major table tile is two
-// 64-colatitude x 32-degree boxes with 128 B swizzle, the K-major field rows
-// one 64 B swizzle row), four 48 KB stages in flight. Forward: 64
-// colatitudes = one 128 B swizzle row of both K-major operands, two 96 KB
-// stages.
+// K per stage. Forward: 64 colatitudes = one 128 B swizzle row of both
+// K-major operands, two 96 KB stages. Inverse: 32 degrees (the MN-major
+// table tile is two 64-colatitude x 32-degree boxes with 128 B swizzle, the
+// K-major field rows one 64 B swizzle row), four 48 KB stages; or, selected
+// at run time (inverse_bk), 64 degrees in two 96 KB stages like the forward.
 __host__ __device__ constexpr int bk_of(int dir) { return dir == 0 ? 32 : 64; }
-__host__ __device__ constexpr int stages_of(int dir) { return dir == 0 ? 4 : 2; }
-constexpr int kBKInv = bk_of(0);
+__host__ __device__ constexpr int stages_for(int bk) { return bk == 32 ? 4 : 2; }
+// The inverse's field operand rows are padded to a multiple of 64 degrees
+// (zeros), which serves both K steps.
+constexpr int kBKInv = 64;
 
 struct TcArgs {
   int L, lmax, n, na, count, Q, R, nTheta, thetaPad, isReal;
@@ -73,7 +75,7 @@ constexpr int kThreads = 32 * (2 + kEpiWarps);
 // The producer runs ahead across tile boundaries; the epilogue copies its
 // accumulator columns out of TMEM, releases TMEM to the MMA warp (accEmpty),
 // and only then writes results, so stores overlap the next tile's MMAs.
-template <int kDir, int kNA, int kNB, int kNP, int kN, int kStages>
+template <int kDir, int kNA, int kNB, int kNP, int kN, int kStages, int kBK>
 __global__ void __launch_bounds__(kThreads, 1)
     k_legendre_tc(const __grid_constant__ CUtensorMap mapA,
                   const __grid_constant__ CUtensorMap mapB, TcArgs p,
@@ -81,7 +83,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
-  constexpr int kBK = bk_of(kDir);
   constexpr int kTileA = kBM * kBK * 2;
   constexpr int kTileB = kN * kBK * 2;
   constexpr int kStageBytes = kNA * kTileA + kNB * kTileB;
@@ -193,7 +194,8 @@ __global__ void __launch_bounds__(kThreads, 1)
               uint64_t ad, bd;
               if constexpr (kDir == 0) {
                 ad = sdesc_sw128(aBase + k16 * 2048, kTileA / 2, 1024);
-                bd = sdesc_sw64(bBase + k16 * 32, 16, 512);
+                bd = kBK == 32 ? sdesc_sw64(bBase + k16 * 32, 16, 512)
+                               : sdesc_sw128(bBase + k16 * 32, 16, 1024);
               } else {
                 ad = sdesc_sw128(aBase + k16 * 32, 16, 1024);
                 bd = sdesc_sw128(bBase + k16 * 32, 16, 1024);
@@ -314,12 +316,12 @@ __global__ void __launch_bounds__(kThreads, 1)
 constexpr int kPairM = 256;  // field rows per pair tile
 constexpr int kPairN = 128;  // table columns per pair tile
 
-template <int kDir, int kStages>
+template <int kStages, int kBK>
 constexpr size_t tc2_smem_bytes() {
-  return (size_t)kStages * 3 * (kBM + kPairN / 2) * bk_of(kDir) * 2 + 1024 + 256;
+  return (size_t)kStages * 3 * (kBM + kPairN / 2) * kBK * 2 + 1024 + 256;
 }
 
-template <int kDir, int kStages>
+template <int kDir, int kStages, int kBK>
 __global__ void __launch_bounds__(kThreads, 1)
     k_legendre_tc2(const __grid_constant__ CUtensorMap mapT,
                    const __grid_constant__ CUtensorMap mapF, TcArgs p,
@@ -327,7 +329,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
-  constexpr int kBK = bk_of(kDir);
   constexpr int kTileF = kBM * kBK * 2;          // one split plane of this CTA's field rows
   constexpr int kTileT = (kPairN / 2) * kBK * 2;  // one split plane of this CTA's table half
   constexpr int kStageBytes = 3 * kTileF + 3 * kTileT;
@@ -443,7 +444,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int k16 = 0; k16 < kBK / 16; k16++) {
               uint64_t ad, bd;
               if constexpr (kDir == 0) {
-                ad = sdesc_sw64(aBase + k16 * 32, 16, 512);
+                ad = kBK == 32 ? sdesc_sw64(aBase + k16 * 32, 16, 512)
+                               : sdesc_sw128(aBase + k16 * 32, 16, 1024);
                 bd = sdesc_sw128(bBase + k16 * 2048, kTileT, 1024);
               } else {
                 ad = sdesc_sw128(aBase + k16 * 32, 16, 1024);
@@ -728,16 +730,17 @@ gsht_status make_map_bf16(CUtensorMap* map, const void* base, uint64_t inner, ui
 
 constexpr int kNsplit = 3, kNprod = 6;
 
-template <int kDir, int kN>
+template <int kDir, int kN, int kBK>
 gsht_status launch_bf16_n(const gsht_grid* g, const TcArgs& a, const CUtensorMap& mapA,
                           const CUtensorMap& mapB, cudaStream_t s) {
   gsht_status st;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
-  const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kN, bk_of(kDir), &st);
+  const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kN, kBK, &st);
   if (!tl) return st;
-  auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kN, stages_of(kDir)>;
-  const size_t sm = tc_smem_bytes<kNsplit, kNsplit, kN, bk_of(kDir), stages_of(kDir)>();
+  constexpr int kSt = stages_for(kBK);
+  auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kN, kSt, kBK>;
+  const size_t sm = tc_smem_bytes<kNsplit, kNsplit, kN, kBK, kSt>();
   GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int blocks = tl->count < sms ? tl->count : sms;
   kern<<<blocks, kThreads, sm, s>>>(mapA, mapB, a, tl->d_tiles, tl->count);
@@ -749,12 +752,25 @@ gsht_status launch_bf16_n(const gsht_grid* g, const TcArgs& a, const CUtensorMap
 // waste fewer MMA columns on small batches (chosen by the batch autotuner).
 bool valid_ntile(int ntile) { return ntile == 32 || ntile == 64 || ntile == 128; }
 
-template <int kDir>
+template <int kDir, int kBK>
 gsht_status launch_bf16(const gsht_grid* g, int ntile, const TcArgs& a, const CUtensorMap& mapA,
                         const CUtensorMap& mapB, cudaStream_t s) {
-  if (ntile == 32) return launch_bf16_n<kDir, 32>(g, a, mapA, mapB, s);
-  if (ntile == 64) return launch_bf16_n<kDir, 64>(g, a, mapA, mapB, s);
-  return launch_bf16_n<kDir, 128>(g, a, mapA, mapB, s);
+  if (ntile == 32) return launch_bf16_n<kDir, 32, kBK>(g, a, mapA, mapB, s);
+  if (ntile == 64) return launch_bf16_n<kDir, 64, kBK>(g, a, mapA, mapB, s);
+  return launch_bf16_n<kDir, 128, kBK>(g, a, mapA, mapB, s);
+}
+
+// K step of the inverse kernels: 32 or 64 degrees per stage
+// (GSHT_BF16X3_INV_K=32 / 64 for comparisons; default kInverseBK). Measured
+// at lmax 1024, 64 fields: 64 runs the inverse in 1.70 against 1.82 ms but
+// forward+inverse round trip then differs from the input by 9.3e-7 against
+// 8.7e-7 (relative), so 32 keeps the wider margin under 1e-6.
+constexpr int kInverseBK = 32;
+int inverse_bk() {
+  const char* e = getenv("GSHT_BF16X3_INV_K");
+  if (e && atoi(e) == 64) return 64;
+  if (e && atoi(e) == 32) return 32;
+  return kInverseBK;
 }
 
 // The CTA-pair kernels serve batches of at least kPairM field rows. By
@@ -770,16 +786,16 @@ bool pair_form(int R, int dir) {
   return dir == 1;
 }
 
-template <int kDir>
+template <int kDir, int kBK>
 gsht_status launch_bf16_pair(const gsht_grid* g, const TcArgs& a, const CUtensorMap& mapT,
                              const CUtensorMap& mapF, cudaStream_t s) {
   gsht_status st;
   // (m, 128-wide table tile, 256-row field tile, K blocks), table tiles innermost.
-  const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kPairM, bk_of(kDir), &st);
+  const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kPairM, kBK, &st);
   if (!tl) return st;
-  constexpr int kSt = kDir == 0 ? 5 : 3;
-  auto kern = k_legendre_tc2<kDir, kSt>;
-  const size_t sm = tc2_smem_bytes<kDir, kSt>();
+  constexpr int kSt = kBK == 32 ? 5 : 3;
+  auto kern = k_legendre_tc2<kDir, kSt, kBK>;
+  const size_t sm = tc2_smem_bytes<kSt, kBK>();
   GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -862,20 +878,24 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
   auto* op = static_cast<__nv_bfloat16*>(operand);
   {
     StageTimer tm(GSHT_STAGE_PREP_INVERSE, s);
-    dim3 pg((lmax + 63) / 32, (lmax + 32) / 32, Q);
+    // Degrees up to l0 + kp - 1 <= lmax + kBKInv - 1: the zero padding of
+    // every order's row up to its K-step multiple is written too.
+    dim3 pg((lmax + kBKInv + 31) / 32, (lmax + 32) / 32, Q);
     k_prep_inverse_bf16<<<pg, 256, 0, s>>>(lmax, t->n, na, count, Q, R, is_real,
                                            coef_size(lmax, t->n, is_real), pitch, plane,
                                            reinterpret_cast<const double2*>(coef), op);
     GSHT_LAUNCH_CHECK("k_prep_inverse_bf16");
   }
   CUtensorMap mapA, mapB;
+  const int bk = inverse_bk();
   const size_t tplane = (size_t)(t->rows + kTablePadRows) * g->theta_pad;
   gsht_status st = make_map_bf16(&mapA, t->tbf, g->theta_pad, t->rows + kTablePadRows, 3,
-                                 g->theta_pad, tplane, 64, kBKInv, CU_TENSOR_MAP_SWIZZLE_128B);
+                                 g->theta_pad, tplane, 64, bk, CU_TENSOR_MAP_SWIZZLE_128B);
   if (st != GSHT_OK) return st;
   const bool pairForm = pair_form(R, 0);
-  st = make_map_bf16(&mapB, op, pitch, (uint64_t)(lmax + 1) * R, 3, pitch, plane, kBKInv,
-                     pairForm ? kBM : ntile, CU_TENSOR_MAP_SWIZZLE_64B);
+  st = make_map_bf16(&mapB, op, pitch, (uint64_t)(lmax + 1) * R, 3, pitch, plane, bk,
+                     pairForm ? kBM : ntile,
+                     bk == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B);
   if (st != GSHT_OK) return st;
   TcArgs a{};
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count; a.Q = Q; a.R = R;
@@ -884,8 +904,11 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
   a.out32 = spec32 ? reinterpret_cast<float2*>(spec) : nullptr;
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
-  if (pairForm) return launch_bf16_pair<0>(g, a, mapA, mapB, s);
-  return launch_bf16<0>(g, ntile, a, mapA, mapB, s);
+  if (bk == 64)
+    return pairForm ? launch_bf16_pair<0, 64>(g, a, mapA, mapB, s)
+                    : launch_bf16<0, 64>(g, ntile, a, mapA, mapB, s);
+  return pairForm ? launch_bf16_pair<0, 32>(g, a, mapA, mapB, s)
+                  : launch_bf16<0, 32>(g, ntile, a, mapA, mapB, s);
 }
 
 gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
@@ -929,8 +952,8 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   {
     StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
-    st = pairForm ? launch_bf16_pair<1>(g, a, mapA, mapB, s)
-                  : launch_bf16<1>(g, ntile, a, mapA, mapB, s);
+    st = pairForm ? launch_bf16_pair<1, 64>(g, a, mapA, mapB, s)
+                  : launch_bf16<1, 64>(g, ntile, a, mapA, mapB, s);
   }
   if (st != GSHT_OK) return st;
   return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, tp, spec, coef, s);

@@ -11,9 +11,12 @@ transforms with the grid's table of n = alpha; ``VectorExpansion`` holds the
 three coefficient sets and runs the three transforms (each batched over
 ``count`` fields) on the caller's stream.
 
-Complex-valued fields only: the canonical components of a vector field are
-complex in general (the reference's real-valued branch treats them as plain
-reals, VectorFieldOverloads.h:244-249, which has no transform counterpart).
+Complex-valued fields carry the canonical components. The reference's
+real-valued branch (a real vector field in the real basis u_{-1}, u_0, u_{+1})
+is ``RealVectorField``, with the two conversions of
+VectorFieldRealToComplex.h:66-72 (``complexify``) and
+VectorFieldComplexToReal.h:62-69 (``realify``); its components have no
+transform of their own (transform the complexified field).
 
 The three components live in one CUDA tensor [3][count][nTheta * nPhi];
 pointwise operations run the fused expression kernel once per component
@@ -203,3 +206,99 @@ class VectorExpansion:
     @classmethod
     def of(cls, u: VectorField, precision: str = "fp64", lmax: int | None = None):
         return cls(u.grid, u.count, lmax=lmax).from_field(u, precision)
+
+
+class RealVectorField:
+    """VectorField<Grid, RealValued> on the GPU: three real components in the
+    reference's real basis, one CUDA tensor [3][count][nTheta * nPhi]
+    (alpha = -1, 0, +1)."""
+
+    def __init__(self, grid, count: int = 1, data=None):
+        import torch
+
+        self.grid, self.count = grid, int(count)
+        fs = grid.FieldSize()
+        if data is None:
+            self._data = torch.zeros((3, count, fs), dtype=torch.float64, device="cuda")
+        else:
+            if data.dtype != torch.float64 or data.numel() != 3 * count * fs or not data.is_cuda:
+                raise BadArgument(1, "data must be a float64 CUDA tensor of 3 x count fields")
+            self._data = data.contiguous().view(3, count, fs)
+        self._comp = [Field(grid, 0, True, count, self._data[a + 1]) for a in CANONICAL_INDICES]
+
+    @staticmethod
+    def CanonicalIndices():
+        return range(-1, 2)
+
+    def __getitem__(self, alpha: int) -> Field:
+        return self._comp[_check_alpha(alpha)]
+
+    def Data(self):
+        return self._data
+
+    def _same(self, o):
+        if not isinstance(o, RealVectorField) or o.grid is not self.grid or o.count != self.count:
+            raise BadArgument(1, "real vector fields differ in grid or batch size")
+
+    def _map(self, fn) -> "RealVectorField":
+        out = RealVectorField(self.grid, self.count)
+        for a in CANONICAL_INDICES:
+            out[a].assign(fn(a), upper_index=0)
+        return out
+
+    def assign(self, o: "RealVectorField") -> "RealVectorField":
+        self._same(o)
+        for a in CANONICAL_INDICES:
+            self[a].assign(o[a], upper_index=0)
+        return self
+
+    def __neg__(self):
+        return self._map(lambda a: -self[a])
+
+    def __add__(self, o):
+        self._same(o)
+        return self._map(lambda a: self[a] + o[a])
+
+    def __sub__(self, o):
+        self._same(o)
+        return self._map(lambda a: self[a] - o[a])
+
+    def __mul__(self, s):
+        """By a real scalar or by a real scalar field."""
+        if isinstance(s, complex) or (isinstance(s, F.Expr) and not s.is_real):
+            raise BadArgument(1, "real vector fields scale by real scalars or real fields")
+        return self._map(lambda a: self[a] * s)
+
+    __rmul__ = __mul__
+
+
+def complexify(u: RealVectorField) -> VectorField:
+    """VectorFieldRealToComplex (VectorFieldRealToComplex.h:66-72): canonical
+    components c_0 = u_0, c_alpha = alpha u_{+1} + i u_{-1} (alpha = +-1), one
+    fused kernel per component."""
+    out = VectorField(u.grid, u.count)
+    out[0].assign(u[0] + 0j, upper_index=0)
+    for a in (-1, 1):
+        # (real field + 0j) is the field as a complex value; the operations
+        # then stay within one value type, as the reference requires.
+        out[a].assign(a * (u[1] + 0j) + 1j * (u[-1] + 0j), upper_index=a)
+    return out
+
+
+def realify(v: VectorField) -> RealVectorField:
+    """VectorFieldComplexToReal (VectorFieldComplexToReal.h:62-69): with
+    w_alpha = (v_alpha + (-1)^alpha conj(v_{-alpha})) / 2, the real components
+    are Im w_alpha for alpha < 0 and Re w_alpha otherwise."""
+    out = RealVectorField(v.grid, v.count)
+    for a in CANONICAL_INDICES:
+        sgn = -1.0 if a % 2 else 1.0
+        w = 0.5 * (v[a] + sgn * F.conj(v[-a], upper_index=a))
+        out[a].assign(F.imag(w) if a < 0 else F.real(w), upper_index=0)
+    return out
+
+
+def RealInnerProduct(u: RealVectorField, v: RealVectorField) -> Field:
+    """sum_alpha u_alpha v_alpha of two real vector fields (the reference's
+    real-valued InnerProduct, VectorFieldOverloads.h:244-249), one fused kernel."""
+    u._same(v)
+    return (u[-1] * v[-1] + u[0] * v[0] + u[1] * v[1]).evaluate(upper_index=0)

@@ -270,6 +270,10 @@ gsht_status gsht_batch_info(const gsht_batch* batch, int* groups, int* grids,
                             long* graph_nodes /* [3] or NULL */);
 gsht_status gsht_batch_group(const gsht_batch* batch, int index, int* lmax, int* n,
                              int* is_real, int* count, int* ntile);
+/* Number of streams the plan's graphs spread the groups over (each group
+ * has its own workspace; with `autotune` the count is the fastest of 1, 2,
+ * 4, 8, 16 for the round trip). Groups are listed largest first. */
+gsht_status gsht_batch_schedule(const gsht_batch* batch, int* streams);
 gsht_status gsht_batch_destroy(gsht_batch* batch);
 
 /* Stage timing. No counterpart in the reference (which has no tracing):

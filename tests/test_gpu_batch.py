@@ -51,6 +51,13 @@ def test_batch_matches_single_field_calls(gsht, precision, tol):
     assert min(nodes) > 0
     for lm, n, re, cnt, tile in batch.groups():
         assert tile in (32, 64, 128)
+    assert batch.streams() in (1, 2, 4, 8, 16)
+    # planning (warm-up, tile-width and schedule tuning) leaves the callers'
+    # buffers as they were
+    torch.cuda.synchronize()
+    for lmax, n, is_real, cin, grid, cout, init in fields:
+        assert not torch.any(grid)
+        assert np.array_equal(cout.cpu().numpy(), init)
     batch.round_trip()
     torch.cuda.synchronize()
     forms = () if precision == "fp64" else (precision,)

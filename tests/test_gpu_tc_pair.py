@@ -4,7 +4,9 @@ the two CTAs of a cluster, B = a 128-wide table tile split likewise, four
 TMEM accumulators per CTA. Checked against the FP64 path at the BF16x3
 tier (<= 1e-6 inverse, 2e-6 forward) and against the one-CTA form of the
 same products (GSHT_BF16X3_PAIR=1 forces the pair form in both directions,
-=0 the one-CTA form) on the same inputs: the results are bit-identical. Shapes: 64 complex
+=0 the one-CTA form) on the same inputs: the results are bit-identical.
+Both inverse K steps (GSHT_BF16X3_INV_K = 32 and 64 degrees per stage) are
+covered. Shapes: 64 complex
 fields (exactly one pair tile of field rows), 65 (a second, mostly empty
 field tile), 128 real fields; odd and even colatitude counts; upper indices
 0 and -2; lmax < L."""
@@ -58,18 +60,23 @@ def test_pair_form_matches_fp64_and_the_one_cta_form(gsht, L, lmax, n, is_real, 
     c = np.stack([oracle.random_coefficients(rng, L, lmax, n, is_real, 1.5) for _ in range(B)])
     with gsht.GaussLegendreGrid(L, 2, forms=("bf16x3",)) as g:
         f64, b64 = _round(g, L, lmax, n, is_real, c, "fp64")
+        res = {}
         try:
-            os.environ["GSHT_BF16X3_PAIR"] = "1"
-            fp, bp = _round(g, L, lmax, n, is_real, c, "bf16x3")
-            os.environ["GSHT_BF16X3_PAIR"] = "0"
-            f1, b1 = _round(g, L, lmax, n, is_real, c, "bf16x3")
+            for k in ("32", "64"):
+                os.environ["GSHT_BF16X3_INV_K"] = k
+                for form in ("1", "0"):
+                    os.environ["GSHT_BF16X3_PAIR"] = form
+                    res[k, form] = _round(g, L, lmax, n, is_real, c, "bf16x3")
         finally:
-            del os.environ["GSHT_BF16X3_PAIR"]
-    # the forward's input is each form's own inverse, so compare the forward
-    # through the round trip and the inverse directly
-    assert relerr(fp, f64) < TOL, "inverse vs FP64"
-    assert relerr(bp, b64) < 3 * TOL, "round trip vs FP64"
-    assert np.array_equal(fp, f1), "inverse vs one-CTA form"
-    assert np.array_equal(bp, b1), "round trip vs one-CTA form"
-    print(f"L={L} B={B} real={is_real}: pair vs one-CTA inverse {relerr(fp, f1):.2e}, "
-          f"vs FP64 {relerr(fp, f64):.2e} (one-CTA {relerr(f1, f64):.2e})")
+            os.environ.pop("GSHT_BF16X3_PAIR", None)
+            os.environ.pop("GSHT_BF16X3_INV_K", None)
+    for k in ("32", "64"):
+        (fp, bp), (f1, b1) = res[k, "1"], res[k, "0"]
+        # the forward's input is each form's own inverse, so the forward is
+        # checked through the round trip and the inverse directly
+        assert relerr(fp, f64) < TOL, ("inverse vs FP64", k)
+        assert relerr(bp, b64) < 3 * TOL, ("round trip vs FP64", k)
+        assert np.array_equal(fp, f1), ("inverse: pair vs one-CTA form", k)
+        assert np.array_equal(bp, b1), ("round trip: pair vs one-CTA form", k)
+    print(f"L={L} B={B} real={is_real}: inverse vs FP64 {relerr(res['32', '1'][0], f64):.2e} "
+          f"(K 32), {relerr(res['64', '1'][0], f64):.2e} (K 64)")
