@@ -295,11 +295,12 @@ gsht_status legendre_forward_rec(const gsht_grid* g, const Table* t, int lmax, i
                                  int count, double* spec, void* partial, double* coef,
                                  cudaStream_t s);
 
-// Adds order-major result rows R[m][q][l - l0] (pitch `pitch`) into the
-// packed coefficients of `count` fields (forward accumulate semantics).
+// Adds order-major result rows R[m][q][l - l0] (pitch `pitch`; complex
+// FP64, or FP32 with rows32) into the packed coefficients of `count` fields
+// (forward accumulate semantics).
 gsht_status accumulate_forward(int L, int lmax, int n, int na, int count, int Q, int is_real,
                                long coefSize, int pitch, const double* rows, double* coef,
-                               cudaStream_t s);
+                               cudaStream_t s, bool rows32 = false);
 
 // Cached operand layout (legendre_fp64.cu); the caller holds g->mu.
 const OperandLayout* operand_layout(const gsht_grid* g, int lmax, int na,

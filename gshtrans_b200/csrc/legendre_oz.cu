@@ -23,6 +23,7 @@
 // along the contraction and is folded into the field-side rows before they
 // are sliced.
 #include <cstdio>
+#include <type_traits>
 
 #include "gsht_internal.cuh"
 #include "tc_common.cuh"
@@ -155,7 +156,11 @@ __global__ void __launch_bounds__(kThreads, 1)
       int it = 0, tc = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < numTiles && ok; t += gridDim.x, tc++) {
-        const int nk = tiles[t].w;
+        const int4 tl = tiles[t];
+        const int nk = tl.w;
+        // K steps of 32 past the last degree (inverse) or colatitude
+        // (forward) multiply zero padding and are not issued.
+        const int kLim = kDir == 0 ? p.lmax - (tl.x > p.na ? tl.x : p.na) + 1 : p.nTheta;
         if (tc > 0 && !mbar_wait(accEmpty, (tc - 1) & 1, p.err, 14)) break;
         tc_fence_after();
         for (int kc = 0; kc < nk; kc++, it++) {
@@ -172,6 +177,10 @@ __global__ void __launch_bounds__(kThreads, 1)
           // diagonal accumulators back to back in TMEM, so one MMA of N =
           // 64 x (number of slices) covers up to four of them. 10 MMAs per
           // K step instead of 28: A is read from shared memory 10 times.
+          // The last K block may end inside the padding: its K steps past
+          // kLim are skipped (a separate copy of the loop, so that the full
+          // blocks keep the branch-free one).
+          auto issue = [&](auto whole) {
 #pragma unroll
           for (int i = 0; i < kS; i++) {
 #pragma unroll
@@ -183,6 +192,8 @@ __global__ void __launch_bounds__(kThreads, 1)
               const uint32_t d = tmem + (uint32_t)((i + j0) * kN);
 #pragma unroll
               for (int k32 = 0; k32 < kBK / 32; k32++) {
+                if constexpr (!decltype(whole)::value)
+                  if (k32 > 0 && kc * kBK + k32 * 32 >= kLim) break;
                 const uint64_t ad = kDir == 0 ? sdesc_sw128(aBase + k32 * 4096, 8192, 1024)
                                               : sdesc_sw64(aBase + k32 * 32, 16, 512);
                 const uint64_t bd = sdesc_sw64(bBase + k32 * 32, 16, 512);
@@ -190,6 +201,9 @@ __global__ void __launch_bounds__(kThreads, 1)
               }
             }
           }
+          };
+          if ((kc + 1) * kBK <= kLim) issue(std::true_type{});
+          else issue(std::false_type{});
           mma_commit(&empty[s]);
         }
         mma_commit(accFull);

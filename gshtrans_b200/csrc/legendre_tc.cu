@@ -159,7 +159,11 @@ __global__ void __launch_bounds__(kThreads, 1)
       int it = 0, tc = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < numTiles && ok; t += gridDim.x, tc++) {
-        const int nk = tiles[t].w;
+        const int4 tl = tiles[t];
+        const int nk = tl.w;
+        // K steps of 16 past the last degree (inverse) or colatitude
+        // (forward) multiply zero padding and are not issued.
+        const int kLim = kDir == 0 ? p.lmax - (tl.x > p.na ? tl.x : p.na) + 1 : p.nTheta;
         if (tc > 0 && !mbar_wait(accEmptyA, (tc - 1) & 1, p.err, 4)) break;
         tc_fence_after();
         bool haveB = tc == 0;
@@ -184,6 +188,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             haveB = true;
           }
           const uint32_t st = smem_u32(smem + s * kStageBytes);
+          // The last K block may end inside the padding: its K steps past
+          // kLim are skipped (a separate copy of the loop, so that the
+          // full blocks keep the branch-free one).
+          auto issue = [&](auto whole) {
 #pragma unroll
           for (int pr = 0; pr < kNP; pr++) {
             const uint32_t aBase = st + prodA(pr) * kTileA;
@@ -191,6 +199,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t d = tmem + (uint32_t)((pr == 0 ? big : 0) * kN);
 #pragma unroll
             for (int k16 = 0; k16 < kBK / 16; k16++) {
+              if constexpr (!decltype(whole)::value)
+                if (k16 > 0 && kc * kBK + k16 * 16 >= kLim) break;
               uint64_t ad, bd;
               if constexpr (kDir == 0) {
                 ad = sdesc_sw128(aBase + k16 * 2048, kTileA / 2, 1024);
@@ -205,6 +215,9 @@ __global__ void __launch_bounds__(kThreads, 1)
               mma_f16(d, ad, bd, id, first ? 0u : 1u);
             }
           }
+          };
+          if ((kc + 1) * kBK <= kLim) issue(std::true_type{});
+          else issue(std::false_type{});
           mma_commit(&empty[s]);
         }
         // Keep accEmptyB in step with the tiles even if this one used no
@@ -277,6 +290,14 @@ __global__ void __launch_bounds__(kThreads, 1)
           p.out32[((size_t)m * p.Q + q) * p.thetaPad + col] =
               make_float2((float)acc[2 * i], (float)acc[2 * i + 1]);
         }
+      } else if (kDir == 1 && p.out32) {
+#pragma unroll
+        for (int i = 0; i < kCols / 2; i++) {
+          const int q = q0 + i;
+          if (q < p.Q)
+            p.out32[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
+                make_float2((float)acc[2 * i], (float)acc[2 * i + 1]);
+        }
       } else {
 #pragma unroll
         for (int i = 0; i < kCols / 2; i++) {
@@ -315,10 +336,22 @@ __global__ void __launch_bounds__(kThreads, 1)
 // ---------------------------------------------------------------------------
 constexpr int kPairM = 256;  // field rows per pair tile
 constexpr int kPairN = 128;  // table columns per pair tile
+// Output staging per epilogue warp: 16 complex rows x 8 FP32 or 4 FP64
+// columns, XOR-swizzled so that both the per-lane writes and the
+// row-segment reads are free of bank conflicts.
+constexpr int kPairStage = 1024;
 
 template <int kStages, int kBK>
 constexpr size_t tc2_smem_bytes() {
-  return (size_t)kStages * 3 * (kBM + kPairN / 2) * kBK * 2 + 1024 + 256;
+  return (size_t)kStages * 3 * (kBM + kPairN / 2) * kBK * 2 + 1024 + 256 +
+         kEpiWarps * kPairStage;
+}
+
+// Table columns one pair tile computes: kPairN, or for the last tile of an
+// order its valid columns rounded up to 32 (16 per CTA), so that the MMAs
+// of a short tail tile run at N = 32..96 instead of 128.
+__device__ __forceinline__ int pair_tile_n(int valid) {
+  return valid >= kPairN ? kPairN : (valid + 31) / 32 * 32;
 }
 
 template <int kDir, int kStages, int kBK>
@@ -372,6 +405,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int4 tl = tiles[t];  // (m, table tile, field tile, K blocks)
         const long long tRow = p.rowOff[tl.x];
         const int fRow = tl.x * p.R + tl.z * kPairM + (int)rank * kBM;
+        // Rank 1 holds table columns [nT/2, nT) of a tile nT wide.
+        const int limit = kDir == 0 ? p.nTheta : p.lmax - (tl.x > p.na ? tl.x : p.na) + 1;
+        const int half = (int)rank * (pair_tile_n(limit - tl.y * kPairN) / 2);
         for (int kc = 0; kc < tl.w; kc++, it++) {
           const int s = it % kStages;
           if (it >= kStages && !mbar_wait(&empty[s], ((it / kStages) - 1) & 1, p.err, 11)) {
@@ -388,12 +424,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             unsigned char* dst = st + 3 * kTileF + a * kTileT;
             if (kDir == 0) {
               // MN-major: 64 colatitudes (this CTA's half) x kBK degree rows.
-              tma_load_3d_pair(dst, &mapT, fbar, tl.y * kPairN + (int)rank * (kPairN / 2),
-                               (int)(tRow + kc * kBK), a);
+              tma_load_3d_pair(dst, &mapT, fbar, tl.y * kPairN + half, (int)(tRow + kc * kBK), a);
             } else {
               // K-major: 64 degree rows (this CTA's half) x kBK colatitudes.
-              tma_load_3d_pair(dst, &mapT, fbar, kc * kBK,
-                               (int)(tRow + tl.y * kPairN + (int)rank * (kPairN / 2)), a);
+              tma_load_3d_pair(dst, &mapT, fbar, kc * kBK, (int)(tRow + tl.y * kPairN + half), a);
             }
           }
         }
@@ -407,11 +441,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp == 1) {
     if (rank == 0 && lane == 0) {
-      constexpr uint32_t id = idesc(1, 1, 0, kDir == 0 ? 1 : 0, kPairN, kPairM);
       int it = 0, tc = 0;
       bool ok = true;
       for (int t = pair; t < numTiles && ok; t += npairs, tc++) {
-        const int nk = tiles[t].w;
+        const int4 tl = tiles[t];
+        const int nk = tl.w;
+        const int kLim = kDir == 0 ? p.lmax - (tl.x > p.na ? tl.x : p.na) + 1 : p.nTheta;
+        const int limit = kDir == 0 ? p.nTheta : p.lmax - (tl.x > p.na ? tl.x : p.na) + 1;
+        const uint32_t id =
+            idesc(1, 1, 0, kDir == 0 ? 1 : 0, pair_tile_n(limit - tl.y * kPairN), kPairM);
         if (tc > 0 && !mbar_wait(accEmptyA, (tc - 1) & 1, p.err, 14)) break;
         tc_fence_after();
         bool haveB = tc == 0;
@@ -434,6 +472,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             haveB = true;
           }
           const uint32_t st = smem_u32(smem + s * kStageBytes);
+          auto issue = [&](auto whole) {
 #pragma unroll
           for (int pr = 0; pr < kNprodTc; pr++) {
             // A = field rows (split prodB), B = table (split prodA).
@@ -442,6 +481,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t d = tmem + (uint32_t)((pr == 0 ? big : 0) * kPairN);
 #pragma unroll
             for (int k16 = 0; k16 < kBK / 16; k16++) {
+              if constexpr (!decltype(whole)::value)
+                if (k16 > 0 && kc * kBK + k16 * 16 >= kLim) break;
               uint64_t ad, bd;
               if constexpr (kDir == 0) {
                 ad = kBK == 32 ? sdesc_sw64(aBase + k16 * 32, 16, 512)
@@ -456,6 +497,9 @@ __global__ void __launch_bounds__(kThreads, 1)
               mma_f16_pair(d, ad, bd, id, first ? 0u : 1u);
             }
           }
+          };
+          if ((kc + 1) * kBK <= kLim) issue(std::true_type{});
+          else issue(std::false_type{});
           mma_commit_pair(&empty[s], 0x3);
         }
         if (ok && !haveB && !mbar_wait(accEmptyB, (tc - 1) & 1, p.err, 15)) ok = false;
@@ -468,12 +512,21 @@ __global__ void __launch_bounds__(kThreads, 1)
     // group (warp - 2) / 4 (64 table columns each).
     const int quarter = warp & 3;
     const int group = (warp - 2) >> 2;
-    const int row = quarter * 32 + lane;
     const uint32_t emptyA0 = cluster_addr(accEmptyA, 0), emptyB0 = cluster_addr(accEmptyB, 0);
+    unsigned char* stg = smem + kStages * kStageBytes + 256 + (warp - 2) * kPairStage;
+    // Lane = field row 2 ql + part of the warp's 32 (16 complex rows).
+    const int ql = lane >> 1, part = lane & 1;
+    const bool fp32 = kDir == 1 || p.out32 != nullptr;
     int tc = 0;
     for (int t = pair; t < numTiles; t += npairs, tc++) {
       const int4 tl = tiles[t];
       const int m = tl.x, nk = tl.w;
+      const int l0 = m > p.na ? m : p.na;
+      const int limit = kDir == 0 ? p.nTheta : p.lmax - l0 + 1;
+      const int colW = tl.y * kPairN + group * kCols;  // first table column of this warp
+      // Columns of a narrowed tail tile past its width hold stale values:
+      // a warp whose 64 columns all lie there drains nothing.
+      const bool live = group * kCols < pair_tile_n(limit - tl.y * kPairN);
       if (!mbar_wait(accFull, tc & 1, p.err, 13)) break;
       tc_fence_after();
       const int nbig = nk < kBigAcc ? nk : kBigAcc;
@@ -495,60 +548,75 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
         }
       };
-      drain(0);
-      drain(1);
+      if (live) {
+        drain(0);
+        drain(1);
+      }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cluster(emptyA0);
+      if (live) {
 #pragma unroll
-      for (int a = 2; a <= kBigAcc; a++)
-        if (a <= nbig) drain(a);
+        for (int a = 2; a <= kBigAcc; a++)
+          if (a <= nbig) drain(a);
+      }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cluster(emptyB0);
-      // Field row r of this lane, and its partner (the other part of the
-      // same complex row q) in the neighbouring lane.
-      const int r = tl.z * kPairM + (int)rank * kBM + row;
-      const int q = r >> 1, part = r & 1;
-      const int l0 = m > p.na ? m : p.na;
-      const int keff = p.lmax - l0 + 1;
-      const int c0 = tl.y * kPairN + group * kCols;  // first table column of this warp
-      const int limit = kDir == 0 ? p.nTheta : keff;
-      // Even lanes write columns [0, kCols/2), odd lanes [kCols/2, kCols):
-      // at step j the even lane needs the partner's column j, the odd lane
-      // the partner's column kCols/2 + j.
-      constexpr int kHalf = kCols / 2;
-      const bool rowOk = q < p.Q;
-      const int cBase = c0 + (part ? kHalf : 0);
+      if (!live) continue;
+      // First complex row of this warp's 16.
+      const int qw = (tl.z * kPairM + (int)rank * kBM + quarter * 32) >> 1;
+      // Rows leave in chunks through the warp's staging buffer: each lane
+      // writes its row's values, then each store instruction writes 64
+      // contiguous bytes of 4 (FP32) or 2 (FP64) complex rows.
+      if (fp32) {
+        float* sf = reinterpret_cast<float*>(stg);
+        const int swW = 2 * ((ql >> 1) & 7);
+        const int c = lane & 7;
 #pragma unroll
-      for (int j = 0; j < kHalf; j += 2) {
-        double2 v[2];
+        for (int cc = 0; cc < kCols; cc += 8) {
+          if (colW + cc < limit) {
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
-          const double send = part ? acc[j + u] : acc[kHalf + j + u];
-          const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
-          v[u] = part ? make_double2(recv, acc[kHalf + j + u]) : make_double2(acc[j + u], recv);
-        }
-        if (!rowOk) continue;
-        const int col = cBase + j;
-        if (kDir == 0 && p.out32) {
-          float2* rowp = p.out32 + ((size_t)m * p.Q + q) * p.thetaPad;
-          if (q < p.count && col + 1 < limit) {
-            *reinterpret_cast<float4*>(rowp + col) =
-                make_float4((float)v[0].x, (float)v[0].y, (float)v[1].x, (float)v[1].y);
-          } else {
+            for (int u = 0; u < 8; u++) sf[ql * 16 + ((2 * u + part) ^ swW)] = (float)acc[cc + u];
+            __syncwarp();
+            const int col = colW + cc + c;
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
-              if (col + u >= limit) continue;
-              const int cc = q >= p.count ? p.nTheta - 1 - (col + u) : col + u;
-              rowp[cc] = make_float2((float)v[u].x, (float)v[u].y);
+            for (int i = 0; i < 4; i++) {
+              const int qr = (lane >> 3) + 4 * i;
+              const float2 v =
+                  *reinterpret_cast<const float2*>(sf + qr * 16 + ((2 * c) ^ (2 * ((qr >> 1) & 7))));
+              const int q = qw + qr;
+              if (col < limit && q < p.Q) {
+                // Inverse: table column col holds +m at colatitude col and
+                // -m at its mirror nTheta-1-col.
+                const int cj = (kDir == 0 && q >= p.count) ? p.nTheta - 1 - col : col;
+                p.out32[((size_t)m * p.Q + q) * p.thetaPad + cj] = v;
+              }
             }
+            __syncwarp();
           }
-        } else {
-          double2* rowp = p.out + ((size_t)m * p.Q + q) * p.thetaPad;
+        }
+      } else {
+        double* sd = reinterpret_cast<double*>(stg);
+        const int swW = 2 * ((ql >> 1) & 3);
+        const int c = lane & 3;
 #pragma unroll
-          for (int u = 0; u < 2; u++)
-            if (col + u < limit) rowp[col + u] = v[u];
+        for (int cc = 0; cc < kCols; cc += 4) {
+          if (colW + cc < limit) {
+#pragma unroll
+            for (int u = 0; u < 4; u++) sd[ql * 8 + ((2 * u + part) ^ swW)] = acc[cc + u];
+            __syncwarp();
+            const int col = colW + cc + c;
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+              const int qr = (lane >> 2) + 8 * i;
+              const double2 v =
+                  *reinterpret_cast<const double2*>(sd + qr * 8 + ((2 * c) ^ (2 * ((qr >> 1) & 3))));
+              const int q = qw + qr;
+              if (col < limit && q < p.Q) p.out[((size_t)m * p.Q + q) * p.thetaPad + col] = v;
+            }
+            __syncwarp();
+          }
         }
       }
     }
@@ -564,12 +632,26 @@ __global__ void __launch_bounds__(kThreads, 1)
 // ---------------------------------------------------------------------------
 // Field-side operands: BF16 hi/mid/lo planes of the real rows r = 2q + part.
 // ---------------------------------------------------------------------------
+// FP64 value: hi rounds x itself; the residual x - hi (at most 2^-8 |x|) is
+// rounded once to FP32 (a relative error of 2^-24 of the residual, below
+// 2^-32 |x|) and split on the FP32 pipe: four FP64-pipe operations per
+// value instead of seven.
 __device__ __forceinline__ void split3(double x, __nv_bfloat16& h, __nv_bfloat16& md,
                                        __nv_bfloat16& lo) {
   h = __double2bfloat16(x);
-  const double r1 = x - (double)__bfloat162float(h);
-  md = __double2bfloat16(r1);
-  lo = __double2bfloat16(r1 - (double)__bfloat162float(md));
+  const float r1 = (float)(x - (double)__bfloat162float(h));
+  md = __float2bfloat16_rn(r1);
+  lo = __float2bfloat16_rn(r1 - __bfloat162float(md));
+}
+
+// FP32 value: every residual is exact in FP32, so this equals the FP64
+// split of the same value, on the FP32 pipe.
+__device__ __forceinline__ void split3(float x, __nv_bfloat16& h, __nv_bfloat16& md,
+                                       __nv_bfloat16& lo) {
+  h = __float2bfloat16_rn(x);
+  const float r1 = x - __bfloat162float(h);
+  md = __float2bfloat16_rn(r1);
+  lo = __float2bfloat16_rn(r1 - __bfloat162float(md));
 }
 
 // Inverse: packed coefficients -> B[split][m*R + 2q + part][k], k = l - l0(m)
@@ -577,11 +659,19 @@ __device__ __forceinline__ void split3(double x, __nv_bfloat16& h, __nv_bfloat16
 // field row q: the packed layout is contiguous along orders for a fixed
 // degree, so the tile is read order-major (coalesced), transposed in shared
 // memory and written degree-major (each order's operand row segment).
+// blockIdx.x walks the triangle of (degree tile a, order tile b <= a) pairs
+// row by row (row b holds nA - b tiles), so no block is launched for the
+// empty upper half.
 __global__ void __launch_bounds__(256) k_prep_inverse_bf16(
     int lmax, int n, int na, int count, int Q, int R, int isReal, long coefSize, int pitch,
-    size_t plane, const double2* __restrict__ coef, __nv_bfloat16* __restrict__ op) {
+    size_t plane, int nA, const double2* __restrict__ coef, __nv_bfloat16* __restrict__ op) {
   __shared__ double2 tile[32][33];
-  const int lt = blockIdx.x * 32, mt = blockIdx.y * 32, q = blockIdx.z;
+  int i0 = blockIdx.x, b = 0;
+  while (i0 >= nA - b) {
+    i0 -= nA - b;
+    b++;
+  }
+  const int lt = (b + i0) * 32, mt = b * 32, q = blockIdx.z;
   const int sgn = q / count, f = q - sgn * count;
   if (lt + 31 < (mt > na ? mt : na) || mt > lmax) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -625,10 +715,12 @@ __global__ void __launch_bounds__(256) k_prep_inverse_bf16(
 // c_{L,L} = 0 rule of complex fields (GaussLegendreGrid.h:209-215). One block
 // per 32 degrees x 32 orders of one row q: rows are read degree-contiguous,
 // transposed in shared memory, and the packed layout (order-contiguous for a
-// fixed degree) is read-modify-written coalesced.
+// fixed degree) is read-modify-written coalesced. RowT: double2, or float2
+// for the rows of the BF16x3 form.
+template <typename RowT>
 __global__ void __launch_bounds__(256) k_accumulate_forward(
     int L, int lmax, int n, int na, int count, int Q, int isReal, long coefSize, int pitch,
-    const double2* __restrict__ rows, double2* __restrict__ coef) {
+    const RowT* __restrict__ rows, double2* __restrict__ coef) {
   __shared__ double2 tile[32][33];
   const int lt = blockIdx.x * 32, mt = blockIdx.y * 32, q = blockIdx.z;
   if (mt > lt + 31 || mt > lmax) return;
@@ -639,8 +731,10 @@ __global__ void __launch_bounds__(256) k_accumulate_forward(
     const int m = mt + i, l = lt + lane;
     const int l0 = m > na ? m : na;
     double2 v = make_double2(0.0, 0.0);
-    if (m <= lmax && l <= lmax && l >= l0)
-      v = rows[((size_t)m * Q + q) * pitch + (l - l0)];
+    if (m <= lmax && l <= lmax && l >= l0) {
+      const RowT x = rows[((size_t)m * Q + q) * pitch + (l - l0)];
+      v = make_double2(x.x, x.y);
+    }
     tile[i][lane] = v;
   }
   __syncthreads();
@@ -675,22 +769,21 @@ __global__ void k_prep_forward_bf16(int lmax, int Q, int R, int count, int nThet
   const int j = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   if (j >= thetaPad) return;
   const size_t row = ((size_t)m * Q + q) * thetaPad;
-  double2 v[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+  // double2 for FP64 spectra, float2 (split on the FP32 pipe) for FP32 ones.
+  using V = typename std::conditional<std::is_same<SpecT, double2>::value, double2, float2>::type;
+  V v[2] = {};
   if constexpr (std::is_same<SpecT, double2>::value) {
     v[0] = spec[row + j];
     v[1] = spec[row + j + 1];
   } else if (q < count) {
     const float4 f = *reinterpret_cast<const float4*>(spec + row + j);
-    v[0] = make_double2(f.x, f.y);
-    v[1] = make_double2(f.z, f.w);
+    v[0] = make_float2(f.x, f.y);
+    v[1] = make_float2(f.z, f.w);
   } else {
 #pragma unroll
     for (int t = 0; t < 2; t++) {
       const int col = nTheta - 1 - (j + t);
-      if (col >= 0) {
-        const float2 f = spec[row + col];
-        v[t] = make_double2(f.x, f.y);
-      }
+      if (col >= 0) v[t] = spec[row + col];
     }
   }
   const size_t r0 = ((size_t)m * R + 2 * q) * thetaPad + j;
@@ -762,10 +855,11 @@ gsht_status launch_bf16(const gsht_grid* g, int ntile, const TcArgs& a, const CU
 
 // K step of the inverse kernels: 32 or 64 degrees per stage
 // (GSHT_BF16X3_INV_K=32 / 64 for comparisons; default kInverseBK). Measured
-// at lmax 1024, 64 fields: 64 runs the inverse in 1.70 against 1.82 ms but
-// forward+inverse round trip then differs from the input by 9.3e-7 against
-// 8.7e-7 (relative), so 32 keeps the wider margin under 1e-6.
-constexpr int kInverseBK = 32;
+// at lmax 1024, 64 fields, after the other forms in one run: 64 runs the
+// inverse in 1.78 against 1.97 ms, with an error against the FP64 path of
+// 8.1e-7 against 7.4e-7 (relative; the hi.hi accumulators split the degrees
+// at other points).
+constexpr int kInverseBK = 64;
 int inverse_bk() {
   const char* e = getenv("GSHT_BF16X3_INV_K");
   if (e && atoi(e) == 64) return 64;
@@ -880,9 +974,10 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
     StageTimer tm(GSHT_STAGE_PREP_INVERSE, s);
     // Degrees up to l0 + kp - 1 <= lmax + kBKInv - 1: the zero padding of
     // every order's row up to its K-step multiple is written too.
-    dim3 pg((lmax + kBKInv + 31) / 32, (lmax + 32) / 32, Q);
+    const int nA = (lmax + kBKInv + 31) / 32, nB = (lmax + 32) / 32;
+    dim3 pg(nB * nA - nB * (nB - 1) / 2, 1, Q);
     k_prep_inverse_bf16<<<pg, 256, 0, s>>>(lmax, t->n, na, count, Q, R, is_real,
-                                           coef_size(lmax, t->n, is_real), pitch, plane,
+                                           coef_size(lmax, t->n, is_real), pitch, plane, nA,
                                            reinterpret_cast<const double2*>(coef), op);
     GSHT_LAUNCH_CHECK("k_prep_inverse_bf16");
   }
@@ -947,8 +1042,11 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
   a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count; a.Q = Q; a.R = R;
   a.nTheta = g->n_theta; a.thetaPad = tp; a.isReal = is_real;
   // The spectra are consumed (split into the BF16 planes) by now: their
-  // buffer holds the kernel's order-major result rows (keff <= thetaPad).
+  // buffer holds the kernel's order-major result rows (keff <= thetaPad),
+  // in FP32 (the form's accuracy is FP32-class; half the bytes of FP64 for
+  // the kernel to write and the accumulation to read).
   a.rowOff = t->d_row_off; a.out = reinterpret_cast<double2*>(spec);
+  a.out32 = reinterpret_cast<float2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   {
     StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
@@ -956,17 +1054,23 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
                   : launch_bf16<1, 64>(g, ntile, a, mapA, mapB, s);
   }
   if (st != GSHT_OK) return st;
-  return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, tp, spec, coef, s);
+  return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, tp, spec, coef, s,
+                            true);
 }
 
 gsht_status accumulate_forward(int L, int lmax, int n, int na, int count, int Q, int is_real,
                                long coefSize, int pitch, const double* rows, double* coef,
-                               cudaStream_t s) {
+                               cudaStream_t s, bool rows32) {
   StageTimer tm(GSHT_STAGE_ACCUMULATE_FORWARD, s);
   dim3 ag((lmax + 32) / 32, (lmax + 32) / 32, Q);
-  k_accumulate_forward<<<ag, 256, 0, s>>>(L, lmax, n, na, count, Q, is_real, coefSize, pitch,
-                                          reinterpret_cast<const double2*>(rows),
-                                          reinterpret_cast<double2*>(coef));
+  if (rows32)
+    k_accumulate_forward<float2><<<ag, 256, 0, s>>>(L, lmax, n, na, count, Q, is_real, coefSize,
+                                                    pitch, reinterpret_cast<const float2*>(rows),
+                                                    reinterpret_cast<double2*>(coef));
+  else
+    k_accumulate_forward<double2><<<ag, 256, 0, s>>>(L, lmax, n, na, count, Q, is_real, coefSize,
+                                                     pitch, reinterpret_cast<const double2*>(rows),
+                                                     reinterpret_cast<double2*>(coef));
   GSHT_LAUNCH_CHECK("k_accumulate_forward");
   return GSHT_OK;
 }
