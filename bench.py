@@ -54,6 +54,9 @@ def parse():
     p.add_argument("--lmax", type=int, default=L_MAX)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--trace", action="store_true",
+                   help="after timing, run one traced round trip per tensor-core form and "
+                        "add the per-role cycle split of its Legendre kernels to the mode line")
     p.add_argument("--no-secondary", action="store_true",
                    help="skip the batch / large / pipeline workloads the default run adds")
     p.add_argument("--workload", default="headline",
@@ -381,10 +384,25 @@ def measure_mode(gsht, grid, torch, dev, coef, field, back, precision, args, wor
         ms = reduce_max_ms(ms, dist, dev)
     stages = {STAGES[i]: {"ms_per_step": stage_ms[i] / args.steps,
                           "launches_per_step": stage_n[i] / args.steps} for i in range(ns)}
+    trace = None
+    if getattr(args, "trace", False) and precision != "fp64":
+        # Outside the timed region: one round trip through the traced kernel
+        # copies; fractions of each role's cycles (summed over CTAs).
+        with gsht.TensorCoreTrace() as tr:
+            step()
+            trace = {}
+            for d, name in ((0, "inverse"), (1, "forward")):
+                c = tr.read(precision, d)
+                trace[name] = {k: round(v, 4) for k, v in c.items() if "frac" in k}
+                trace[name]["ctas"] = int(c["ctas"])
+                trace[name]["mma_ctas"] = int(c["mma_ctas"])
+                if c["mma_ctas"]:
+                    trace[name]["mma_cycles_per_issuer"] = c["mma"] / c["mma_ctas"]
+        grid.device_status()
     return {"ms": ms, "launches": launches, "stages": stages, "clocks": clk.summary(),
             "round_trip_rel_err": rt_err,
             "legendre_ms": (stage_ms[1] + stage_ms[5]) / args.steps,
-            "legendre_launches": int(stage_n[1] + stage_n[5])}
+            "legendre_launches": int(stage_n[1] + stage_n[5]), "trace": trace}
 
 
 def legendre_roofline(precision, res, args, peaks):
@@ -506,6 +524,8 @@ def impl_ours(args):
                 "stages": r["stages"],
                 "roofline": legendre_roofline(m, r, args, peaks),
             }
+            if r.get("trace"):
+                mode_lines[m]["trace"] = r["trace"]
         if "fp64" in modes:
             for m in modes:
                 mode_lines[m]["speedup_vs_fp64_gpu"] = mode_lines[m]["value"] / mode_lines["fp64"]["value"]

@@ -184,6 +184,46 @@ class StageProfile:
         return False
 
 
+library.gsht_tc_trace_enable.argtypes = [ctypes.c_int]
+library.gsht_tc_trace_read.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+TRACE_SLOTS = ("producer", "producer_wait_free_stage", "mma", "mma_wait_loaded_stage",
+               "mma_wait_epilogue", "epilogue", "epilogue_wait_accumulators", "ctas", "mma_ctas")
+
+
+class TensorCoreTrace:
+    """Per-role cycle trace of the tensor-core Legendre kernels launched
+    inside a ``with`` block (gsht_tc_trace_enable / gsht_tc_trace_read: the
+    traced kernel copies time every pipeline wait with clock64). ``read(form,
+    direction)`` returns the last traced launch's counters as a dict of
+    TRACE_SLOTS, plus per-role fractions: the share of the MMA issuer's time
+    spent waiting for loaded stages and for the epilogue, and the rest, during
+    which it issues MMAs. No counterpart in the reference."""
+
+    def __enter__(self):
+        _check(library.gsht_tc_trace_enable(1))
+        return self
+
+    def __exit__(self, *exc):
+        library.gsht_tc_trace_enable(0)
+        return False
+
+    @staticmethod
+    def read(form="bf16x3", direction=0):
+        out = (ctypes.c_double * len(TRACE_SLOTS))()
+        _check(library.gsht_tc_trace_read(_precision(form), int(direction),
+                                          ctypes.cast(out, ctypes.c_void_p), len(TRACE_SLOTS)))
+        c = {name: out[i] for i, name in enumerate(TRACE_SLOTS)}
+        if c["mma"] > 0:
+            c["mma_frac_wait_loaded_stage"] = c["mma_wait_loaded_stage"] / c["mma"]
+            c["mma_frac_wait_epilogue"] = c["mma_wait_epilogue"] / c["mma"]
+            c["mma_frac_issuing"] = 1.0 - c["mma_frac_wait_loaded_stage"] - c["mma_frac_wait_epilogue"]
+        if c["producer"] > 0:
+            c["producer_frac_wait_free_stage"] = c["producer_wait_free_stage"] / c["producer"]
+        if c["epilogue"] > 0:
+            c["epilogue_frac_wait_accumulators"] = c["epilogue_wait_accumulators"] / c["epilogue"]
+        return c
+
+
 def _check(status: int):
     if status != 0:
         msg = library.gsht_last_error().decode()

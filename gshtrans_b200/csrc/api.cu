@@ -518,8 +518,12 @@ gsht_status gsht_grid_create(int lmax, int nmax, int mrange, int nrange,
       tw[2 * t] = (double)cosl(a);
       tw[2 * t + 1] = (double)-sinl(a);
     }
+    std::vector<float> tw32(tw.begin(), tw.end());
     if (dev_malloc(&g->d_twiddle, sizeof(double) * tw.size()) != cudaSuccess ||
         cudaMemcpy(g->d_twiddle, tw.data(), sizeof(double) * tw.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess ||
+        dev_malloc(&g->d_twiddle32, sizeof(float) * tw32.size()) != cudaSuccess ||
+        cudaMemcpy(g->d_twiddle32, tw32.data(), sizeof(float) * tw32.size(),
                    cudaMemcpyHostToDevice) != cudaSuccess) {
       cudaGetLastError();
       st = fail(GSHT_ERR_OOM, "twiddle table allocation failed");
@@ -555,6 +559,7 @@ gsht_status gsht_grid_destroy(gsht_grid* g) {
   dev_free(g->d_theta);
   dev_free(g->d_weight);
   dev_free(g->d_twiddle);
+  dev_free(g->d_twiddle32);
   dev_free(g->d_err);
   dev_free(g->ws);
   if (g->ws_done) cudaEventDestroy(g->ws_done);

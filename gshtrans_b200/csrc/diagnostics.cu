@@ -14,8 +14,12 @@
 namespace gsht {
 namespace {
 
-// Error code a diagnostic wait raises (the pipelines use 1..5).
+// Error code a diagnostic wait raises (the pipelines use 1..16).
 constexpr int kDiagnosticWaitCode = 100;
+
+// Per-role cycle counters of traced tensor-core launches, [form][direction]
+// (form 0: BF16x3, 1: Ozaki), reset by each traced launch.
+__device__ unsigned long long g_trace_counters[2][2][tc::kTrSlots];
 
 __global__ void k_wait_never_completes(int* err) {
   __shared__ uint64_t bar;
@@ -30,9 +34,44 @@ __global__ void k_wait_never_completes(int* err) {
 }
 
 }  // namespace
+
+int g_tc_trace = 0;
+
+unsigned long long* trace_slots(int form, int dir, cudaStream_t s) {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_trace_counters) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  auto* slots = static_cast<unsigned long long*>(p) + (form * 2 + dir) * tc::kTrSlots;
+  if (cudaMemsetAsync(slots, 0, sizeof(unsigned long long) * tc::kTrSlots, s) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return slots;
+}
+
 }  // namespace gsht
 
 using namespace gsht;
+
+extern "C" gsht_status gsht_tc_trace_enable(int on) {
+  g_tc_trace = on != 0;
+  return GSHT_OK;
+}
+
+extern "C" gsht_status gsht_tc_trace_read(int form, int direction, double* out, int n) {
+  if (!out || n < GSHT_TRACE_SLOTS) return fail(GSHT_ERR_BAD_ARG, "need %d output slots", GSHT_TRACE_SLOTS);
+  if (form != GSHT_BF16X3 && form != GSHT_OZAKI && form != GSHT_OZAKI4)
+    return fail(GSHT_ERR_BAD_ARG, "form %d has no traced kernel", form);
+  if (direction != 0 && direction != 1) return fail(GSHT_ERR_BAD_ARG, "direction %d", direction);
+  static_assert(GSHT_TRACE_SLOTS == tc::kTrSlots, "trace slot count");
+  unsigned long long h[2][2][tc::kTrSlots];
+  GSHT_CUDA(cudaMemcpyFromSymbol(h, g_trace_counters, sizeof(h)));
+  const int f = form == GSHT_BF16X3 ? 0 : 1;
+  for (int i = 0; i < tc::kTrSlots; i++) out[i] = (double)h[f][direction][i];
+  return GSHT_OK;
+}
 
 extern "C" gsht_status gsht_check_bounded_wait(const gsht_grid* g, void* stream) {
   if (!g) return fail(GSHT_ERR_BAD_ARG, "grid is NULL");

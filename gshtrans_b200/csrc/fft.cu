@@ -83,6 +83,39 @@ __device__ __forceinline__ double2 twiddle(const double2* __restrict__ tw, int t
   return sign < 0 ? w : cconj(w);
 }
 
+// FP32 complex arithmetic of the FP32-spectrum path (the three-pass kernels
+// with float2 spectra run their butterflies in FP32: the BF16x3 form they
+// serve keeps ~1e-6, and FP32 halves the shared-memory bytes per point and
+// runs on the FP32 pipe).
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cmul_si(float2 a, int sign) {
+  return sign > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+__device__ __forceinline__ float2 twiddle(const float2* __restrict__ tw, int t, int stride,
+                                          int sign) {
+  float2 w = __ldg(tw + (size_t)t * stride);
+  return sign < 0 ? w : cconj(w);
+}
+// Complex value of compute type C from a stored one.
+template <typename C>
+__device__ __forceinline__ C to_c(double2 v);
+template <>
+__device__ __forceinline__ double2 to_c<double2>(double2 v) { return v; }
+template <>
+__device__ __forceinline__ float2 to_c<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+template <typename C>
+__device__ __forceinline__ C to_c(float2 v);
+template <>
+__device__ __forceinline__ double2 to_c<double2>(float2 v) { return make_double2(v.x, v.y); }
+template <>
+__device__ __forceinline__ float2 to_c<float2>(float2 v) { return v; }
+
 // Stockham FFT of length plan.n on buffer a (scratch b); returns the buffer
 // holding the result. All threads of the block must call it.
 __device__ double2* fft_block(double2* a, double2* b, const FftPlan& plan,
@@ -703,6 +736,68 @@ __global__ void __launch_bounds__(256) k_fft_forward_p2(
   }
 }
 
+// FP32 register DFTs of length 2, 4, 8, 16: the same operations as the FP64
+// specialisations above, in float2.
+template <int P>
+__device__ __forceinline__ void dft_reg(float2 (&c)[P], int sign) {
+  if constexpr (P == 2) {
+    const float2 a = cadd(c[0], c[1]), b = csub(c[0], c[1]);
+    c[0] = a;
+    c[1] = b;
+  } else if constexpr (P == 4) {
+    const float2 s02 = cadd(c[0], c[2]), d02 = csub(c[0], c[2]);
+    const float2 s13 = cadd(c[1], c[3]), d13 = cmul_si(csub(c[1], c[3]), sign);
+    c[0] = cadd(s02, s13);
+    c[1] = cadd(d02, d13);
+    c[2] = csub(s02, s13);
+    c[3] = csub(d02, d13);
+  } else if constexpr (P == 8) {
+    float2 e[4] = {c[0], c[2], c[4], c[6]};
+    float2 o[4] = {c[1], c[3], c[5], c[7]};
+    dft_reg<4>(e, sign);
+    dft_reg<4>(o, sign);
+    const float h = 0.70710678118654752440f;
+    const float sg = (float)sign;
+    o[1] = make_float2(h * (o[1].x - sg * o[1].y), h * (o[1].y + sg * o[1].x));
+    o[2] = cmul_si(o[2], sign);
+    o[3] = make_float2(h * (-o[3].x - sg * o[3].y), h * (-o[3].y + sg * o[3].x));
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      c[r] = cadd(e[r], o[r]);
+      c[r + 4] = csub(e[r], o[r]);
+    }
+  } else {
+    static_assert(P == 16, "FP32 register DFTs: 2, 4, 8, 16");
+    const float sg = (float)sign;
+    const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;
+    const float h = 0.70710678118654752440f;
+    float2 a[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) {
+      float2 t[4] = {c[n2], c[4 + n2], c[8 + n2], c[12 + n2]};
+      dft_reg<4>(t, sign);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; k1++) a[n2][k1] = t[k1];
+    }
+    a[1][1] = cmul(a[1][1], make_float2(c1, sg * s1));
+    a[1][2] = cmul(a[1][2], make_float2(h, sg * h));
+    a[1][3] = cmul(a[1][3], make_float2(s1, sg * c1));
+    a[2][1] = cmul(a[2][1], make_float2(h, sg * h));
+    a[2][2] = cmul_si(a[2][2], sign);
+    a[2][3] = cmul(a[2][3], make_float2(-h, sg * h));
+    a[3][1] = cmul(a[3][1], make_float2(s1, sg * c1));
+    a[3][2] = cmul(a[3][2], make_float2(-h, sg * h));
+    a[3][3] = cmul(a[3][3], make_float2(-c1, -sg * s1));
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) {
+      float2 t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+      dft_reg<4>(t, sign);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; k2++) c[k1 + 4 * k2] = t[k2];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Three-pass power-of-two path (rings of 256..4096 points). A block holds
 // 4096 points (R = 4096 / N rings), 16 per thread, and runs the Stockham
@@ -723,7 +818,7 @@ struct P3 {
   static constexpr int kThreads = kPoints / 16;
   static constexpr int R = kPoints / N;
   static constexpr int RS = N + N / 16 + (R > 8 ? 1 : (R > 1 ? 8 / R : 0));
-  static constexpr int kSmem = R * RS;  // double2 units
+  static constexpr int kSmem = R * RS;  // complex elements
   __device__ __forceinline__ static int at(int ring, int u) { return ring * RS + u + (u >> 4); }
 };
 
@@ -736,26 +831,34 @@ struct P3Radix {
                               : (rem % 8 == 0 ? 8 : (rem % 4 == 0 ? 4 : 2)));
 };
 
+// Blocks per SM the three-pass kernels are compiled for: two of 4096 FP64
+// points (128 registers a thread; one of 8192), three of 4096 FP32 points
+// (85 registers) and two of 8192 (64).
+template <int kPts, typename C>
+constexpr int p3_min_blocks() {
+  return sizeof(C) == 16 ? 8192 / kPts : (kPts >= 8192 ? 2 : 3);
+}
+
 // v[r] *= w^(t r), w = exp(sign 2 pi i / N) from the table at stride twStride.
-template <int P>
-__device__ __forceinline__ void p3_twiddle(double2 (&v)[P], const double2* __restrict__ tw, int t,
+template <int P, typename C>
+__device__ __forceinline__ void p3_twiddle(C (&v)[P], const C* __restrict__ tw, int t,
                                            int twStride, int sign) {
   if (t == 0) return;
-  const double2 a = twiddle(tw, t, twStride, sign);
+  const C a = twiddle(tw, t, twStride, sign);
   v[1] = cmul(v[1], a);
   if constexpr (P > 2) {
-    const double2 a2 = cmul(a, a), a3 = cmul(a2, a);
+    const C a2 = cmul(a, a), a3 = cmul(a2, a);
     v[2] = cmul(v[2], a2);
     v[3] = cmul(v[3], a3);
     if constexpr (P > 4) {
-      const double2 b = twiddle(tw, 4 * t, twStride, sign);
-      const double2 b1 = cmul(b, a), b2 = cmul(b, a2), b3 = cmul(b, a3);
+      const C b = twiddle(tw, 4 * t, twStride, sign);
+      const C b1 = cmul(b, a), b2 = cmul(b, a2), b3 = cmul(b, a3);
       v[4] = cmul(v[4], b);
       v[5] = cmul(v[5], b1);
       v[6] = cmul(v[6], b2);
       v[7] = cmul(v[7], b3);
       if constexpr (P > 8) {
-        const double2 c = twiddle(tw, 8 * t, twStride, sign);
+        const C c = twiddle(tw, 8 * t, twStride, sign);
         v[8] = cmul(v[8], c);
         v[9] = cmul(v[9], cmul(c, a));
         v[10] = cmul(v[10], cmul(c, a2));
@@ -770,15 +873,15 @@ __device__ __forceinline__ void p3_twiddle(double2 (&v)[P], const double2* __res
 }
 
 // Middle stages (every stage after the first and before the last), in place.
-template <int N, int kPts, int M>
-__device__ __forceinline__ void p3_middle(double2* buf, const double2* __restrict__ tw,
-                                          int twStride, int sign) {
+template <int N, int kPts, int M, typename C>
+__device__ __forceinline__ void p3_middle(C* buf, const C* __restrict__ tw, int twStride,
+                                          int sign) {
   constexpr int P = P3Radix<N, M>::P;
   if constexpr (M * P < N) {
     constexpr int L = N / (P * M);
     constexpr int NBR = N / P;
     constexpr int NB = 16 / P;
-    double2 v[NB][P];
+    C v[NB][P];
 #pragma unroll
     for (int b = 0; b < NB; b++) {
       const int g = threadIdx.x + b * P3<N, kPts>::kThreads;
@@ -799,7 +902,7 @@ __device__ __forceinline__ void p3_middle(double2* buf, const double2* __restric
       for (int r = 0; r < P; r++) buf[P3<N, kPts>::at(ring, k + j * P * M + r * M)] = v[b][r];
     }
     __syncthreads();
-    p3_middle<N, kPts, M * P>(buf, tw, twStride, sign);
+    p3_middle<N, kPts, M * P, C>(buf, tw, twStride, sign);
   }
 }
 
@@ -816,37 +919,70 @@ constexpr int kSpecBox = 64;
 
 // kTma: the block's spectral rows (orders 0..lmax for each sign, R
 // colatitudes each; the -m rows at the mirrored colatitudes) are brought into
-// shared memory by 4-D TMA boxes of kSpecBox rows before the first stage, so
-// the strided 16R-byte row segments cost no load instructions or registers;
-// the first stage reads them from shared memory. Without kTma the first
-// stage loads them from global memory directly.
+// a staging buffer by 4-D TMA boxes of kSpecBox rows, so the strided 16R-byte
+// row segments cost no load instructions or registers; the first stage
+// reads them from there. The kernel is then persistent: a block walks the
+// work items (ring group, field) with stride gridDim.x, and as soon as the
+// first stage has read an item's rows it starts the TMA of its next item's
+// rows, which arrive while the middle and last stages run. Without kTma,
+// one block per item, and the first stage loads from global memory.
 //
 // SpecT: double2 (the FP64 layout above) or float2, the spectra of the
 // BF16x3 form, which keeps its -m rows at their own colatitudes (no mirror:
 // the Legendre epilogue and operand preparation of that form apply it), so
 // both signs' TMA boxes start at colatitude j0.
-template <bool kReal, int N, bool kTma, int kPts, typename SpecT>
-__global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
+//
+// C: the butterflies' precision (double2, or float2 with float2 spectra);
+// the grid is written in FP64.
+template <bool kReal, int N, bool kTma, int kPts, typename SpecT, typename C>
+__global__ void __launch_bounds__(kPts / 16, p3_min_blocks<kPts, C>()) k_fft_inverse_p3(
     const __grid_constant__ CUtensorMap specMap, int L, int lmax, int nTheta, int thetaPad,
-    int count, const SpecT* __restrict__ spec, const double2* __restrict__ tw,
-    double* __restrict__ out, int* err, int smemElems, RingRange rr) {
+    int count, const SpecT* __restrict__ spec, const C* __restrict__ tw,
+    double* __restrict__ out, int* err, int stageOff, RingRange rr, int nGroups) {
   constexpr bool kMir = std::is_same<SpecT, double2>::value;
   // TMA destinations want 128-byte alignment: round the dynamic base up (the
-  // launch adds 128 bytes of slack plus the barrier word after the buffer).
+  // launch adds 128 bytes of slack plus the barrier word after the buffers).
   extern __shared__ unsigned char p3_raw[];
-  double2* smem = reinterpret_cast<double2*>(
+  unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(p3_raw) + 127) & ~uintptr_t(127));
-  uint64_t& bar = *reinterpret_cast<uint64_t*>(smem + smemElems);
+  C* smem = reinterpret_cast<C*>(base);
   constexpr int R = P3<N, kPts>::R;
-  const int j0 = (blockIdx.x + rr.jBegin / R) * R, f = blockIdx.y;
   const int nPhi = 2 * L;
   const int sgnCount = kReal ? 1 : 2;
   const int twStride = nPhi / N;
   const int nbox = (lmax + 1 + kSpecBox - 1) / kSpecBox;
   const int M1 = nbox * kSpecBox;  // staged rows per sign
-  SpecT* staged = reinterpret_cast<SpecT*>(smem);
-  auto S = [&](int m, int sgn, int jj) {
-    return to_d2(spec[((size_t)(m * sgnCount + sgn) * count + f) * thetaPad + jj]);
+  // stageOff: byte offset of the staging buffer. The barrier word lies
+  // past both buffers (which may overlap).
+  SpecT* staged = reinterpret_cast<SpecT*>(base + stageOff);
+  constexpr size_t kFftBytes = (sizeof(C) * P3<N, kPts>::kSmem + 127) / 128 * 128;
+  const size_t stageEnd = (size_t)stageOff + (size_t)sgnCount * M1 * R * sizeof(SpecT);
+  uint64_t& bar =
+      *reinterpret_cast<uint64_t*>(base + (stageEnd > kFftBytes ? stageEnd : kFftBytes));
+  const int items = kTma ? nGroups * count : 1;
+  // Colatitude of an item's first ring, and its field.
+  auto item = [&](int w, int& j0, int& f) {
+    if constexpr (kTma) {
+      const int grp = w % nGroups;
+      f = w / nGroups;
+      j0 = (grp + rr.jBegin / R) * R;
+    } else {
+      j0 = (blockIdx.x + rr.jBegin / R) * R;
+      f = blockIdx.y;
+    }
+  };
+  auto fetch = [&](int w) {  // one thread: the TMA boxes of item w
+    int j0, f;
+    item(w, j0, f);
+    tc::mbar_arrive_expect_tx(&bar, (uint32_t)(sgnCount * M1 * R * sizeof(SpecT)));
+    for (int sg = 0; sg < sgnCount; sg++) {
+      // Colatitudes j0.. (sign 0, and sign 1 without mirror) or their mirror
+      // images nTheta-j0-R.. (sign 1, FP64 layout).
+      const int x = 2 * ((sg == 0 || !kMir) ? j0 : nTheta - j0 - R);
+      for (int b = 0; b < nbox; b++)
+        tc::tma_load_4d(staged + (size_t)(sg * M1 + b * kSpecBox) * R, &specMap, &bar, x, f, sg,
+                        b * kSpecBox);
+    }
   };
   if constexpr (kTma) {
     if (threadIdx.x == 0) {
@@ -854,93 +990,109 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_inverse_p3(
       tc::fence_barrier_init();
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && (int)blockIdx.x < items) {
       tc::prefetch_tmap(&specMap);
-      tc::mbar_arrive_expect_tx(&bar, (uint32_t)(sgnCount * M1 * R * sizeof(SpecT)));
-      for (int sg = 0; sg < sgnCount; sg++) {
-        // Colatitudes j0.. (sign 0, and sign 1 without mirror) or their mirror
-        // images nTheta-j0-R.. (sign 1, FP64 layout).
-        const int x = 2 * ((sg == 0 || !kMir) ? j0 : nTheta - j0 - R);
-        for (int b = 0; b < nbox; b++)
-          tc::tma_load_4d(staged + (size_t)(sg * M1 + b * kSpecBox) * R, &specMap, &bar, x, f,
-                          sg, b * kSpecBox);
-      }
+      fetch(blockIdx.x);
     }
-    tc::mbar_wait(&bar, 0, err, 21);
   }
-  // First stage (radix 16, M = 1), rings interleaved across lanes so that
-  // lanes 0..R-1 read R consecutive colatitudes of one spectral row.
-  {
-    const int r = threadIdx.x & (R - 1), jj = threadIdx.x >> ilog2(R);
-    const int th = j0 + r;
-    double2 v[16];
-    // Row m of sign sg (staged): colatitude j0 + r is element r, its mirror
-    // nTheta-1-(j0+r) element R-1-r.
-    auto T = [&](int m, int sg) {
-      return to_d2(sg == 0 ? staged[(size_t)m * R + r]
-                           : staged[(size_t)(M1 + m) * R + (kMir ? R - 1 - r : r)]);
+  int it = 0;
+  for (int w = kTma ? (int)blockIdx.x : 0; w < items; w += kTma ? (int)gridDim.x : 1, it++) {
+    int j0, f;
+    item(w, j0, f);
+    auto S = [&](int m, int sgn, int jj) {
+      return to_c<C>(spec[((size_t)(m * sgnCount + sgn) * count + f) * thetaPad + jj]);
     };
+    if constexpr (kTma) {
+      // Every thread leaves together if the rows do not arrive in time.
+      const bool ok = tc::mbar_wait(&bar, it & 1, err, 21);
+      if (__syncthreads_or(!ok)) break;
+    }
+    // First stage (radix 16, M = 1), rings interleaved across lanes so that
+    // lanes 0..R-1 read R consecutive colatitudes of one spectral row.
+    {
+      const int r = threadIdx.x & (R - 1), jj = threadIdx.x >> ilog2(R);
+      const int th = j0 + r;
+      C v[16];
+      // Row m of sign sg (staged): colatitude j0 + r is element r, its mirror
+      // nTheta-1-(j0+r) element R-1-r.
+      auto T = [&](int m, int sg) {
+        return to_c<C>(sg == 0 ? staged[(size_t)m * R + r]
+                               : staged[(size_t)(M1 + m) * R + (kMir ? R - 1 - r : r)]);
+      };
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-      const int bin = jj + q * (N / 16);
-      double2 x = make_double2(0.0, 0.0);
-      if (kTma || th < nTheta) {
-        if (!kReal) {
-          if (bin <= lmax) x = kTma ? T(bin, 0) : S(bin, 0, th);
-          if (bin >= nPhi - lmax)
-            x = cadd(x, kTma ? T(nPhi - bin, 1) : S(nPhi - bin, 1, kMir ? nTheta - 1 - th : th));
-        } else {
-          const int M = L, bc = M - bin;
-          double2 x0 = bin <= lmax ? (kTma ? T(bin, 0) : S(bin, 0, th)) : make_double2(0.0, 0.0);
-          double2 x1 = bc <= lmax ? (kTma ? T(bc, 0) : S(bc, 0, th)) : make_double2(0.0, 0.0);
-          if (bin == 0) x0.y = 0.0;
-          if (bc == M) x1.y = 0.0;
-          const double2 xc = cconj(x1);
-          const double2 w = twiddle(tw, bin, 1, +1);
-          x = cadd(cadd(x0, xc), cmul_si(cmul(w, csub(x0, xc)), +1));
+      for (int q = 0; q < 16; q++) {
+        const int bin = jj + q * (N / 16);
+        C x{};
+        if (kTma || th < nTheta) {
+          if (!kReal) {
+            if (bin <= lmax) x = kTma ? T(bin, 0) : S(bin, 0, th);
+            if (bin >= nPhi - lmax)
+              x = cadd(x, kTma ? T(nPhi - bin, 1) : S(nPhi - bin, 1, kMir ? nTheta - 1 - th : th));
+          } else {
+            const int M = L, bc = M - bin;
+            C x0 = bin <= lmax ? (kTma ? T(bin, 0) : S(bin, 0, th)) : C{};
+            C x1 = bc <= lmax ? (kTma ? T(bc, 0) : S(bc, 0, th)) : C{};
+            if (bin == 0) x0.y = 0;
+            if (bc == M) x1.y = 0;
+            const C xc = cconj(x1);
+            const C w2 = twiddle(tw, bin, 1, +1);
+            x = cadd(cadd(x0, xc), cmul_si(cmul(w2, csub(x0, xc)), +1));
+          }
+        }
+        v[q] = x;
+      }
+      // The staging buffer is read and the previous item's last stage has
+      // read the FFT buffer: start the next item's rows (a block has a next
+      // item only when the staging buffer is its own), then fill the FFT
+      // buffer.
+      __syncthreads();
+      if constexpr (kTma) {
+        if (threadIdx.x == 0 && w + (int)gridDim.x < items) {
+          tc::fence_proxy_async();
+          fetch(w + gridDim.x);
         }
       }
-      v[q] = x;
+      dft_reg<16>(v, +1);
+      p3_twiddle<16>(v, tw, jj, twStride, +1);
+#pragma unroll
+      for (int q = 0; q < 16; q++) smem[P3<N, kPts>::at(r, jj * 16 + q)] = v[q];
     }
-    if constexpr (kTma) __syncthreads();  // the staged rows share the buffer
-    dft_reg<16>(v, +1);
-    p3_twiddle<16>(v, tw, jj, twStride, +1);
+    __syncthreads();
+    p3_middle<N, kPts, 16>(smem, tw, twStride, +1);
+    // Last stage (L = 1, no twiddles), ring-major so that lanes write
+    // consecutive longitudes.
+    constexpr int M = p3_last_m<N>();
+    constexpr int P = N / M;
+    constexpr int NB = 16 / P;
 #pragma unroll
-    for (int q = 0; q < 16; q++) smem[P3<N, kPts>::at(r, jj * 16 + q)] = v[q];
-  }
-  __syncthreads();
-  p3_middle<N, kPts, 16>(smem, tw, twStride, +1);
-  // Last stage (L = 1, no twiddles), ring-major so that lanes write
-  // consecutive longitudes.
-  constexpr int M = p3_last_m<N>();
-  constexpr int P = N / M;
-  constexpr int NB = 16 / P;
+    for (int b = 0; b < NB; b++) {
+      const int g = threadIdx.x + b * P3<N, kPts>::kThreads;
+      const int ring = g >> ilog2(M), k = g & (M - 1);
+      C v[P];
 #pragma unroll
-  for (int b = 0; b < NB; b++) {
-    const int g = threadIdx.x + b * P3<N, kPts>::kThreads;
-    const int ring = g >> ilog2(M), k = g & (M - 1);
-    double2 v[P];
+      for (int q = 0; q < P; q++) v[q] = smem[P3<N, kPts>::at(ring, k + q * M)];
+      dft_reg<P>(v, +1);
+      const int th = j0 + ring;
+      if (rr.has(th)) {
+        double2* row = kReal ? reinterpret_cast<double2*>(out + ((size_t)f * nTheta + th) * nPhi)
+                             : reinterpret_cast<double2*>(out) + ((size_t)f * nTheta + th) * nPhi;
 #pragma unroll
-    for (int q = 0; q < P; q++) v[q] = smem[P3<N, kPts>::at(ring, k + q * M)];
-    dft_reg<P>(v, +1);
-    const int th = j0 + ring;
-    if (rr.has(th)) {
-      double2* row = kReal ? reinterpret_cast<double2*>(out + ((size_t)f * nTheta + th) * nPhi)
-                           : reinterpret_cast<double2*>(out) + ((size_t)f * nTheta + th) * nPhi;
-#pragma unroll
-      for (int r = 0; r < P; r++) row[k + r * M] = v[r];
+        for (int r = 0; r < P; r++) row[k + r * M] = to_c<double2>(v[r]);
+      }
     }
   }
 }
 
 // SpecT as for the inverse: float2 spectra keep the -m rows unmirrored.
 template <bool kReal, int N, int kPts, typename SpecT>
-__global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
+__global__ void __launch_bounds__(kPts / 16, p3_min_blocks<kPts, SpecT>()) k_fft_forward_p3(
     int L, int lmax, int nTheta, int thetaPad, int count, const double* __restrict__ in,
-    const double* __restrict__ weight, const double2* __restrict__ tw,
+    const double* __restrict__ weight, const SpecT* __restrict__ tw,
     SpecT* __restrict__ spec, RingRange rr) {
+  using C = SpecT;  // butterflies in the spectra's precision
   constexpr bool kMir = std::is_same<SpecT, double2>::value;
-  extern __shared__ double2 smem[];
+  extern __shared__ unsigned char p3f_raw[];
+  C* smem = reinterpret_cast<C*>(p3f_raw);
   constexpr int R = P3<N, kPts>::R;
   const int j0 = (blockIdx.x + rr.jBegin / R) * R, f = blockIdx.y;
   const int nPhi = 2 * L;
@@ -961,11 +1113,11 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
     constexpr int NBR = N / 16;
     const int ring = threadIdx.x >> ilog2(NBR), jj = threadIdx.x & (NBR - 1);
     const int th = j0 + ring;
-    double2 v[16];
+    C v[16];
     const double2* row = kReal ? reinterpret_cast<const double2*>(in + ((size_t)f * nTheta + th) * nPhi)
                                : reinterpret_cast<const double2*>(in) + ((size_t)f * nTheta + th) * nPhi;
 #pragma unroll
-    for (int q = 0; q < 16; q++) v[q] = th < nTheta ? row[jj + q * NBR] : make_double2(0.0, 0.0);
+    for (int q = 0; q < 16; q++) v[q] = th < nTheta ? to_c<C>(row[jj + q * NBR]) : C{};
     dft_reg<16>(v, -1);
     p3_twiddle<16>(v, tw, jj, twStride, -1);
 #pragma unroll
@@ -984,7 +1136,7 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
     for (int b = 0; b < NB; b++) {
       const int g = threadIdx.x + b * P3<N, kPts>::kThreads;
       const int ring = g & (R - 1), k = g >> ilog2(R);
-      double2 v[P];
+      C v[P];
 #pragma unroll
       for (int q = 0; q < P; q++) v[q] = smem[P3<N, kPts>::at(ring, k + q * M)];
       dft_reg<P>(v, -1);
@@ -994,16 +1146,16 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
 #pragma unroll
         for (int r = 0; r < P; r++) {
           const int bin = k + r * M;
-          const double2 x = cscale(v[r], scale);
+          const C x = cscale(v[r], scale);
           const int thm = kMir ? nTheta - 1 - th : th;
-          if (bin <= lmax) S(bin, 0, th) = from_d2<SpecT>(x);
-          if (bin == 0) S(0, 1, thm) = from_d2<SpecT>(make_double2(0.0, 0.0));
-          else if (bin >= nPhi - lmax) S(nPhi - bin, 1, thm) = from_d2<SpecT>(x);
+          if (bin <= lmax) S(bin, 0, th) = x;
+          if (bin == 0) S(0, 1, thm) = C{};
+          else if (bin >= nPhi - lmax) S(nPhi - bin, 1, thm) = x;
         }
       }
     }
   } else {
-    double2 v[NB][P];
+    C v[NB][P];
 #pragma unroll
     for (int b = 0; b < NB; b++) {
       const int g = threadIdx.x + b * P3<N, kPts>::kThreads;
@@ -1029,12 +1181,12 @@ __global__ void __launch_bounds__(kPts / 16, 8192 / kPts) k_fft_forward_p3(
       if (!rr.has(th)) continue;
       const double scale = weight[th] * twoPiOverN;
       const int Mh = L;
-      const double2 z0 = smem[P3<N, kPts>::at(r, m == Mh ? 0 : m)];
-      const double2 zc = cconj(smem[P3<N, kPts>::at(r, m == 0 ? 0 : Mh - m)]);
-      const double2 w = twiddle(tw, m, 1, -1);
-      const double2 ev = cscale(cadd(z0, zc), 0.5);
-      const double2 od = cscale(cmul_si(csub(z0, zc), -1), 0.5);
-      S(m, 0, th) = from_d2<SpecT>(cscale(cadd(ev, cmul(w, od)), scale));
+      const C z0 = smem[P3<N, kPts>::at(r, m == Mh ? 0 : m)];
+      const C zc = cconj(smem[P3<N, kPts>::at(r, m == 0 ? 0 : Mh - m)]);
+      const C w = twiddle(tw, m, 1, -1);
+      const C ev = cscale(cadd(z0, zc), 0.5);
+      const C od = cscale(cmul_si(csub(z0, zc), -1), 0.5);
+      S(m, 0, th) = cscale(cadd(ev, cmul(w, od)), scale);
     }
   }
 }
@@ -1065,15 +1217,25 @@ inline unsigned ring_blocks(RingRange rr, int R) {
   return (unsigned)((rr.jEnd + R - 1) / R - rr.jBegin / R);
 }
 
-template <int N, int kPts, typename SpecT>
-gsht_status launch_p3_dir(const gsht_grid* g, int dir, int lmax, int is_real, int count,
-                          const void* src, void* dst, cudaStream_t s, RingRange rr) {
+// Butterflies of the inverse with FP32 spectra: FP64 by default (measured at
+// lmax 1024, 64 fields: 0.91 ms against 1.08 ms for FP32 butterflies, whose
+// FFT buffer lets three blocks share an SM); GSHT_FFT_INV_FP32=1 selects the
+// FP32 ones for comparisons.
+bool fp32_inverse_butterflies() {
+  const char* e = getenv("GSHT_FFT_INV_FP32");
+  return e && e[0] == '1';
+}
+
+template <int N, int kPts, typename SpecT, typename C>
+gsht_status launch_p3_inverse(const gsht_grid* g, int lmax, int is_real, int count,
+                              const void* src, void* dst, cudaStream_t s, RingRange rr) {
   constexpr int kThr = P3<N, kPts>::kThreads;
-  size_t shmem = sizeof(double2) * P3<N, kPts>::kSmem;
+  size_t shmem = sizeof(C) * P3<N, kPts>::kSmem;  // FFT buffer of the butterflies' precision
   constexpr int R = P3<N, kPts>::R;
   dim3 grid(ring_blocks(rr, R), count);
-  const double2* tw = reinterpret_cast<const double2*>(g->d_twiddle);
-  if (dir == 1) {
+  const C* tw = std::is_same<C, float2>::value ? reinterpret_cast<const C*>(g->d_twiddle32)
+                                               : reinterpret_cast<const C*>(g->d_twiddle);
+  {
     const SpecT* spec = static_cast<const SpecT*>(src);
     double* out = static_cast<double*>(dst);
     // Staged spectral rows: sign x ceil((lmax+1)/kSpecBox) boxes x R colatitudes.
@@ -1083,26 +1245,65 @@ gsht_status launch_p3_dir(const gsht_grid* g, int dir, int lmax, int is_real, in
     CUtensorMap map{};
     // TMA boxes start at x = 2 j0 components: 16-byte aligned for FP64
     // always, for FP32 when R (and so j0) is even; the box is 2R components.
+    // With a staging buffer of its own after the FFT buffer (128-byte
+    // aligned, then the barrier word; 128 bytes of slack align the dynamic
+    // base), the kernel runs persistent with the next item's rows in flight,
+    // as long as two blocks still fit on an SM (the FP32 spectra of the
+    // BF16x3 form). Otherwise (FP64 spectra, twice the bytes) the staging
+    // shares the FFT buffer and each block takes one item.
     const bool aligned = sizeof(SpecT) == 16 || R % 2 == 0;
-    const bool tma = aligned && staged <= (shmem > 110 * 1024 ? shmem : 110 * 1024) &&
+    const size_t fftBytes = (shmem + 127) / 128 * 128;
+    const bool tma = aligned && staged + 16 + 128 <= 227 * 1024 &&
                      spec_map(&map, spec, g->theta_pad, count, sgnCount, lmax, R);
-    if (tma) shmem = shmem > staged ? shmem : staged;
-    const int smemElems = (int)(shmem / sizeof(double2));
-    shmem += 128 + 16;
+    const bool ahead = tma && fftBytes + staged + 16 + 128 <= 113 * 1024;
+    const int stageOff = ahead ? (int)fftBytes : 0;  // bytes
+    shmem = (ahead ? fftBytes + staged : (fftBytes > staged ? fftBytes : staged)) + 16 + 128;
+    const int groups = (int)ring_blocks(rr, R);
     if (tma) {
-      auto k = is_real ? k_fft_inverse_p3<true, N, true, kPts, SpecT>
-                       : k_fft_inverse_p3<false, N, true, kPts, SpecT>;
+      auto k = is_real ? k_fft_inverse_p3<true, N, true, kPts, SpecT, C>
+                       : k_fft_inverse_p3<false, N, true, kPts, SpecT, C>;
       GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
-      k<<<grid, kThr, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count, spec, tw, out,
-                                  g->d_err, smemElems, rr);
+      const long items = (long)groups * count;
+      long blocks = items;
+      if (ahead) {
+        int sms = 148, per = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kThr, shmem) != cudaSuccess ||
+            per < 1) {
+          cudaGetLastError();
+          per = 1;
+        }
+        if (blocks > (long)sms * per) blocks = (long)sms * per;
+      }
+      k<<<(unsigned)blocks, kThr, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count,
+                                              spec, tw, out, g->d_err, stageOff, rr, groups);
     } else {
-      auto k = is_real ? k_fft_inverse_p3<true, N, false, kPts, SpecT>
-                       : k_fft_inverse_p3<false, N, false, kPts, SpecT>;
+      auto k = is_real ? k_fft_inverse_p3<true, N, false, kPts, SpecT, C>
+                       : k_fft_inverse_p3<false, N, false, kPts, SpecT, C>;
       GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
       k<<<grid, kThr, shmem, s>>>(map, g->L, lmax, g->n_theta, g->theta_pad, count, spec, tw, out,
-                                  g->d_err, smemElems, rr);
+                                  g->d_err, stageOff, rr, groups);
     }
     GSHT_LAUNCH_CHECK("k_fft_inverse_p3");
+  }
+  return GSHT_OK;
+}
+
+template <int N, int kPts, typename SpecT>
+gsht_status launch_p3_dir(const gsht_grid* g, int dir, int lmax, int is_real, int count,
+                          const void* src, void* dst, cudaStream_t s, RingRange rr) {
+  constexpr int kThr = P3<N, kPts>::kThreads;
+  // Forward: butterflies in the spectra's precision.
+  size_t shmem = sizeof(SpecT) * P3<N, kPts>::kSmem;
+  constexpr int R = P3<N, kPts>::R;
+  dim3 grid(ring_blocks(rr, R), count);
+  const SpecT* tw = std::is_same<SpecT, float2>::value
+                        ? reinterpret_cast<const SpecT*>(g->d_twiddle32)
+                        : reinterpret_cast<const SpecT*>(g->d_twiddle);
+  if (dir == 1) {
+    if (std::is_same<SpecT, float2>::value && fp32_inverse_butterflies())
+      return launch_p3_inverse<N, kPts, SpecT, SpecT>(g, lmax, is_real, count, src, dst, s, rr);
+    return launch_p3_inverse<N, kPts, SpecT, double2>(g, lmax, is_real, count, src, dst, s, rr);
   } else {
     auto k = is_real ? k_fft_forward_p3<true, N, kPts, SpecT> : k_fft_forward_p3<false, N, kPts, SpecT>;
     GSHT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));

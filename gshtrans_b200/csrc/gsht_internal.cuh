@@ -25,6 +25,13 @@ extern std::atomic<unsigned long long> g_launches;
 // one thread, whichever other threads launch meanwhile).
 extern thread_local unsigned long long t_launches;
 
+// Per-role trace of the tensor-core Legendre kernels (diagnostics.cu): when
+// set, launches take the traced kernel copies, whose counters trace_slots
+// (form 0 BF16x3, 1 Ozaki; dir 0 inverse, 1 forward) clears on stream s and
+// returns (NULL on failure).
+extern int g_tc_trace;
+unsigned long long* trace_slots(int form, int dir, cudaStream_t s);
+
 #define GSHT_CUDA(call)                                   \
   do {                                                    \
     cudaError_t e_ = (call);                              \
@@ -165,6 +172,7 @@ struct gsht_grid {
   double* d_theta = nullptr;              // device nodes
   double* d_weight = nullptr;
   double* d_twiddle = nullptr;            // FFT twiddles exp(-2 pi i t / nPhi), t < nPhi
+  float* d_twiddle32 = nullptr;           // the same rounded to FP32 (FP32-spectrum FFTs)
   int* d_err = nullptr;                   // device error word (bounded-wait timeouts)
 
   std::vector<gsht::Table> tables;        // index n - min_n

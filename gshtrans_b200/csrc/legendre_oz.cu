@@ -61,6 +61,7 @@ struct OzArgs {
   double2* out;
   long coefSize;
   int* err;
+  unsigned long long* trace;  // kTrSlots counters of a traced launch
 };
 
 // Four warps per TMEM lane quarter, 16 columns each: the MMA warp waits for
@@ -80,7 +81,7 @@ __device__ __forceinline__ double i32_to_f64(uint32_t v) {
 // Persistent kernel over the tile list (see legendre_tc.cu for the protocol):
 // the epilogue sums the 7 diagonal accumulators of its 32 columns in FP64,
 // releases TMEM, then writes.
-template <int kDir, int kS, int kN>
+template <int kDir, int kS, int kN, bool kTrace>
 __global__ void __launch_bounds__(kThreads, 1)
     k_legendre_oz(const __grid_constant__ CUtensorMap mapA,
                   const __grid_constant__ CUtensorMap mapB, OzArgs p,
@@ -103,6 +104,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (threadIdx.x == 0) skip = *reinterpret_cast<volatile int*>(p.err);
   __syncthreads();
   if (skip || blockIdx.x >= numTiles) return;
+  long long trStart = 0, trW1 = 0, trW2 = 0;  // trace: start, first and second wait
+  if constexpr (kTrace) trStart = clock64();
 
   if (warp == 0 && lane == 0) {
     for (int s = 0; s < kStages; s++) {
@@ -131,7 +134,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int bRow = tl.x * p.R + tl.z * kN;
         for (int kc = 0; kc < tl.w; kc++, it++) {
           const int s = it % kStages;
-          if (it >= kStages && !mbar_wait(&empty[s], ((it / kStages) - 1) & 1, p.err, 11)) {
+          if (it >= kStages && !timed_wait<kTrace>(trW1, &empty[s], ((it / kStages) - 1) & 1, p.err, 11)) {
             ok = false;
             break;
           }
@@ -161,11 +164,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         // K steps of 32 past the last degree (inverse) or colatitude
         // (forward) multiply zero padding and are not issued.
         const int kLim = kDir == 0 ? p.lmax - (tl.x > p.na ? tl.x : p.na) + 1 : p.nTheta;
-        if (tc > 0 && !mbar_wait(accEmpty, (tc - 1) & 1, p.err, 14)) break;
+        if (tc > 0 && !timed_wait<kTrace>(trW2, accEmpty, (tc - 1) & 1, p.err, 14)) break;
         tc_fence_after();
         for (int kc = 0; kc < nk; kc++, it++) {
           const int s = it % kStages;
-          if (!mbar_wait(&full[s], (it / kStages) & 1, p.err, 12)) {
+          if (!timed_wait<kTrace>(trW1, &full[s], (it / kStages) & 1, p.err, 12)) {
             ok = false;
             break;
           }
@@ -217,7 +220,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int t = blockIdx.x; t < numTiles; t += gridDim.x, tc++) {
       const int4 tl = tiles[t];
       const int m = tl.x;
-      if (!mbar_wait(accFull, tc & 1, p.err, 13)) break;
+      if (!timed_wait<kTrace>(trW1, accFull, tc & 1, p.err, 13)) break;
       tc_fence_after();
       double acc[kCols];
 #pragma unroll
@@ -259,6 +262,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   }
+  if constexpr (kTrace)
+    if (lane == 0) trace_role(p.trace, warp, true, trStart, trW1, trW2);
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
@@ -474,11 +479,21 @@ gsht_status launch_oz(const gsht_grid* g, const OzArgs& a, const CUtensorMap& ma
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
   const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kN, kBK, &st);
   if (!tl) return st;
-  auto kern = k_legendre_oz<kDir, kS, kN>;
   constexpr size_t kSmem = OzCfg<kS, kN>::kSmemBytes;
-  GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
   const int blocks = tl->count < sms ? tl->count : sms;
-  kern<<<blocks, kThreads, kSmem, s>>>(mapA, mapB, a, tl->d_tiles, tl->count);
+  if (g_tc_trace) {
+    // Traced copy (same results), counters of the form's direction.
+    OzArgs b = a;
+    b.trace = trace_slots(1, kDir, s);
+    if (!b.trace) return fail(GSHT_ERR_CUDA, "trace counters unavailable");
+    auto kern = k_legendre_oz<kDir, kS, kN, true>;
+    GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+    kern<<<blocks, kThreads, kSmem, s>>>(mapA, mapB, b, tl->d_tiles, tl->count);
+  } else {
+    auto kern = k_legendre_oz<kDir, kS, kN, false>;
+    GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+    kern<<<blocks, kThreads, kSmem, s>>>(mapA, mapB, a, tl->d_tiles, tl->count);
+  }
   GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_oz<inverse>" : "k_legendre_oz<forward>");
   return GSHT_OK;
 }

@@ -49,6 +49,7 @@ struct TcArgs {
   float2* out32;
   long coefSize;
   int* err;
+  unsigned long long* trace;  // kTrSlots counters of a traced launch
 };
 
 // TMEM accumulators per tile: products of very different magnitude would
@@ -75,7 +76,7 @@ constexpr int kThreads = 32 * (2 + kEpiWarps);
 // The producer runs ahead across tile boundaries; the epilogue copies its
 // accumulator columns out of TMEM, releases TMEM to the MMA warp (accEmpty),
 // and only then writes results, so stores overlap the next tile's MMAs.
-template <int kDir, int kNA, int kNB, int kNP, int kN, int kStages, int kBK>
+template <int kDir, int kNA, int kNB, int kNP, int kN, int kStages, int kBK, bool kTrace>
 __global__ void __launch_bounds__(kThreads, 1)
     k_legendre_tc(const __grid_constant__ CUtensorMap mapA,
                   const __grid_constant__ CUtensorMap mapB, TcArgs p,
@@ -102,6 +103,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (threadIdx.x == 0) skip = *reinterpret_cast<volatile int*>(p.err);
   __syncthreads();
   if (skip || blockIdx.x >= numTiles) return;
+  long long trStart = 0, trW1 = 0, trW2 = 0;  // trace: start, first and second wait
+  if constexpr (kTrace) trStart = clock64();
 
   if (warp == 0 && lane == 0) {
     for (int s = 0; s < kStages; s++) {
@@ -131,7 +134,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int bRow = tl.x * p.R + tl.z * kN;
         for (int kc = 0; kc < tl.w; kc++, it++) {
           const int s = it % kStages;
-          if (it >= kStages && !mbar_wait(&empty[s], ((it / kStages) - 1) & 1, p.err, 1)) {
+          if (it >= kStages && !timed_wait<kTrace>(trW1, &empty[s], ((it / kStages) - 1) & 1, p.err, 1)) {
             ok = false;
             break;
           }
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         // K steps of 16 past the last degree (inverse) or colatitude
         // (forward) multiply zero padding and are not issued.
         const int kLim = kDir == 0 ? p.lmax - (tl.x > p.na ? tl.x : p.na) + 1 : p.nTheta;
-        if (tc > 0 && !mbar_wait(accEmptyA, (tc - 1) & 1, p.err, 4)) break;
+        if (tc > 0 && !timed_wait<kTrace>(trW2, accEmptyA, (tc - 1) & 1, p.err, 4)) break;
         tc_fence_after();
         bool haveB = tc == 0;
         // hi.hi products go to one of nbig accumulators by K block; the five
@@ -172,7 +175,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int nbig = nk < kBigAcc ? nk : kBigAcc;
         for (int kc = 0; kc < nk; kc++, it++) {
           const int s = it % kStages;
-          if (!mbar_wait(&full[s], (it / kStages) & 1, p.err, 2)) {
+          if (!timed_wait<kTrace>(trW1, &full[s], (it / kStages) & 1, p.err, 2)) {
             ok = false;
             break;
           }
@@ -180,7 +183,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           const int big = 1 + (kc * nbig) / nk;
           const int bigFirst = ((big - 1) * nk + nbig - 1) / nbig;
           if (!haveB && big >= 2) {
-            if (!mbar_wait(accEmptyB, (tc - 1) & 1, p.err, 5)) {
+            if (!timed_wait<kTrace>(trW2, accEmptyB, (tc - 1) & 1, p.err, 5)) {
               ok = false;
               break;
             }
@@ -222,7 +225,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         // Keep accEmptyB in step with the tiles even if this one used no
         // accumulator above 1.
-        if (ok && !haveB && !mbar_wait(accEmptyB, (tc - 1) & 1, p.err, 5)) ok = false;
+        if (ok && !haveB && !timed_wait<kTrace>(trW2, accEmptyB, (tc - 1) & 1, p.err, 5)) ok = false;
         if (!ok) break;
         mma_commit(accFull);
       }
@@ -236,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int t = blockIdx.x; t < numTiles; t += gridDim.x, tc++) {
       const int4 tl = tiles[t];
       const int m = tl.x, nk = tl.w;
-      if (!mbar_wait(accFull, tc & 1, p.err, 3)) break;
+      if (!timed_wait<kTrace>(trW1, accFull, tc & 1, p.err, 3)) break;
       tc_fence_after();
       const int nbig = nk < kBigAcc ? nk : kBigAcc;
       double acc[kCols];
@@ -309,6 +312,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   }
+  if constexpr (kTrace)
+    if (lane == 0) trace_role(p.trace, warp, true, trStart, trW1, trW2);
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
@@ -354,7 +359,7 @@ __device__ __forceinline__ int pair_tile_n(int valid) {
   return valid >= kPairN ? kPairN : (valid + 31) / 32 * 32;
 }
 
-template <int kDir, int kStages, int kBK>
+template <int kDir, int kStages, int kBK, bool kTrace>
 __global__ void __launch_bounds__(kThreads, 1)
     k_legendre_tc2(const __grid_constant__ CUtensorMap mapT,
                    const __grid_constant__ CUtensorMap mapF, TcArgs p,
@@ -377,6 +382,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t rank = cluster_rank();
   const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
   if (pair >= numTiles) return;  // both CTAs of the pair leave together
+  long long trStart = 0, trW1 = 0, trW2 = 0;  // trace: start, first and second wait
+  if constexpr (kTrace) trStart = clock64();
 
   if (warp == 0 && lane == 0) {
     for (int s = 0; s < kStages; s++) {
@@ -410,7 +417,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int half = (int)rank * (pair_tile_n(limit - tl.y * kPairN) / 2);
         for (int kc = 0; kc < tl.w; kc++, it++) {
           const int s = it % kStages;
-          if (it >= kStages && !mbar_wait(&empty[s], ((it / kStages) - 1) & 1, p.err, 11)) {
+          if (it >= kStages && !timed_wait<kTrace>(trW1, &empty[s], ((it / kStages) - 1) & 1, p.err, 11)) {
             ok = false;
             break;
           }
@@ -437,7 +444,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       // the CTA leaves.
       const int pending = it < kStages ? it : kStages;
       for (int i = it - pending; i < it && ok; i++)
-        if (!mbar_wait(&empty[i % kStages], (i / kStages) & 1, p.err, 16)) ok = false;
+        if (!timed_wait<kTrace>(trW1, &empty[i % kStages], (i / kStages) & 1, p.err, 16)) ok = false;
     }
   } else if (warp == 1) {
     if (rank == 0 && lane == 0) {
@@ -450,13 +457,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int limit = kDir == 0 ? p.nTheta : p.lmax - (tl.x > p.na ? tl.x : p.na) + 1;
         const uint32_t id =
             idesc(1, 1, 0, kDir == 0 ? 1 : 0, pair_tile_n(limit - tl.y * kPairN), kPairM);
-        if (tc > 0 && !mbar_wait(accEmptyA, (tc - 1) & 1, p.err, 14)) break;
+        if (tc > 0 && !timed_wait<kTrace>(trW2, accEmptyA, (tc - 1) & 1, p.err, 14)) break;
         tc_fence_after();
         bool haveB = tc == 0;
         const int nbig = nk < kBigAcc ? nk : kBigAcc;
         for (int kc = 0; kc < nk; kc++, it++) {
           const int s = it % kStages;
-          if (!mbar_wait(&full[s], (it / kStages) & 1, p.err, 12)) {
+          if (!timed_wait<kTrace>(trW1, &full[s], (it / kStages) & 1, p.err, 12)) {
             ok = false;
             break;
           }
@@ -464,7 +471,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           const int big = 1 + (kc * nbig) / nk;
           const int bigFirst = ((big - 1) * nk + nbig - 1) / nbig;
           if (!haveB && big >= 2) {
-            if (!mbar_wait(accEmptyB, (tc - 1) & 1, p.err, 15)) {
+            if (!timed_wait<kTrace>(trW2, accEmptyB, (tc - 1) & 1, p.err, 15)) {
               ok = false;
               break;
             }
@@ -502,7 +509,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           else issue(std::false_type{});
           mma_commit_pair(&empty[s], 0x3);
         }
-        if (ok && !haveB && !mbar_wait(accEmptyB, (tc - 1) & 1, p.err, 15)) ok = false;
+        if (ok && !haveB && !timed_wait<kTrace>(trW2, accEmptyB, (tc - 1) & 1, p.err, 15)) ok = false;
         if (!ok) break;
         mma_commit_pair(accFull, 0x3);
       }
@@ -527,7 +534,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       // Columns of a narrowed tail tile past its width hold stale values:
       // a warp whose 64 columns all lie there drains nothing.
       const bool live = group * kCols < pair_tile_n(limit - tl.y * kPairN);
-      if (!mbar_wait(accFull, tc & 1, p.err, 13)) break;
+      if (!timed_wait<kTrace>(trW1, accFull, tc & 1, p.err, 13)) break;
       tc_fence_after();
       const int nbig = nk < kBigAcc ? nk : kBigAcc;
       double acc[kCols];
@@ -621,6 +628,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   }
+  if constexpr (kTrace)
+    if (lane == 0) trace_role(p.trace, warp, rank == 0, trStart, trW1, trW2);
   tc_fence_before();
   cluster_sync();  // no arrival is still on its way into either CTA
   if (warp == 1) {
@@ -655,58 +664,69 @@ __device__ __forceinline__ void split3(float x, __nv_bfloat16& h, __nv_bfloat16&
 }
 
 // Inverse: packed coefficients -> B[split][m*R + 2q + part][k], k = l - l0(m)
-// < Kp_m (zero beyond lmax). One block per 32 degrees x 32 orders of one
-// field row q: the packed layout is contiguous along orders for a fixed
-// degree, so the tile is read order-major (coalesced), transposed in shared
+// < Kp_m (zero beyond lmax). One block per 32 degrees x 32 orders of kQB
+// field rows q: the packed layout is contiguous along orders for a fixed
+// degree, so each tile is read order-major (coalesced), transposed in shared
 // memory and written degree-major (each order's operand row segment).
 // blockIdx.x walks the triangle of (degree tile a, order tile b <= a) pairs
 // row by row (row b holds nA - b tiles), so no block is launched for the
 // empty upper half.
+template <int kQB>
 __global__ void __launch_bounds__(256) k_prep_inverse_bf16(
     int lmax, int n, int na, int count, int Q, int R, int isReal, long coefSize, int pitch,
     size_t plane, int nA, const double2* __restrict__ coef, __nv_bfloat16* __restrict__ op) {
-  __shared__ double2 tile[32][33];
+  __shared__ double2 tile[kQB][32][33];
   int i0 = blockIdx.x, b = 0;
   while (i0 >= nA - b) {
     i0 -= nA - b;
     b++;
   }
-  const int lt = (b + i0) * 32, mt = b * 32, q = blockIdx.z;
-  const int sgn = q / count, f = q - sgn * count;
+  const int lt = (b + i0) * 32, mt = b * 32, qBase = blockIdx.z * kQB;
   if (lt + 31 < (mt > na ? mt : na) || mt > lmax) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // All kQB tiles' loads are issued before the one barrier.
 #pragma unroll
-  for (int i = warp; i < 32; i += 8) {
-    const int l = lt + i, m = mt + lane;
-    double2 v = make_double2(0.0, 0.0);
-    if (l <= lmax && m <= l && l >= na && !(sgn == 1 && m == 0)) {
-      const long idx = isReal ? (long)l * (l + 1) / 2 - (long)na * (na + 1) / 2 + m
-                              : (long)l * l - (long)n * n + l + (sgn ? -m : m);
-      v = coef[(size_t)f * coefSize + idx];
-      if (sgn == 1 && ((l + n) & 1)) v = make_double2(-v.x, -v.y);
+  for (int u = 0; u < kQB; u++) {
+    const int q = qBase + u;
+    const int sgn = q / count, f = q - sgn * count;
+#pragma unroll
+    for (int i = warp; i < 32; i += 8) {
+      const int l = lt + i, m = mt + lane;
+      double2 v = make_double2(0.0, 0.0);
+      if (q < Q && l <= lmax && m <= l && l >= na && !(sgn == 1 && m == 0)) {
+        const long idx = isReal ? (long)l * (l + 1) / 2 - (long)na * (na + 1) / 2 + m
+                                : (long)l * l - (long)n * n + l + (sgn ? -m : m);
+        v = coef[(size_t)f * coefSize + idx];
+        if (sgn == 1 && ((l + n) & 1)) v = make_double2(-v.x, -v.y);
+      }
+      tile[u][i][lane] = v;
     }
-    tile[i][lane] = v;
   }
   __syncthreads();
 #pragma unroll
-  for (int jj = warp; jj < 32; jj += 8) {
-    const int m = mt + jj;
-    if (m > lmax) break;
-    const int l0 = m > na ? m : na;
-    const int kp = (lmax - l0 + 1 + kBKInv - 1) / kBKInv * kBKInv;
-    const int k = lt + lane - l0;
-    if (k < 0 || k >= kp) continue;
-    const double2 v = tile[lane][jj];
-    const size_t r0 = ((size_t)m * R + 2 * q) * pitch + k;
-    __nv_bfloat16 h, md, lo;
-    split3(v.x, h, md, lo);
-    op[r0] = h;
-    op[plane + r0] = md;
-    op[2 * plane + r0] = lo;
-    split3(v.y, h, md, lo);
-    op[r0 + pitch] = h;
-    op[plane + r0 + pitch] = md;
-    op[2 * plane + r0 + pitch] = lo;
+  for (int u = 0; u < kQB; u++) {
+    const int q = qBase + u;
+    if (q >= Q) break;
+#pragma unroll
+    for (int jj = warp; jj < 32; jj += 8) {
+      const int m = mt + jj;
+      if (m > lmax) break;
+      const int l0 = m > na ? m : na;
+      const int kp = (lmax - l0 + 1 + kBKInv - 1) / kBKInv * kBKInv;
+      const int k = lt + lane - l0;
+      if (k < 0 || k >= kp) continue;
+      const double2 v = tile[u][lane][jj];
+      const size_t r0 = ((size_t)m * R + 2 * q) * pitch + k;
+      __nv_bfloat16 h, md, lo;
+      split3(v.x, h, md, lo);
+      op[r0] = h;
+      op[plane + r0] = md;
+      op[2 * plane + r0] = lo;
+      split3(v.y, h, md, lo);
+      op[r0 + pitch] = h;
+      op[plane + r0 + pitch] = md;
+      op[2 * plane + r0 + pitch] = lo;
+    }
   }
 }
 
@@ -832,10 +852,24 @@ gsht_status launch_bf16_n(const gsht_grid* g, const TcArgs& a, const CUtensorMap
   const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kN, kBK, &st);
   if (!tl) return st;
   constexpr int kSt = stages_for(kBK);
-  auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kN, kSt, kBK>;
   const size_t sm = tc_smem_bytes<kNsplit, kNsplit, kN, kBK, kSt>();
-  GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int blocks = tl->count < sms ? tl->count : sms;
+  if constexpr (kN == 128) {
+    if (g_tc_trace) {
+      // Traced copy (same results) of the 128-row tile kernel.
+      TcArgs b = a;
+      b.trace = trace_slots(0, kDir, s);
+      if (!b.trace) return fail(GSHT_ERR_CUDA, "trace counters unavailable");
+      auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kN, kSt, kBK, true>;
+      GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      kern<<<blocks, kThreads, sm, s>>>(mapA, mapB, b, tl->d_tiles, tl->count);
+      GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_tc<inverse,bf16x3,traced>"
+                                  : "k_legendre_tc<forward,bf16x3,traced>");
+      return GSHT_OK;
+    }
+  }
+  auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kN, kSt, kBK, false>;
+  GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   kern<<<blocks, kThreads, sm, s>>>(mapA, mapB, a, tl->d_tiles, tl->count);
   GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_tc<inverse,bf16x3>" : "k_legendre_tc<forward,bf16x3>");
   return GSHT_OK;
@@ -888,7 +922,12 @@ gsht_status launch_bf16_pair(const gsht_grid* g, const TcArgs& a, const CUtensor
   const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kPairM, kBK, &st);
   if (!tl) return st;
   constexpr int kSt = kBK == 32 ? 5 : 3;
-  auto kern = k_legendre_tc2<kDir, kSt, kBK>;
+  TcArgs b = a;
+  if (g_tc_trace) {
+    b.trace = trace_slots(0, kDir, s);
+    if (!b.trace) return fail(GSHT_ERR_CUDA, "trace counters unavailable");
+  }
+  auto kern = g_tc_trace ? k_legendre_tc2<kDir, kSt, kBK, true> : k_legendre_tc2<kDir, kSt, kBK, false>;
   const size_t sm = tc2_smem_bytes<kSt, kBK>();
   GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   cudaLaunchAttribute attr[1];
@@ -912,7 +951,7 @@ gsht_status launch_bf16_pair(const gsht_grid* g, const TcArgs& a, const CUtensor
   }
   const int pairs = tl->count < clusters ? tl->count : clusters;
   cfg.gridDim = dim3(2 * pairs);
-  GSHT_CUDA(cudaLaunchKernelEx(&cfg, kern, mapT, mapF, a, (const int4*)tl->d_tiles, tl->count));
+  GSHT_CUDA(cudaLaunchKernelEx(&cfg, kern, mapT, mapF, b, (const int4*)tl->d_tiles, tl->count));
   GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_tc2<inverse,bf16x3>" : "k_legendre_tc2<forward,bf16x3>");
   return GSHT_OK;
 }
@@ -975,8 +1014,9 @@ gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, 
     // Degrees up to l0 + kp - 1 <= lmax + kBKInv - 1: the zero padding of
     // every order's row up to its K-step multiple is written too.
     const int nA = (lmax + kBKInv + 31) / 32, nB = (lmax + 32) / 32;
-    dim3 pg(nB * nA - nB * (nB - 1) / 2, 1, Q);
-    k_prep_inverse_bf16<<<pg, 256, 0, s>>>(lmax, t->n, na, count, Q, R, is_real,
+    constexpr int kQB = 2;  // field rows per block
+    dim3 pg(nB * nA - nB * (nB - 1) / 2, 1, (Q + kQB - 1) / kQB);
+    k_prep_inverse_bf16<kQB><<<pg, 256, 0, s>>>(lmax, t->n, na, count, Q, R, is_real,
                                            coef_size(lmax, t->n, is_real), pitch, plane, nA,
                                            reinterpret_cast<const double2*>(coef), op);
     GSHT_LAUNCH_CHECK("k_prep_inverse_bf16");

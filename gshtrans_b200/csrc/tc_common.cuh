@@ -85,6 +85,12 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
+// Orders this thread's earlier generic-proxy shared-memory accesses before
+// its later async-proxy (TMA) ones.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
 __device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {
   asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
@@ -282,6 +288,61 @@ inline EncodeTiledFn encode_fn() {
       cudaGetLastError();
   }
   return fn;
+}
+
+// ---------------------------------------------------------------------------
+// Per-role cycle trace of the tensor-core pipelines (a diagnostic; the
+// traced kernels are separate instantiations, so the untraced ones carry no
+// trace code). Slots, summed over CTAs with atomics at the end of a launch:
+// ---------------------------------------------------------------------------
+enum TraceSlot {
+  kTrProducer = 0,      // TMA producer thread: cycles from kernel start to its end
+  kTrProducerWait = 1,  //   of which waiting for a free stage
+  kTrMma = 2,           // MMA issuing thread: cycles from kernel start to its end
+  kTrMmaWaitFull = 3,   //   of which waiting for a loaded stage
+  kTrMmaWaitAcc = 4,    //   of which waiting for the epilogue to free TMEM
+  kTrEpilogue = 5,      // epilogue warps (summed over warps)
+  kTrEpilogueWait = 6,  //   of which waiting for finished accumulators
+  kTrCtas = 7,          // CTAs that ran
+  kTrMmaCtas = 8,       // CTAs whose thread issued MMAs
+  kTrSlots = 9
+};
+
+// mbar_wait that adds its cycles to `acc` when kOn.
+template <bool kOn>
+__device__ __forceinline__ bool timed_wait(long long& acc, uint64_t* bar, uint32_t parity,
+                                           int* err, int code) {
+  if constexpr (kOn) {
+    const long long t0 = clock64();
+    const bool r = mbar_wait(bar, parity, err, code);
+    acc += clock64() - t0;
+    return r;
+  } else {
+    return mbar_wait(bar, parity, err, code);
+  }
+}
+
+// Called by lane 0 of every warp at the end of a traced launch: warp 0 is
+// the producer, warp 1 the MMA issuer (when `issues`), warps 2.. the
+// epilogue; w1 / w2 are the role's waits in slot order.
+__device__ __forceinline__ void trace_role(unsigned long long* slots, int warp, bool issues,
+                                           long long start, long long w1, long long w2) {
+  const unsigned long long total = (unsigned long long)(clock64() - start);
+  if (warp == 0) {
+    atomicAdd(&slots[kTrProducer], total);
+    atomicAdd(&slots[kTrProducerWait], (unsigned long long)w1);
+    atomicAdd(&slots[kTrCtas], 1ull);
+  } else if (warp == 1) {
+    if (issues) {
+      atomicAdd(&slots[kTrMma], total);
+      atomicAdd(&slots[kTrMmaWaitFull], (unsigned long long)w1);
+      atomicAdd(&slots[kTrMmaWaitAcc], (unsigned long long)w2);
+      atomicAdd(&slots[kTrMmaCtas], 1ull);
+    }
+  } else {
+    atomicAdd(&slots[kTrEpilogue], total);
+    atomicAdd(&slots[kTrEpilogueWait], (unsigned long long)w1);
+  }
 }
 
 }  // namespace tc

@@ -316,6 +316,27 @@ gsht_status gsht_device_status(const gsht_grid* grid);
  * handling sees device-side timeouts. Enqueued on `stream`. */
 gsht_status gsht_check_bounded_wait(const gsht_grid* grid, void* stream);
 
+/* Per-role cycle trace of the tensor-core Legendre kernels. No counterpart
+ * in the reference (it has no device code). While enabled (a process-wide
+ * switch), the Legendre stage of BF16x3 and Ozaki transforms launches traced
+ * copies of its kernels (the BF16x3 one-CTA kernel only at its 128-row tile
+ * width): same results, and every thread that waits in the pipeline times its
+ * waits with clock64. gsht_tc_trace_read synchronises the calling thread's
+ * current device and returns the counters of the last traced launch of one
+ * form (GSHT_BF16X3, or GSHT_OZAKI / GSHT_OZAKI4, which share them) and
+ * direction (0 inverse, 1 forward) as GSHT_TRACE_SLOTS doubles, in SM clock
+ * cycles summed over the CTAs (the epilogue slots also over its warps):
+ *   [0] producer thread, kernel start to its end  [1] of which waiting for a
+ *   free stage  [2] MMA issuing thread, start to end  [3] of which waiting for
+ *   a loaded stage  [4] of which waiting for the epilogue to free the
+ *   accumulators  [5] epilogue warps, start to end  [6] of which waiting for
+ *   finished accumulators  [7] CTAs  [8] CTAs that issued MMAs (in the
+ *   CTA-pair kernels only the first CTA of a pair issues).
+ * A diagnostic: the traced kernels add a few instructions per wait. */
+#define GSHT_TRACE_SLOTS 9
+gsht_status gsht_tc_trace_enable(int on);
+gsht_status gsht_tc_trace_read(int form, int direction, double* out, int n);
+
 /* Device-memory allocator hook. No counterpart in the reference (its tables
  * live in host std::vector storage, Wigner.h:126-128). Every device
  * allocation of the library (grid tables and nodes, workspaces, batch plans,

@@ -127,3 +127,12 @@ def test_stage_profile_without_calls():
         pass
     assert tuple(p.stages) == g.STAGES
     assert all(v == (0.0, 0) for v in p.stages.values())
+
+
+def test_trace_read_rejects_bad_arguments_without_a_device():
+    import gshtrans_b200 as gsht
+
+    with pytest.raises(gsht.BadArgument):
+        gsht.TensorCoreTrace.read("fp64", 0)
+    with pytest.raises(gsht.BadArgument):
+        gsht.TensorCoreTrace.read("bf16x3", 2)
