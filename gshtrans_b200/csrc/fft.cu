@@ -1217,10 +1217,12 @@ inline unsigned ring_blocks(RingRange rr, int R) {
   return (unsigned)((rr.jEnd + R - 1) / R - rr.jBegin / R);
 }
 
-// Butterflies of the inverse with FP32 spectra: FP64 by default (measured at
-// lmax 1024, 64 fields: 0.91 ms against 1.08 ms for FP32 butterflies, whose
-// FFT buffer lets three blocks share an SM); GSHT_FFT_INV_FP32=1 selects the
-// FP32 ones for comparisons.
+// Butterflies of the inverse with FP32 spectra: FP64 by default. Measured at
+// lmax 1024, 64 fields: 0.93 ms; FP32 butterflies 1.07 ms at the three blocks
+// per SM their smaller FFT buffer allows (0.88 ms when held to two; faster
+// at 16 fields, 0.18 against 0.22 ms), for a larger error against the FP64
+// path (8.3e-7 against 8.1e-7). GSHT_FFT_INV_FP32=1 selects the FP32 ones
+// for comparisons.
 bool fp32_inverse_butterflies() {
   const char* e = getenv("GSHT_FFT_INV_FP32");
   return e && e[0] == '1';

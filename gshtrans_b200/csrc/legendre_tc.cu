@@ -667,15 +667,19 @@ __device__ __forceinline__ void split3(float x, __nv_bfloat16& h, __nv_bfloat16&
 // < Kp_m (zero beyond lmax). One block per 32 degrees x 32 orders of kQB
 // field rows q: the packed layout is contiguous along orders for a fixed
 // degree, so each tile is read order-major (coalesced), transposed in shared
-// memory and written degree-major (each order's operand row segment).
-// blockIdx.x walks the triangle of (degree tile a, order tile b <= a) pairs
-// row by row (row b holds nA - b tiles), so no block is launched for the
-// empty upper half.
+// memory and written degree-major, two degrees per lane as BF16 pairs. A
+// pair starts at an even k; so that every k is written exactly once the tile
+// holds degrees lt-1 .. lt+31 and order m writes k in [kb, kb + 32), kb =
+// lt - l0 rounded down to even (consecutive degree tiles of one order then
+// cover consecutive k ranges). blockIdx.x walks the triangle of (degree tile
+// a, order tile b <= a) pairs row by row (row b holds nA - b tiles), so no
+// block is launched for the empty upper half.
 template <int kQB>
 __global__ void __launch_bounds__(256) k_prep_inverse_bf16(
     int lmax, int n, int na, int count, int Q, int R, int isReal, long coefSize, int pitch,
     size_t plane, int nA, const double2* __restrict__ coef, __nv_bfloat16* __restrict__ op) {
-  __shared__ double2 tile[kQB][32][33];
+  constexpr int kRows = 33;  // degrees lt-1 .. lt+31
+  __shared__ double2 tile[kQB][kRows][33];
   int i0 = blockIdx.x, b = 0;
   while (i0 >= nA - b) {
     i0 -= nA - b;
@@ -690,10 +694,10 @@ __global__ void __launch_bounds__(256) k_prep_inverse_bf16(
     const int q = qBase + u;
     const int sgn = q / count, f = q - sgn * count;
 #pragma unroll
-    for (int i = warp; i < 32; i += 8) {
-      const int l = lt + i, m = mt + lane;
+    for (int i = warp; i < kRows; i += 8) {
+      const int l = lt - 1 + i, m = mt + lane;
       double2 v = make_double2(0.0, 0.0);
-      if (q < Q && l <= lmax && m <= l && l >= na && !(sgn == 1 && m == 0)) {
+      if (q < Q && l >= 0 && l <= lmax && m <= l && l >= na && !(sgn == 1 && m == 0)) {
         const long idx = isReal ? (long)l * (l + 1) / 2 - (long)na * (na + 1) / 2 + m
                                 : (long)l * l - (long)n * n + l + (sgn ? -m : m);
         v = coef[(size_t)f * coefSize + idx];
@@ -703,29 +707,37 @@ __global__ void __launch_bounds__(256) k_prep_inverse_bf16(
     }
   }
   __syncthreads();
+  // Half-warp h of warp w writes order jj = 2 (w + 8 it) + h; lane p of the
+  // half-warp the pair k = kb + 2p, kb + 2p + 1.
+  const int h = lane >> 4, pr = lane & 15;
 #pragma unroll
   for (int u = 0; u < kQB; u++) {
     const int q = qBase + u;
     if (q >= Q) break;
 #pragma unroll
-    for (int jj = warp; jj < 32; jj += 8) {
+    for (int it = 0; it < 2; it++) {
+      const int jj = 2 * (warp + 8 * it) + h;
       const int m = mt + jj;
-      if (m > lmax) break;
+      if (m > lmax) continue;
       const int l0 = m > na ? m : na;
       const int kp = (lmax - l0 + 1 + kBKInv - 1) / kBKInv * kBKInv;
-      const int k = lt + lane - l0;
+      const int d = lt - l0;
+      const int k = d - (d & 1) + 2 * pr;
       if (k < 0 || k >= kp) continue;
-      const double2 v = tile[u][lane][jj];
+      const int i = k + l0 - (lt - 1);  // tile row of degree l0 + k
+      const double2 v0 = tile[u][i][jj], v1 = tile[u][i + 1][jj];
       const size_t r0 = ((size_t)m * R + 2 * q) * pitch + k;
-      __nv_bfloat16 h, md, lo;
-      split3(v.x, h, md, lo);
-      op[r0] = h;
-      op[plane + r0] = md;
-      op[2 * plane + r0] = lo;
-      split3(v.y, h, md, lo);
-      op[r0 + pitch] = h;
-      op[plane + r0 + pitch] = md;
-      op[2 * plane + r0 + pitch] = lo;
+      __nv_bfloat162 hh, mm, ll;
+      split3(v0.x, hh.x, mm.x, ll.x);
+      split3(v1.x, hh.y, mm.y, ll.y);
+      *reinterpret_cast<__nv_bfloat162*>(op + r0) = hh;
+      *reinterpret_cast<__nv_bfloat162*>(op + plane + r0) = mm;
+      *reinterpret_cast<__nv_bfloat162*>(op + 2 * plane + r0) = ll;
+      split3(v0.y, hh.x, mm.x, ll.x);
+      split3(v1.y, hh.y, mm.y, ll.y);
+      *reinterpret_cast<__nv_bfloat162*>(op + r0 + pitch) = hh;
+      *reinterpret_cast<__nv_bfloat162*>(op + plane + r0 + pitch) = mm;
+      *reinterpret_cast<__nv_bfloat162*>(op + 2 * plane + r0 + pitch) = ll;
     }
   }
 }
