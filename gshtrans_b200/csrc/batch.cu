@@ -21,7 +21,14 @@
 //     groups are spread over (largest groups first), by timing the captured
 //     round-trip graph of each candidate;
 //   - captures the whole sequence (gathers, transforms, scatters) for each
-//     direction into a CUDA graph, so an execution is one graph launch.
+//     direction into a CUDA graph, so an execution is one graph launch;
+//   - for the BF16x3 form, runs each direction's Legendre stage as ONE
+//     persistent tensor-core launch over the (group, order, tile) work list
+//     of all groups (every group's tensor maps and arguments in device
+//     memory), between the per-group operand preparations / ring FFTs, which
+//     run concurrently on the plan's streams; the field-row tile width of
+//     that launch is autotuned (GSHT_BATCH_FUSED=0 keeps one transform per
+//     group, for comparisons).
 #include <algorithm>
 #include <map>
 #include <string>
@@ -75,6 +82,9 @@ struct Group {
   double2** coefOutPtrs = nullptr;
   void* ws = nullptr;                 // private workspace of the group's transforms
   size_t wsBytes = 0;
+  double* spec = nullptr;             // fused BF16x3 path: spectra / forward result rows
+  void* op = nullptr;                 //   and the operand rows of either direction
+  bool spec32 = false;                //   FP32 spectra (three-pass ring FFTs)
   double work = 0.0;                  // estimated cost (fields x lmax^3), for the schedule
 };
 
@@ -90,6 +100,9 @@ struct gsht_batch {
   std::vector<cudaStream_t> lanes;     // streams the groups are spread over
   std::vector<cudaEvent_t> laneDone;   // join events (one per lane) and the fork event
   int nlanes = 1;                      // chosen by the schedule autotuner
+  bool fused = false;                  // one Legendre launch over all groups (BF16x3)
+  gsht::Bf16Multi multi[2];            // its work lists: [0] inverse, [1] forward
+  int fusedTile = 64;                  // its field-row tile width (autotuned)
   cudaGraph_t graph[3] = {nullptr, nullptr, nullptr};
   cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
   size_t nodes[3] = {0, 0, 0};
@@ -155,7 +168,10 @@ gsht_status run_one(gsht_batch* b, Group& gr, int mode, cudaStream_t s, bool use
 // then forward, the grids of the round trip also written back), with the
 // groups (ordered largest first) dealt round-robin over `lanes` streams
 // forked from and joined back into s.
+gsht_status run_all_fused(gsht_batch* b, int mode, cudaStream_t s, int lanes, bool userIO);
+
 gsht_status run_all(gsht_batch* b, int mode, cudaStream_t s, int lanes, bool userIO = true) {
+  if (b->fused) return run_all_fused(b, mode, s, lanes, userIO);
   gsht_status st;
   if (lanes <= 1) {
     for (auto& gr : b->groups)
@@ -176,6 +192,127 @@ gsht_status run_all(gsht_batch* b, int mode, cudaStream_t s, int lanes, bool use
   return GSHT_OK;
 }
 
+// The fused BF16x3 execution of `mode` (as run_all): per direction, the
+// groups' gathers and operand preparations (and forward ring FFTs) spread
+// over the lanes, one multi-group Legendre launch on s, then the groups'
+// inverse ring FFTs or forward accumulations and scatters over the lanes.
+gsht_status run_all_fused(gsht_batch* b, int mode, cudaStream_t s, int lanes, bool userIO) {
+  gsht_status st = GSHT_OK;
+  const int L = lanes < 1 ? 1 : lanes;
+  auto lane = [&](size_t gi) { return L == 1 ? s : b->lanes[gi % L]; };
+  auto fork = [&]() -> gsht_status {
+    if (L == 1) return GSHT_OK;
+    GSHT_CUDA(cudaEventRecord(b->laneDone[0], s));
+    for (int i = 0; i < L; i++) GSHT_CUDA(cudaStreamWaitEvent(b->lanes[i], b->laneDone[0], 0));
+    return GSHT_OK;
+  };
+  auto join = [&]() -> gsht_status {
+    if (L == 1) return GSHT_OK;
+    for (int i = 0; i < L; i++) {
+      GSHT_CUDA(cudaEventRecord(b->laneDone[1 + i], b->lanes[i]));
+      GSHT_CUDA(cudaStreamWaitEvent(s, b->laneDone[1 + i], 0));
+    }
+    return GSHT_OK;
+  };
+  auto inverse = [&](bool gather, bool scatter) -> gsht_status {
+    gsht_status r;
+    if ((r = fork()) != GSHT_OK) return r;
+    for (size_t gi = 0; gi < b->groups.size(); gi++) {
+      Group& gr = b->groups[gi];
+      const int k = (int)gr.fields.size();
+      if (gather && (r = copy_group(gr, 0, gr.coefElems, gr.coefInPtrs, gr.coefIn, lane(gi))) != GSHT_OK)
+        return r;
+      r = bf16_prep_inverse(gr.grid, gr.grid->table(gr.n), gr.lmax, gr.isReal, k,
+                            reinterpret_cast<const double*>(gr.coefIn), gr.op, lane(gi));
+      if (r != GSHT_OK) return r;
+    }
+    if ((r = join()) != GSHT_OK) return r;
+    if ((r = bf16_multi_launch(b->multi[0], s)) != GSHT_OK) return r;
+    if ((r = fork()) != GSHT_OK) return r;
+    for (size_t gi = 0; gi < b->groups.size(); gi++) {
+      Group& gr = b->groups[gi];
+      const int k = (int)gr.fields.size();
+      {
+        StageTimer tm(GSHT_STAGE_FFT_INVERSE, lane(gi));
+        double* out = reinterpret_cast<double*>(gr.gridBuf);
+        r = gr.spec32 ? fft_inverse32(gr.grid, gr.lmax, gr.isReal, k,
+                                      reinterpret_cast<const float*>(gr.spec), out, lane(gi))
+                      : fft_inverse(gr.grid, gr.lmax, gr.isReal, k, gr.spec, out, lane(gi));
+      }
+      if (r != GSHT_OK) return r;
+      if (scatter && (r = copy_group(gr, 1, gr.gridElems, gr.gridPtrs, gr.gridBuf, lane(gi))) != GSHT_OK)
+        return r;
+    }
+    return join();
+  };
+  auto forward = [&](bool gather, bool scatter) -> gsht_status {
+    gsht_status r;
+    if ((r = fork()) != GSHT_OK) return r;
+    for (size_t gi = 0; gi < b->groups.size(); gi++) {
+      Group& gr = b->groups[gi];
+      const int k = (int)gr.fields.size();
+      if (gather && (r = copy_group(gr, 0, gr.gridElems, gr.gridPtrs, gr.gridBuf, lane(gi))) != GSHT_OK)
+        return r;
+      {
+        StageTimer tm(GSHT_STAGE_FFT_FORWARD, lane(gi));
+        const double* in = reinterpret_cast<const double*>(gr.gridBuf);
+        r = gr.spec32 ? fft_forward32(gr.grid, gr.lmax, gr.isReal, k, in,
+                                      reinterpret_cast<float*>(gr.spec), lane(gi))
+                      : fft_forward(gr.grid, gr.lmax, gr.isReal, k, in, gr.spec, lane(gi));
+      }
+      if (r != GSHT_OK) return r;
+      r = bf16_prep_forward(gr.grid, gr.lmax, gr.isReal, k, gr.spec, gr.op, lane(gi), gr.spec32);
+      if (r != GSHT_OK) return r;
+    }
+    if ((r = join()) != GSHT_OK) return r;
+    if ((r = bf16_multi_launch(b->multi[1], s)) != GSHT_OK) return r;
+    if ((r = fork()) != GSHT_OK) return r;
+    for (size_t gi = 0; gi < b->groups.size(); gi++) {
+      Group& gr = b->groups[gi];
+      const int k = (int)gr.fields.size();
+      const int na = gr.n < 0 ? -gr.n : gr.n;
+      GSHT_CUDA(cudaMemsetAsync(gr.coefOut, 0, sizeof(double2) * gr.coefElems * k, lane(gi)));
+      r = accumulate_forward(gr.grid->L, gr.lmax, gr.n, na, k, (gr.isReal ? 1 : 2) * k, gr.isReal,
+                             gr.coefElems, gr.grid->theta_pad, gr.spec,
+                             reinterpret_cast<double*>(gr.coefOut), lane(gi), true);
+      if (r != GSHT_OK) return r;
+      // Every field's lmax is its grid's degree, so complex fields get c_{L,L} = 0.
+      const int cm = gr.isReal ? 2 : 3;
+      if (scatter && (r = copy_group(gr, cm, gr.coefElems, gr.coefOutPtrs, gr.coefOut, lane(gi))) != GSHT_OK)
+        return r;
+    }
+    return join();
+  };
+  if (mode == 1 || mode == 2) st = inverse(userIO, userIO);
+  if (st == GSHT_OK && mode == 0) st = forward(userIO, userIO);
+  if (st == GSHT_OK && mode == 2) st = forward(false, userIO);
+  return st;
+}
+
+// Buffers of the fused path and its two work lists at tile width `tile`.
+gsht_status fused_build(gsht_batch* b, int tile) {
+  for (auto& mp : b->multi) bf16_multi_free(&mp);
+  std::vector<Bf16MultiGroup> gs;
+  for (auto& gr : b->groups) {
+    Bf16MultiGroup q;
+    q.g = gr.grid;
+    q.t = gr.grid->table(gr.n);
+    q.lmax = gr.lmax;
+    q.isReal = gr.isReal;
+    q.count = (int)gr.fields.size();
+    q.operand = gr.op;
+    q.spec = gr.spec;
+    q.spec32 = gr.spec32;
+    gs.push_back(q);
+  }
+  for (int dir = 0; dir < 2; dir++) {
+    gsht_status st = bf16_multi_build(dir, gs.data(), (int)gs.size(), tile, &b->multi[dir]);
+    if (st != GSHT_OK) return st;
+  }
+  b->fusedTile = tile;
+  return GSHT_OK;
+}
+
 void free_batch(gsht_batch* b) {
   if (!b) return;
   cudaSetDevice(b->device);
@@ -192,7 +329,10 @@ void free_batch(gsht_batch* b) {
     dev_free(gr.gridPtrs);
     dev_free(gr.coefOutPtrs);
     dev_free(gr.ws);
+    dev_free(gr.spec);
+    dev_free(gr.op);
   }
+  for (auto& mp : b->multi) bf16_multi_free(&mp);
   for (auto& kv : b->grids) gsht_grid_destroy(kv.second);
   for (cudaStream_t l : b->lanes) cudaStreamDestroy(l);
   for (cudaEvent_t e : b->laneDone) cudaEventDestroy(e);
@@ -297,9 +437,24 @@ gsht_status plan(const gsht_field_desc* fields, int count, int precision, int au
   // transforms start early and the small ones fill in behind them.
   std::stable_sort(b->groups.begin(), b->groups.end(),
                    [](const Group& x, const Group& y) { return x.work > y.work; });
+  const char* fusedEnv = getenv("GSHT_BATCH_FUSED");
+  b->fused = precision == GSHT_BF16X3 && !(fusedEnv && fusedEnv[0] == '0');
+  if (b->fused) {
+    for (auto& gr : b->groups) {
+      const int k = (int)gr.fields.size();
+      const size_t specBytes = sizeof(double) * 2 * spec_elems(gr.grid, gr.lmax, gr.isReal, k);
+      const size_t opBytes = std::max(bf16_operand_bytes(gr.grid, gr.lmax, gr.isReal, k, 0),
+                                      bf16_operand_bytes(gr.grid, gr.lmax, gr.isReal, k, 1));
+      GSHT_CUDA(dev_malloc(&gr.spec, specBytes));
+      GSHT_CUDA(dev_malloc_bytes(&gr.op, opBytes));
+      gr.spec32 = fft_spec32_supported(gr.grid, gr.isReal);
+    }
+  }
   // Warm-up (sizes every workspace, builds tile lists and layouts), then
-  // the autotuner: per group, the fastest BF16x3 tile width.
+  // the autotuner: per group, the fastest BF16x3 tile width (the fused path
+  // tunes the tile width of its one launch further below).
   for (auto& gr : b->groups) {
+    if (b->fused) break;
     gsht_status st = run_group(b, gr, 1, false, false, b->stream);
     if (st == GSHT_OK) st = run_group(b, gr, 0, false, false, b->stream);
     if (st != GSHT_OK) return st;
@@ -351,35 +506,72 @@ gsht_status plan(const gsht_field_desc* fields, int count, int precision, int au
     if (e != cudaSuccess) return cuda_fail(e, "batch graph capture");
     return GSHT_OK;
   };
+  // Time of the round-trip graph with `lanes` streams (callers' buffers
+  // untouched), over three launches after one.
+  auto time_graph = [&](int lanes, float* ms) -> gsht_status {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    gsht_status st = capture(2, lanes, &graph, false);
+    if (st != GSHT_OK) return st;
+    if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      return cuda_fail(cudaGetLastError(), "batch graph instantiation");
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaGraphLaunch(exec, b->stream);
+    cudaEventRecord(e0, b->stream);
+    for (int r = 0; r < 3; r++) cudaGraphLaunch(exec, b->stream);
+    cudaEventRecord(e1, b->stream);
+    const cudaError_t se = cudaEventSynchronize(e1);
+    *ms = 0.f;
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (se != cudaSuccess) return cuda_fail(se, "batch schedule tuning");
+    return GSHT_OK;
+  };
+  // Fused path: the tile width of the one Legendre launch per direction
+  // (each candidate warmed up uncaptured, then timed as a graph).
+  if (b->fused) {
+    const int guessLanes = std::min(maxLanes, 8);
+    int bestTile = 64;
+    float best = 3.4e38f;
+    for (int tile : {32, 64, 128}) {
+      if (!autotune && tile != 64) continue;
+      gsht_status st = fused_build(b, tile);
+      if (st == GSHT_OK) st = run_all_fused(b, 2, b->stream, 1, false);
+      if (st != GSHT_OK) return st;
+      GSHT_CUDA(cudaStreamSynchronize(b->stream));
+      if (!autotune) break;
+      float ms = 0.f;
+      if ((st = time_graph(guessLanes, &ms)) != GSHT_OK) return st;
+      if (ms < best) {
+        best = ms;
+        bestTile = tile;
+      }
+    }
+    if (b->fusedTile != bestTile) {
+      gsht_status st = fused_build(b, bestTile);
+      if (st != GSHT_OK) return st;
+    }
+    for (auto& gr : b->groups) gr.ntile = b->fusedTile;
+    for (auto& kv : b->grids) {
+      gsht_status st = gsht_device_status(kv.second);
+      if (st != GSHT_OK) return st;
+    }
+  }
   b->nlanes = 1;
   if (maxLanes > 1 && autotune) {
     float best = 3.4e38f;
     for (int lanes : {1, 2, 4, 8, 16}) {
       if (lanes > maxLanes) break;
-      cudaGraph_t graph = nullptr;
-      cudaGraphExec_t exec = nullptr;
-      // Timed without the callers' buffers (no gathers or scatters).
-      gsht_status st = capture(2, lanes, &graph, false);
-      if (st != GSHT_OK) return st;
-      if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
-        cudaGraphDestroy(graph);
-        return cuda_fail(cudaGetLastError(), "batch graph instantiation");
-      }
-      cudaEvent_t e0, e1;
-      cudaEventCreate(&e0);
-      cudaEventCreate(&e1);
-      cudaGraphLaunch(exec, b->stream);
-      cudaEventRecord(e0, b->stream);
-      for (int r = 0; r < 3; r++) cudaGraphLaunch(exec, b->stream);
-      cudaEventRecord(e1, b->stream);
-      const cudaError_t se = cudaEventSynchronize(e1);
       float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
-      cudaGraphExecDestroy(exec);
-      cudaGraphDestroy(graph);
-      if (se != cudaSuccess) return cuda_fail(se, "batch schedule tuning");
+      gsht_status st = time_graph(lanes, &ms);
+      if (st != GSHT_OK) return st;
       if (ms < best) {
         best = ms;
         b->nlanes = lanes;

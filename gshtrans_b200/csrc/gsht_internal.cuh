@@ -255,6 +255,33 @@ gsht_status legendre_inverse_fp64_layout(const gsht_grid* g, const Table* t, int
                                          const long long* dOff, const int* dPitch, int kpMax,
                                          double* operand, double* spec, cudaStream_t s);
 
+// BF16x3 stages for batch plans (legendre_tc.cu): the operand preparation of
+// each direction on its own, and one persistent Legendre launch over the
+// tiles of several groups (each with its grid, table, operand rows and
+// spectra; every group's tensor maps and arguments in device memory).
+gsht_status bf16_prep_inverse(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                              int count, const double* coef, void* operand, cudaStream_t s);
+gsht_status bf16_prep_forward(const gsht_grid* g, int lmax, int is_real, int count,
+                              const double* spec, void* operand, cudaStream_t s, bool spec32);
+struct Bf16MultiGroup {
+  const gsht_grid* g = nullptr;
+  const Table* t = nullptr;
+  int lmax = 0, isReal = 0, count = 0;
+  void* operand = nullptr;   // prepared operand rows of the direction
+  double* spec = nullptr;    // spectra (inverse output) / result rows (forward output)
+  bool spec32 = false;       // inverse: FP32 spectra
+};
+struct Bf16Multi {
+  void* d_groups = nullptr;  // per-group tensor maps and arguments
+  void* d_tiles = nullptr;   // tiles (group << 16 | m, M tile, N tile, K blocks)
+  int numTiles = 0, dir = 0, ntile = 0, bk = 0, device = 0;
+  int* err = nullptr;        // device error word the launch reports through
+};
+gsht_status bf16_multi_build(int dir, const Bf16MultiGroup* groups, int ngroups, int ntile,
+                             Bf16Multi* out);
+gsht_status bf16_multi_launch(const Bf16Multi& multi, cudaStream_t s);
+void bf16_multi_free(Bf16Multi* multi);
+
 // Legendre stage, BF16x3 on tcgen05 (legendre_tc.cu). dir 0 = forward
 // (operand rows over colatitudes), 1 = inverse (rows over degrees).
 size_t bf16_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, int dir);

@@ -52,6 +52,15 @@ struct TcArgs {
   unsigned long long* trace;  // kTrSlots counters of a traced launch
 };
 
+// One group of a multi-group launch (batch plans): its tensor maps live in
+// global memory beside its arguments (64-byte aligned, as TMA requires).
+struct alignas(64) TcGroup {
+  CUtensorMap mapA, mapB;
+  TcArgs a;
+};
+// Tile x of a multi-group launch: group << 16 | m.
+constexpr int kGroupShift = 16;
+
 // TMEM accumulators per tile: products of very different magnitude would
 // otherwise share one FP32 accumulator whose every update truncates; hi.hi
 // goes to up to kBigAcc accumulators by K block and the other five products to
@@ -76,11 +85,17 @@ constexpr int kThreads = 32 * (2 + kEpiWarps);
 // The producer runs ahead across tile boundaries; the epilogue copies its
 // accumulator columns out of TMEM, releases TMEM to the MMA warp (accEmpty),
 // and only then writes results, so stores overlap the next tile's MMAs.
-template <int kDir, int kNA, int kNB, int kNP, int kN, int kStages, int kBK, bool kTrace>
+//
+// kMulti: the tiles belong to several groups (the batch plans' single
+// launch over all groups of a direction): tile x = group << 16 | m, and each
+// tile takes its arguments and tensor maps from groups[group].
+template <int kDir, int kNA, int kNB, int kNP, int kN, int kStages, int kBK, bool kTrace,
+          bool kMulti>
 __global__ void __launch_bounds__(kThreads, 1)
     k_legendre_tc(const __grid_constant__ CUtensorMap mapA,
                   const __grid_constant__ CUtensorMap mapB, TcArgs p,
-                  const int4* __restrict__ tiles, int numTiles) {
+                  const int4* __restrict__ tiles, int numTiles,
+                  const TcGroup* __restrict__ groups) {
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
@@ -115,10 +130,18 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_init(accEmptyA, kEpiWarps);
     mbar_init(accEmptyB, kEpiWarps);
     fence_barrier_init();
-    prefetch_tmap(&mapA);
-    prefetch_tmap(&mapB);
+    if constexpr (!kMulti) {
+      prefetch_tmap(&mapA);
+      prefetch_tmap(&mapB);
+    }
   }
   if (warp == 1) tmem_alloc(tmemSlot, kAccumulators * kN);
+  // The arguments of tile tl (its group's in a multi-group launch) and its order.
+  auto args = [&](const int4& tl) -> const TcArgs& {
+    if constexpr (kMulti) return groups[tl.x >> kGroupShift].a;
+    else return p;
+  };
+  auto order = [](const int4& tl) { return kMulti ? (tl.x & ((1 << kGroupShift) - 1)) : tl.x; };
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -130,8 +153,16 @@ __global__ void __launch_bounds__(kThreads, 1)
       bool ok = true;
       for (int t = blockIdx.x; t < numTiles && ok; t += gridDim.x) {
         const int4 tl = tiles[t];  // (m, mtile, ntile, nk)
-        const long long tRow = p.rowOff[tl.x];
-        const int bRow = tl.x * p.R + tl.z * kN;
+        const TcArgs& ta = args(tl);
+        const int m = order(tl);
+        const CUtensorMap* mA = &mapA;
+        const CUtensorMap* mB = &mapB;
+        if constexpr (kMulti) {
+          mA = &groups[tl.x >> kGroupShift].mapA;
+          mB = &groups[tl.x >> kGroupShift].mapB;
+        }
+        const long long tRow = ta.rowOff[m];
+        const int bRow = m * ta.R + tl.z * kN;
         for (int kc = 0; kc < tl.w; kc++, it++) {
           const int s = it % kStages;
           if (it >= kStages && !timed_wait<kTrace>(trW1, &empty[s], ((it / kStages) - 1) & 1, p.err, 1)) {
@@ -144,15 +175,15 @@ __global__ void __launch_bounds__(kThreads, 1)
             unsigned char* dst = st + a * kTileA;
             if (kDir == 0) {
               // MN-major: two 64-colatitude halves of 64 degree rows each.
-              tma_load_3d(dst, &mapA, &full[s], tl.y * kBM, (int)(tRow + kc * kBK), a);
-              tma_load_3d(dst + kTileA / 2, &mapA, &full[s], tl.y * kBM + 64,
+              tma_load_3d(dst, mA, &full[s], tl.y * kBM, (int)(tRow + kc * kBK), a);
+              tma_load_3d(dst + kTileA / 2, mA, &full[s], tl.y * kBM + 64,
                           (int)(tRow + kc * kBK), a);
             } else {
-              tma_load_3d(dst, &mapA, &full[s], kc * kBK, (int)(tRow + tl.y * kBM), a);
+              tma_load_3d(dst, mA, &full[s], kc * kBK, (int)(tRow + tl.y * kBM), a);
             }
           }
           for (int b = 0; b < kNB; b++)
-            tma_load_3d(st + kNA * kTileA + b * kTileB, &mapB, &full[s], kc * kBK, bRow, b);
+            tma_load_3d(st + kNA * kTileA + b * kTileB, mB, &full[s], kc * kBK, bRow, b);
         }
       }
     }
@@ -164,9 +195,11 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int t = blockIdx.x; t < numTiles && ok; t += gridDim.x, tc++) {
         const int4 tl = tiles[t];
         const int nk = tl.w;
+        const TcArgs& ta = args(tl);
+        const int m = order(tl);
         // K steps of 16 past the last degree (inverse) or colatitude
         // (forward) multiply zero padding and are not issued.
-        const int kLim = kDir == 0 ? p.lmax - (tl.x > p.na ? tl.x : p.na) + 1 : p.nTheta;
+        const int kLim = kDir == 0 ? ta.lmax - (m > ta.na ? m : ta.na) + 1 : ta.nTheta;
         if (tc > 0 && !timed_wait<kTrace>(trW2, accEmptyA, (tc - 1) & 1, p.err, 4)) break;
         tc_fence_after();
         bool haveB = tc == 0;
@@ -238,7 +271,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     int tc = 0;
     for (int t = blockIdx.x; t < numTiles; t += gridDim.x, tc++) {
       const int4 tl = tiles[t];
-      const int m = tl.x, nk = tl.w;
+      const TcArgs& ta = args(tl);
+      const int m = order(tl), nk = tl.w;
       if (!timed_wait<kTrace>(trW1, accFull, tc & 1, p.err, 3)) break;
       tc_fence_after();
       const int nbig = nk < kBigAcc ? nk : kBigAcc;
@@ -273,40 +307,40 @@ __global__ void __launch_bounds__(kThreads, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(accEmptyB);
-      const int l0 = m > p.na ? m : p.na;
-      const int keff = p.lmax - l0 + 1;
+      const int l0 = m > ta.na ? m : ta.na;
+      const int keff = ta.lmax - l0 + 1;
       const int tileRow = tl.y * kBM + row;
-      const int rowsM = kDir == 0 ? p.nTheta : keff;
+      const int rowsM = kDir == 0 ? ta.nTheta : keff;
       if (tileRow >= rowsM) continue;
       const int q0 = (tl.z * kN + group * kCols) / 2;
       // Both directions write order-major rows [m][q][row] (row = colatitude
       // for the inverse, degree offset l - l0 for the forward); the forward's
       // rows are added into the packed coefficients by k_accumulate_forward.
-      if (kDir == 0 && p.out32) {
+      if (kDir == 0 && ta.out32) {
 #pragma unroll
         for (int i = 0; i < kCols / 2; i++) {
           const int q = q0 + i;
-          if (q >= p.Q) break;
+          if (q >= ta.Q) break;
           // Table column tileRow holds +m at colatitude tileRow and -m at
           // its mirror nTheta-1-tileRow.
-          const int col = q >= p.count ? p.nTheta - 1 - tileRow : tileRow;
-          p.out32[((size_t)m * p.Q + q) * p.thetaPad + col] =
+          const int col = q >= ta.count ? ta.nTheta - 1 - tileRow : tileRow;
+          ta.out32[((size_t)m * ta.Q + q) * ta.thetaPad + col] =
               make_float2((float)acc[2 * i], (float)acc[2 * i + 1]);
         }
-      } else if (kDir == 1 && p.out32) {
+      } else if (kDir == 1 && ta.out32) {
 #pragma unroll
         for (int i = 0; i < kCols / 2; i++) {
           const int q = q0 + i;
-          if (q < p.Q)
-            p.out32[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
+          if (q < ta.Q)
+            ta.out32[((size_t)m * ta.Q + q) * ta.thetaPad + tileRow] =
                 make_float2((float)acc[2 * i], (float)acc[2 * i + 1]);
         }
       } else {
 #pragma unroll
         for (int i = 0; i < kCols / 2; i++) {
           const int q = q0 + i;
-          if (q < p.Q)
-            p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
+          if (q < ta.Q)
+            ta.out[((size_t)m * ta.Q + q) * ta.thetaPad + tileRow] =
                 make_double2(acc[2 * i], acc[2 * i + 1]);
         }
       }
@@ -872,17 +906,17 @@ gsht_status launch_bf16_n(const gsht_grid* g, const TcArgs& a, const CUtensorMap
       TcArgs b = a;
       b.trace = trace_slots(0, kDir, s);
       if (!b.trace) return fail(GSHT_ERR_CUDA, "trace counters unavailable");
-      auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kN, kSt, kBK, true>;
+      auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kN, kSt, kBK, true, false>;
       GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      kern<<<blocks, kThreads, sm, s>>>(mapA, mapB, b, tl->d_tiles, tl->count);
+      kern<<<blocks, kThreads, sm, s>>>(mapA, mapB, b, tl->d_tiles, tl->count, nullptr);
       GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_tc<inverse,bf16x3,traced>"
                                   : "k_legendre_tc<forward,bf16x3,traced>");
       return GSHT_OK;
     }
   }
-  auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kN, kSt, kBK, false>;
+  auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kN, kSt, kBK, false, false>;
   GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  kern<<<blocks, kThreads, sm, s>>>(mapA, mapB, a, tl->d_tiles, tl->count);
+  kern<<<blocks, kThreads, sm, s>>>(mapA, mapB, a, tl->d_tiles, tl->count, nullptr);
   GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_tc<inverse,bf16x3>" : "k_legendre_tc<forward,bf16x3>");
   return GSHT_OK;
 }
@@ -1012,44 +1046,106 @@ size_t bf16_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, 
   return sizeof(__nv_bfloat16) * kNsplit * (size_t)(lmax + 1) * R * pitch;
 }
 
-gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
-                                  int count, const double* coef, void* operand, double* spec,
-                                  int ntile, cudaStream_t s, bool spec32) {
-  if (!valid_ntile(ntile)) return fail(GSHT_ERR_BAD_ARG, "BF16x3 tile width %d not in {32, 64, 128}", ntile);
+gsht_status bf16_prep_inverse(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                              int count, const double* coef, void* operand, cudaStream_t s) {
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
   const int pitch = (int)round_up(lmax + 1, kBKInv);
   const size_t plane = (size_t)(lmax + 1) * R * pitch;
+  StageTimer tm(GSHT_STAGE_PREP_INVERSE, s);
+  // Degrees up to l0 + kp - 1 <= lmax + kBKInv - 1: the zero padding of
+  // every order's row up to its K-step multiple is written too.
+  const int nA = (lmax + kBKInv + 31) / 32, nB = (lmax + 32) / 32;
+  constexpr int kQB = 2;  // field rows per block
+  dim3 pg(nB * nA - nB * (nB - 1) / 2, 1, (Q + kQB - 1) / kQB);
+  k_prep_inverse_bf16<kQB><<<pg, 256, 0, s>>>(lmax, t->n, na, count, Q, R, is_real,
+                                              coef_size(lmax, t->n, is_real), pitch, plane, nA,
+                                              reinterpret_cast<const double2*>(coef),
+                                              static_cast<__nv_bfloat16*>(operand));
+  GSHT_LAUNCH_CHECK("k_prep_inverse_bf16");
+  return GSHT_OK;
+}
+
+gsht_status bf16_prep_forward(const gsht_grid* g, int lmax, int is_real, int count,
+                              const double* spec, void* operand, cudaStream_t s, bool spec32) {
+  const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
+  const int tp = g->theta_pad;
+  const size_t plane = (size_t)(lmax + 1) * R * tp;
   auto* op = static_cast<__nv_bfloat16*>(operand);
-  {
-    StageTimer tm(GSHT_STAGE_PREP_INVERSE, s);
-    // Degrees up to l0 + kp - 1 <= lmax + kBKInv - 1: the zero padding of
-    // every order's row up to its K-step multiple is written too.
-    const int nA = (lmax + kBKInv + 31) / 32, nB = (lmax + 32) / 32;
-    constexpr int kQB = 2;  // field rows per block
-    dim3 pg(nB * nA - nB * (nB - 1) / 2, 1, (Q + kQB - 1) / kQB);
-    k_prep_inverse_bf16<kQB><<<pg, 256, 0, s>>>(lmax, t->n, na, count, Q, R, is_real,
-                                           coef_size(lmax, t->n, is_real), pitch, plane, nA,
-                                           reinterpret_cast<const double2*>(coef), op);
-    GSHT_LAUNCH_CHECK("k_prep_inverse_bf16");
+  StageTimer tm(GSHT_STAGE_PREP_FORWARD, s);
+  dim3 pg((tp / 2 + 127) / 128, lmax + 1, Q);
+  if (spec32)
+    k_prep_forward_bf16<float2><<<pg, 128, 0, s>>>(lmax, Q, R, count, g->n_theta, tp, plane,
+                                                   reinterpret_cast<const float2*>(spec), op);
+  else
+    k_prep_forward_bf16<double2><<<pg, 128, 0, s>>>(lmax, Q, R, count, g->n_theta, tp, plane,
+                                                    reinterpret_cast<const double2*>(spec), op);
+  GSHT_LAUNCH_CHECK("k_prep_forward_bf16");
+  return GSHT_OK;
+}
+
+namespace {
+
+// Arguments and tensor maps of one Legendre launch of the BF16x3 form over
+// the prepared operand rows (dir 0 inverse: K step bk, results into the
+// spectra, FP32 when spec32; dir 1 forward: K step 64, FP32 result rows into
+// the spectra's buffer). fieldRows: field rows per box (the launch's tile
+// width, or 128 for one CTA's share of a pair tile); tableRows likewise for
+// the table boxes (128, or 64 for a pair's half tile).
+gsht_status bf16_stage(const gsht_grid* g, const Table* t, int dir, int lmax, int is_real,
+                       int count, void* operand, double* spec, bool spec32, int bk, int fieldRows,
+                       int tableRows, TcArgs* a, CUtensorMap* mapA, CUtensorMap* mapB) {
+  const int na = t->n < 0 ? -t->n : t->n;
+  const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
+  const int tp = g->theta_pad;
+  const int pitch = dir == 0 ? (int)round_up(lmax + 1, kBKInv) : tp;
+  const size_t plane = (size_t)(lmax + 1) * R * pitch;
+  const size_t tplane = (size_t)(t->rows + kTablePadRows) * tp;
+  gsht_status st;
+  if (dir == 0) {
+    // MN-major table boxes of 64 colatitudes x bk degrees.
+    st = make_map_bf16(mapA, t->tbf, tp, t->rows + kTablePadRows, 3, tp, tplane, 64, bk,
+                       CU_TENSOR_MAP_SWIZZLE_128B);
+    if (st != GSHT_OK) return st;
+    st = make_map_bf16(mapB, operand, pitch, (uint64_t)(lmax + 1) * R, 3, pitch, plane, bk,
+                       fieldRows, bk == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B);
+  } else {
+    st = make_map_bf16(mapA, t->tbf, tp, t->rows + kTablePadRows, 3, tp, tplane, bk_of(1),
+                       tableRows, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (st != GSHT_OK) return st;
+    st = make_map_bf16(mapB, operand, tp, (uint64_t)(lmax + 1) * R, 3, tp, plane, bk_of(1),
+                       fieldRows, CU_TENSOR_MAP_SWIZZLE_128B);
   }
+  if (st != GSHT_OK) return st;
+  *a = TcArgs{};
+  a->L = g->L; a->lmax = lmax; a->n = t->n; a->na = na; a->count = count; a->Q = Q; a->R = R;
+  a->nTheta = g->n_theta; a->thetaPad = tp; a->isReal = is_real;
+  a->rowOff = t->d_row_off; a->out = reinterpret_cast<double2*>(spec);
+  // The forward's spectra are consumed (split into the BF16 planes) by the
+  // time the kernel writes: their buffer holds its order-major result rows
+  // (keff <= thetaPad), in FP32 (the form's accuracy is FP32-class; half the
+  // bytes of FP64 for the kernel to write and the accumulation to read).
+  a->out32 = (dir == 1 || spec32) ? reinterpret_cast<float2*>(spec) : nullptr;
+  a->coefSize = coef_size(lmax, t->n, is_real); a->err = g->d_err;
+  return GSHT_OK;
+}
+
+}  // namespace
+
+gsht_status legendre_inverse_bf16(const gsht_grid* g, const Table* t, int lmax, int is_real,
+                                  int count, const double* coef, void* operand, double* spec,
+                                  int ntile, cudaStream_t s, bool spec32) {
+  if (!valid_ntile(ntile)) return fail(GSHT_ERR_BAD_ARG, "BF16x3 tile width %d not in {32, 64, 128}", ntile);
+  const int R = 2 * (is_real ? 1 : 2) * count;
+  gsht_status st = bf16_prep_inverse(g, t, lmax, is_real, count, coef, operand, s);
+  if (st != GSHT_OK) return st;
   CUtensorMap mapA, mapB;
+  TcArgs a;
   const int bk = inverse_bk();
-  const size_t tplane = (size_t)(t->rows + kTablePadRows) * g->theta_pad;
-  gsht_status st = make_map_bf16(&mapA, t->tbf, g->theta_pad, t->rows + kTablePadRows, 3,
-                                 g->theta_pad, tplane, 64, bk, CU_TENSOR_MAP_SWIZZLE_128B);
-  if (st != GSHT_OK) return st;
   const bool pairForm = pair_form(R, 0);
-  st = make_map_bf16(&mapB, op, pitch, (uint64_t)(lmax + 1) * R, 3, pitch, plane, bk,
-                     pairForm ? kBM : ntile,
-                     bk == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B);
+  st = bf16_stage(g, t, 0, lmax, is_real, count, operand, spec, spec32, bk,
+                  pairForm ? kBM : ntile, kBM, &a, &mapA, &mapB);
   if (st != GSHT_OK) return st;
-  TcArgs a{};
-  a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count; a.Q = Q; a.R = R;
-  a.nTheta = g->n_theta; a.thetaPad = g->theta_pad; a.isReal = is_real;
-  a.rowOff = t->d_row_off; a.out = reinterpret_cast<double2*>(spec);
-  a.out32 = spec32 ? reinterpret_cast<float2*>(spec) : nullptr;
-  a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
   if (bk == 64)
     return pairForm ? launch_bf16_pair<0, 64>(g, a, mapA, mapB, s)
@@ -1064,50 +1160,123 @@ gsht_status legendre_forward_bf16(const gsht_grid* g, const Table* t, int lmax, 
   if (!valid_ntile(ntile)) return fail(GSHT_ERR_BAD_ARG, "BF16x3 tile width %d not in {32, 64, 128}", ntile);
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
-  const int tp = g->theta_pad;
-  const size_t plane = (size_t)(lmax + 1) * R * tp;
-  auto* op = static_cast<__nv_bfloat16*>(operand);
-  {
-    StageTimer tm(GSHT_STAGE_PREP_FORWARD, s);
-    dim3 pg((tp / 2 + 127) / 128, lmax + 1, Q);
-    if (spec32)
-      k_prep_forward_bf16<float2><<<pg, 128, 0, s>>>(lmax, Q, R, count, g->n_theta, tp, plane,
-                                                     reinterpret_cast<const float2*>(spec), op);
-    else
-      k_prep_forward_bf16<double2><<<pg, 128, 0, s>>>(lmax, Q, R, count, g->n_theta, tp, plane,
-                                                      reinterpret_cast<const double2*>(spec), op);
-    GSHT_LAUNCH_CHECK("k_prep_forward_bf16");
-  }
+  gsht_status st = bf16_prep_forward(g, lmax, is_real, count, spec, operand, s, spec32);
+  if (st != GSHT_OK) return st;
   CUtensorMap mapA, mapB;
-  const size_t tplane = (size_t)(t->rows + kTablePadRows) * tp;
+  TcArgs a;
   const bool pairForm = pair_form(R, 1);
   // Table boxes: 128 degree rows (one CTA's M), or 64 (one CTA's half of a
   // pair's 128-wide table tile).
-  gsht_status st = make_map_bf16(&mapA, t->tbf, tp, t->rows + kTablePadRows, 3, tp, tplane,
-                                 bk_of(1), pairForm ? kPairN / 2 : kBM,
-                                 CU_TENSOR_MAP_SWIZZLE_128B);
+  st = bf16_stage(g, t, 1, lmax, is_real, count, operand, spec, spec32, bk_of(1),
+                  pairForm ? kBM : ntile, pairForm ? kPairN / 2 : kBM, &a, &mapA, &mapB);
   if (st != GSHT_OK) return st;
-  st = make_map_bf16(&mapB, op, tp, (uint64_t)(lmax + 1) * R, 3, tp, plane, bk_of(1),
-                     pairForm ? kBM : ntile, CU_TENSOR_MAP_SWIZZLE_128B);
-  if (st != GSHT_OK) return st;
-  TcArgs a{};
-  a.L = g->L; a.lmax = lmax; a.n = t->n; a.na = na; a.count = count; a.Q = Q; a.R = R;
-  a.nTheta = g->n_theta; a.thetaPad = tp; a.isReal = is_real;
-  // The spectra are consumed (split into the BF16 planes) by now: their
-  // buffer holds the kernel's order-major result rows (keff <= thetaPad),
-  // in FP32 (the form's accuracy is FP32-class; half the bytes of FP64 for
-  // the kernel to write and the accumulation to read).
-  a.rowOff = t->d_row_off; a.out = reinterpret_cast<double2*>(spec);
-  a.out32 = reinterpret_cast<float2*>(spec);
-  a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   {
     StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
     st = pairForm ? launch_bf16_pair<1, 64>(g, a, mapA, mapB, s)
                   : launch_bf16<1, 64>(g, ntile, a, mapA, mapB, s);
   }
   if (st != GSHT_OK) return st;
-  return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, tp, spec, coef, s,
-                            true);
+  return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, g->theta_pad,
+                            spec, coef, s, true);
+}
+
+// ---------------------------------------------------------------------------
+// Multi-group launches (batch plans): one persistent launch of the one-CTA
+// kernel over the tiles of every group of a direction.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <int kDir, int kN, int kBK>
+gsht_status launch_multi_n(const Bf16Multi& mp, cudaStream_t s) {
+  constexpr int kSt = stages_for(kBK);
+  auto kern = k_legendre_tc<kDir, kNsplit, kNsplit, kNprod, kN, kSt, kBK, false, true>;
+  const size_t sm = tc_smem_bytes<kNsplit, kNsplit, kN, kBK, kSt>();
+  GSHT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, mp.device);
+  const int blocks = mp.numTiles < sms ? mp.numTiles : sms;
+  // The launch's own maps and arguments are unused by a multi-group kernel
+  // except the error word (the first group's grid).
+  CUtensorMap none{};
+  TcArgs a{};
+  a.err = mp.err;
+  kern<<<blocks, kThreads, sm, s>>>(none, none, a, static_cast<const int4*>(mp.d_tiles),
+                                    mp.numTiles, static_cast<const TcGroup*>(mp.d_groups));
+  GSHT_LAUNCH_CHECK(kDir == 0 ? "k_legendre_tc<inverse,bf16x3,groups>"
+                              : "k_legendre_tc<forward,bf16x3,groups>");
+  return GSHT_OK;
+}
+
+template <int kDir, int kBK>
+gsht_status launch_multi(const Bf16Multi& mp, cudaStream_t s) {
+  if (mp.ntile == 32) return launch_multi_n<kDir, 32, kBK>(mp, s);
+  if (mp.ntile == 64) return launch_multi_n<kDir, 64, kBK>(mp, s);
+  return launch_multi_n<kDir, 128, kBK>(mp, s);
+}
+
+}  // namespace
+
+gsht_status bf16_multi_build(int dir, const Bf16MultiGroup* gs, int ngroups, int ntile,
+                             Bf16Multi* out) {
+  *out = Bf16Multi{};
+  if (ngroups < 1 || ngroups >= (1 << (31 - kGroupShift)))
+    return fail(GSHT_ERR_BAD_ARG, "%d groups for one multi-group launch", ngroups);
+  if (!valid_ntile(ntile)) return fail(GSHT_ERR_BAD_ARG, "BF16x3 tile width %d not in {32, 64, 128}", ntile);
+  const int bk = dir == 0 ? inverse_bk() : bk_of(1);
+  std::vector<TcGroup> hg(ngroups);
+  std::vector<int4> tiles;
+  for (int gi = 0; gi < ngroups; gi++) {
+    const Bf16MultiGroup& q = gs[gi];
+    if (q.lmax >= (1 << kGroupShift))
+      return fail(GSHT_ERR_BAD_ARG, "lmax %d beyond a multi-group tile's order field", q.lmax);
+    gsht_status st = bf16_stage(q.g, q.t, dir, q.lmax, q.isReal, q.count, q.operand, q.spec,
+                                q.spec32, bk, ntile, kBM, &hg[gi].a, &hg[gi].mapA, &hg[gi].mapB);
+    if (st != GSHT_OK) return st;
+    // The group's tiles as tile_list lays them out, tagged with the group.
+    const int na = q.t->n < 0 ? -q.t->n : q.t->n;
+    const int R = hg[gi].a.R;
+    const int ntiles = (R + ntile - 1) / ntile;
+    for (int m = 0; m <= q.lmax; m++) {
+      const int l0 = m > na ? m : na;
+      const int keff = q.lmax - l0 + 1;
+      const int mtiles = dir == 0 ? (q.g->n_theta + kBM - 1) / kBM : (keff + kBM - 1) / kBM;
+      const int nk = dir == 0 ? (keff + bk - 1) / bk : (q.g->theta_pad + bk - 1) / bk;
+      for (int mt = 0; mt < mtiles; mt++)
+        for (int nt = 0; nt < ntiles; nt++)
+          tiles.push_back(make_int4((gi << kGroupShift) | m, mt, nt, nk));
+    }
+  }
+  out->dir = dir;
+  out->ntile = ntile;
+  out->bk = bk;
+  out->device = gs[0].g->device;
+  out->err = gs[0].g->d_err;
+  out->numTiles = (int)tiles.size();
+  if (dev_malloc_bytes(&out->d_groups, sizeof(TcGroup) * hg.size()) != cudaSuccess ||
+      dev_malloc_bytes(&out->d_tiles, sizeof(int4) * tiles.size()) != cudaSuccess ||
+      cudaMemcpy(out->d_groups, hg.data(), sizeof(TcGroup) * hg.size(), cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemcpy(out->d_tiles, tiles.data(), sizeof(int4) * tiles.size(),
+                 cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    bf16_multi_free(out);
+    return fail(GSHT_ERR_OOM, "multi-group launch tables allocation failed");
+  }
+  return GSHT_OK;
+}
+
+gsht_status bf16_multi_launch(const Bf16Multi& mp, cudaStream_t s) {
+  if (mp.numTiles == 0) return GSHT_OK;
+  StageTimer tm(mp.dir == 0 ? GSHT_STAGE_LEGENDRE_INVERSE : GSHT_STAGE_LEGENDRE_FORWARD, s);
+  if (mp.dir == 0)
+    return mp.bk == 64 ? launch_multi<0, 64>(mp, s) : launch_multi<0, 32>(mp, s);
+  return launch_multi<1, 64>(mp, s);
+}
+
+void bf16_multi_free(Bf16Multi* mp) {
+  dev_free(mp->d_groups);
+  dev_free(mp->d_tiles);
+  *mp = Bf16Multi{};
 }
 
 gsht_status accumulate_forward(int L, int lmax, int n, int na, int count, int Q, int is_real,

@@ -98,3 +98,30 @@ def test_batch_modes_and_replays(gsht):
         # and the round trip recovers the coefficients
         assert relerr(o[:k].cpu().numpy(), f[3][:k].cpu().numpy()) < 1e-12
     batch.close()
+
+
+def test_bf16x3_batch_one_legendre_launch_matches_per_group_launches(gsht, monkeypatch):
+    """The BF16x3 plan runs each direction's Legendre stage as one launch over
+    the work list of every group; with GSHT_BATCH_FUSED=0 each group runs
+    its own transform. Same operand rows, same products in the same order per
+    output element: the two agree to the last bits."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    specs = SPECS + [(200, 0, False), (200, 0, False), (200, 2, True)]
+    fa = _fields(torch, rng, specs)
+    fb = [(lm, n, re, cin, torch.zeros_like(g), torch.from_numpy(init).cuda(), init)
+          for lm, n, re, cin, g, cout, init in fa]
+    fused = gsht.Batch([f[:6] for f in fa], precision="bf16x3", autotune=True)
+    monkeypatch.setenv("GSHT_BATCH_FUSED", "0")
+    per_group = gsht.Batch([f[:6] for f in fb], precision="bf16x3", autotune=False)
+    fused.round_trip()
+    per_group.round_trip()
+    torch.cuda.synchronize()
+    for a, b in zip(fa, fb):
+        assert relerr(a[4].cpu().numpy(), b[4].cpu().numpy()) < 1e-15, a[:3]
+        assert relerr(a[5].cpu().numpy(), b[5].cpu().numpy()) < 1e-15, a[:3]
+    tiles = {t for *_, t in fused.groups()}
+    assert len(tiles) == 1 and tiles <= {32, 64, 128}  # one launch, one tile width
+    fused.close()
+    per_group.close()
