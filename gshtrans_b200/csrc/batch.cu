@@ -220,10 +220,11 @@ gsht_status run_all_fused(gsht_batch* b, int mode, cudaStream_t s, int lanes, bo
     for (size_t gi = 0; gi < b->groups.size(); gi++) {
       Group& gr = b->groups[gi];
       const int k = (int)gr.fields.size();
-      if (gather && (r = copy_group(gr, 0, gr.coefElems, gr.coefInPtrs, gr.coefIn, lane(gi))) != GSHT_OK)
-        return r;
+      // With the callers' buffers, the preparation reads their coefficients
+      // through the group's pointer array (no gather).
       r = bf16_prep_inverse(gr.grid, gr.grid->table(gr.n), gr.lmax, gr.isReal, k,
-                            reinterpret_cast<const double*>(gr.coefIn), gr.op, lane(gi));
+                            reinterpret_cast<const double*>(gr.coefIn), gr.op, lane(gi),
+                            gather ? reinterpret_cast<const double* const*>(gr.coefInPtrs) : nullptr);
       if (r != GSHT_OK) return r;
     }
     if ((r = join()) != GSHT_OK) return r;
@@ -233,32 +234,40 @@ gsht_status run_all_fused(gsht_batch* b, int mode, cudaStream_t s, int lanes, bo
       Group& gr = b->groups[gi];
       const int k = (int)gr.fields.size();
       {
+        // With the callers' buffers, the ring FFTs write their grids through
+        // the group's pointer array (no scatter).
         StageTimer tm(GSHT_STAGE_FFT_INVERSE, lane(gi));
         double* out = reinterpret_cast<double*>(gr.gridBuf);
+        double* const* ptrs = scatter ? reinterpret_cast<double* const*>(gr.gridPtrs) : nullptr;
+        RingRange rr;
+        rr.fields = ptrs;
         r = gr.spec32 ? fft_inverse32(gr.grid, gr.lmax, gr.isReal, k,
-                                      reinterpret_cast<const float*>(gr.spec), out, lane(gi))
-                      : fft_inverse(gr.grid, gr.lmax, gr.isReal, k, gr.spec, out, lane(gi));
+                                      reinterpret_cast<const float*>(gr.spec), out, lane(gi), ptrs)
+                      : fft_inverse(gr.grid, gr.lmax, gr.isReal, k, gr.spec, out, lane(gi), rr);
       }
       if (r != GSHT_OK) return r;
-      if (scatter && (r = copy_group(gr, 1, gr.gridElems, gr.gridPtrs, gr.gridBuf, lane(gi))) != GSHT_OK)
-        return r;
     }
     return join();
   };
-  auto forward = [&](bool gather, bool scatter) -> gsht_status {
+  auto forward = [&](bool gridsAtCaller, bool scatter) -> gsht_status {
     gsht_status r;
     if ((r = fork()) != GSHT_OK) return r;
     for (size_t gi = 0; gi < b->groups.size(); gi++) {
       Group& gr = b->groups[gi];
       const int k = (int)gr.fields.size();
-      if (gather && (r = copy_group(gr, 0, gr.gridElems, gr.gridPtrs, gr.gridBuf, lane(gi))) != GSHT_OK)
-        return r;
       {
+        // The grids: the callers' through the group's pointer array when
+        // gathering (a forward on its own) or after an inverse that wrote
+        // them there (a round trip with the callers' buffers), else the
+        // group's contiguous buffer.
         StageTimer tm(GSHT_STAGE_FFT_FORWARD, lane(gi));
         const double* in = reinterpret_cast<const double*>(gr.gridBuf);
+        double* const* ptrs = gridsAtCaller ? reinterpret_cast<double* const*>(gr.gridPtrs) : nullptr;
+        RingRange rr;
+        rr.fields = ptrs;
         r = gr.spec32 ? fft_forward32(gr.grid, gr.lmax, gr.isReal, k, in,
-                                      reinterpret_cast<float*>(gr.spec), lane(gi))
-                      : fft_forward(gr.grid, gr.lmax, gr.isReal, k, in, gr.spec, lane(gi));
+                                      reinterpret_cast<float*>(gr.spec), lane(gi), ptrs)
+                      : fft_forward(gr.grid, gr.lmax, gr.isReal, k, in, gr.spec, lane(gi), rr);
       }
       if (r != GSHT_OK) return r;
       r = bf16_prep_forward(gr.grid, gr.lmax, gr.isReal, k, gr.spec, gr.op, lane(gi), gr.spec32);
@@ -271,21 +280,21 @@ gsht_status run_all_fused(gsht_batch* b, int mode, cudaStream_t s, int lanes, bo
       Group& gr = b->groups[gi];
       const int k = (int)gr.fields.size();
       const int na = gr.n < 0 ? -gr.n : gr.n;
-      GSHT_CUDA(cudaMemsetAsync(gr.coefOut, 0, sizeof(double2) * gr.coefElems * k, lane(gi)));
+      // With the callers' buffers, the accumulation adds straight into their
+      // coefficients through the group's pointer array (it also applies
+      // c_{L,L} = 0 to complex fields, whose lmax is the grid degree).
+      if (!scatter)
+        GSHT_CUDA(cudaMemsetAsync(gr.coefOut, 0, sizeof(double2) * gr.coefElems * k, lane(gi)));
       r = accumulate_forward(gr.grid->L, gr.lmax, gr.n, na, k, (gr.isReal ? 1 : 2) * k, gr.isReal,
                              gr.coefElems, gr.grid->theta_pad, gr.spec,
-                             reinterpret_cast<double*>(gr.coefOut), lane(gi), true);
+                             reinterpret_cast<double*>(gr.coefOut), lane(gi), true,
+                             scatter ? reinterpret_cast<double* const*>(gr.coefOutPtrs) : nullptr);
       if (r != GSHT_OK) return r;
-      // Every field's lmax is its grid's degree, so complex fields get c_{L,L} = 0.
-      const int cm = gr.isReal ? 2 : 3;
-      if (scatter && (r = copy_group(gr, cm, gr.coefElems, gr.coefOutPtrs, gr.coefOut, lane(gi))) != GSHT_OK)
-        return r;
     }
     return join();
   };
   if (mode == 1 || mode == 2) st = inverse(userIO, userIO);
-  if (st == GSHT_OK && mode == 0) st = forward(userIO, userIO);
-  if (st == GSHT_OK && mode == 2) st = forward(false, userIO);
+  if (st == GSHT_OK && (mode == 0 || mode == 2)) st = forward(userIO, userIO);
   return st;
 }
 

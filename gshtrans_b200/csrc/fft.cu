@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(256) k_fft_inverse(
     }
     __syncthreads();
     const double2* r = fft_block(a, b, plan, tw, +1);
-    double2* o = reinterpret_cast<double2*>(out) + ((size_t)f * nTheta + j) * nPhi;
+    double2* o = reinterpret_cast<double2*>(rr.grid(out, f, 2 * (size_t)nTheta * nPhi)) + (size_t)j * nPhi;
     for (int k = threadIdx.x; k < nPhi; k += blockDim.x) o[k] = r[k];
   } else {
     // Bins X[0..M], M = L (Nyquist); imaginary parts of X[0], X[M] dropped.
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(256) k_fft_inverse(
     }
     __syncthreads();
     const double2* r = fft_block(a, b, plan, tw, +1);
-    double2* o = reinterpret_cast<double2*>(out + ((size_t)f * nTheta + j) * nPhi);
+    double2* o = reinterpret_cast<double2*>(rr.grid(out, f, (size_t)nTheta * nPhi) + (size_t)j * nPhi);
     for (int k = threadIdx.x; k < M; k += blockDim.x) o[k] = r[k];
   }
 }
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(256) k_fft_forward(
     }
   }
   if (!kReal) {
-    const double2* x = reinterpret_cast<const double2*>(in) + ((size_t)f * nTheta + j) * nPhi;
+    const double2* x = reinterpret_cast<const double2*>(rr.grid(in, f, 2 * (size_t)nTheta * nPhi)) + (size_t)j * nPhi;
     for (int k = threadIdx.x; k < nPhi; k += blockDim.x) a[k] = x[k];
     __syncthreads();
     const double2* r = fft_block(a, b, plan, tw, -1);
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(256) k_fft_forward(
     }
   } else {
     const int M = L;
-    const double2* x = reinterpret_cast<const double2*>(in + ((size_t)f * nTheta + j) * nPhi);
+    const double2* x = reinterpret_cast<const double2*>(rr.grid(in, f, (size_t)nTheta * nPhi) + (size_t)j * nPhi);
     for (int k = threadIdx.x; k < M; k += blockDim.x) a[k] = x[k];
     __syncthreads();
     const double2* r = fft_block(a, b, plan, tw, -1);
@@ -483,9 +483,9 @@ __global__ void __launch_bounds__(256) k_fft_inverse_reg(
     const int j = j0 + r;
     if (!rr.has(j)) continue;
     if (!kReal) {
-      reinterpret_cast<double2*>(out)[((size_t)f * nTheta + j) * nPhi + k] = smem[pad8(e)];
+      reinterpret_cast<double2*>(rr.grid(out, f, 2 * (size_t)nTheta * nPhi))[(size_t)j * nPhi + k] = smem[pad8(e)];
     } else {
-      reinterpret_cast<double2*>(out + ((size_t)f * nTheta + j) * nPhi)[k] = smem[pad8(e)];
+      reinterpret_cast<double2*>(rr.grid(out, f, (size_t)nTheta * nPhi) + (size_t)j * nPhi)[k] = smem[pad8(e)];
     }
   }
 }
@@ -516,9 +516,9 @@ __global__ void __launch_bounds__(256) k_fft_forward_reg(
     double2 x = make_double2(0.0, 0.0);
     if (j < nTheta) {
       if (!kReal) {
-        x = reinterpret_cast<const double2*>(in)[((size_t)f * nTheta + j) * nPhi + k];
+        x = reinterpret_cast<const double2*>(rr.grid(in, f, 2 * (size_t)nTheta * nPhi))[(size_t)j * nPhi + k];
       } else {
-        x = reinterpret_cast<const double2*>(in + ((size_t)f * nTheta + j) * nPhi)[k];
+        x = reinterpret_cast<const double2*>(rr.grid(in, f, (size_t)nTheta * nPhi) + (size_t)j * nPhi)[k];
       }
     }
     smem[pad8(e)] = x;
@@ -665,9 +665,9 @@ __global__ void __launch_bounds__(256) k_fft_inverse_p2(
     const int j = j0 + r;
     if (!rr.has(j)) continue;
     if (!kReal) {
-      reinterpret_cast<double2*>(out)[((size_t)f * nTheta + j) * nPhi + k] = smem[P2<N>::at(r, k)];
+      reinterpret_cast<double2*>(rr.grid(out, f, 2 * (size_t)nTheta * nPhi))[(size_t)j * nPhi + k] = smem[P2<N>::at(r, k)];
     } else {
-      reinterpret_cast<double2*>(out + ((size_t)f * nTheta + j) * nPhi)[k] = smem[P2<N>::at(r, k)];
+      reinterpret_cast<double2*>(rr.grid(out, f, (size_t)nTheta * nPhi) + (size_t)j * nPhi)[k] = smem[P2<N>::at(r, k)];
     }
   }
 }
@@ -702,8 +702,8 @@ __global__ void __launch_bounds__(256) k_fft_forward_p2(
     const int j = j0 + r;
     double2 x = make_double2(0.0, 0.0);
     if (j < nTheta) {
-      x = kReal ? reinterpret_cast<const double2*>(in + ((size_t)f * nTheta + j) * nPhi)[k]
-                : reinterpret_cast<const double2*>(in)[((size_t)f * nTheta + j) * nPhi + k];
+      x = kReal ? reinterpret_cast<const double2*>(rr.grid(in, f, (size_t)nTheta * nPhi) + (size_t)j * nPhi)[k]
+                : reinterpret_cast<const double2*>(rr.grid(in, f, 2 * (size_t)nTheta * nPhi))[(size_t)j * nPhi + k];
     }
     xv[it] = x;
   }
@@ -1074,8 +1074,8 @@ __global__ void __launch_bounds__(kPts / 16, p3_min_blocks<kPts, C>()) k_fft_inv
       dft_reg<P>(v, +1);
       const int th = j0 + ring;
       if (rr.has(th)) {
-        double2* row = kReal ? reinterpret_cast<double2*>(out + ((size_t)f * nTheta + th) * nPhi)
-                             : reinterpret_cast<double2*>(out) + ((size_t)f * nTheta + th) * nPhi;
+        double2* row = kReal ? reinterpret_cast<double2*>(rr.grid(out, f, (size_t)nTheta * nPhi) + (size_t)th * nPhi)
+                             : reinterpret_cast<double2*>(rr.grid(out, f, 2 * (size_t)nTheta * nPhi)) + (size_t)th * nPhi;
 #pragma unroll
         for (int r = 0; r < P; r++) row[k + r * M] = to_c<double2>(v[r]);
       }
@@ -1114,8 +1114,8 @@ __global__ void __launch_bounds__(kPts / 16, p3_min_blocks<kPts, SpecT>()) k_fft
     const int ring = threadIdx.x >> ilog2(NBR), jj = threadIdx.x & (NBR - 1);
     const int th = j0 + ring;
     C v[16];
-    const double2* row = kReal ? reinterpret_cast<const double2*>(in + ((size_t)f * nTheta + th) * nPhi)
-                               : reinterpret_cast<const double2*>(in) + ((size_t)f * nTheta + th) * nPhi;
+    const double2* row = kReal ? reinterpret_cast<const double2*>(rr.grid(in, f, (size_t)nTheta * nPhi) + (size_t)th * nPhi)
+                               : reinterpret_cast<const double2*>(rr.grid(in, f, 2 * (size_t)nTheta * nPhi)) + (size_t)th * nPhi;
 #pragma unroll
     for (int q = 0; q < 16; q++) v[q] = th < nTheta ? to_c<C>(row[jj + q * NBR]) : C{};
     dft_reg<16>(v, -1);
@@ -1520,8 +1520,9 @@ bool fft_spec32_supported(const gsht_grid* g, int is_real) {
 // The three-pass kernels with FP32 spectra (unmirrored -m rows); only for the
 // ring lengths fft_spec32_supported accepts.
 gsht_status fft_spec32(const gsht_grid* g, int dir, int lmax, int is_real, int count,
-                       const void* src, void* dst, cudaStream_t s) {
-  const RingRange rr = resolve(RingRange{}, g->n_theta);
+                       const void* src, void* dst, cudaStream_t s, double* const* fields) {
+  RingRange rr = resolve(RingRange{}, g->n_theta);
+  rr.fields = fields;
   switch (is_real ? g->n_phi / 2 : g->n_phi) {
     case 256: return launch_p3<256, float2>(g, dir, lmax, is_real, count, src, dst, s, rr);
     case 512: return launch_p3<512, float2>(g, dir, lmax, is_real, count, src, dst, s, rr);
@@ -1533,13 +1534,13 @@ gsht_status fft_spec32(const gsht_grid* g, int dir, int lmax, int is_real, int c
 }
 
 gsht_status fft_inverse32(const gsht_grid* g, int lmax, int is_real, int count, const float* spec,
-                          double* out, cudaStream_t s) {
-  return fft_spec32(g, 1, lmax, is_real, count, spec, out, s);
+                          double* out, cudaStream_t s, double* const* fields) {
+  return fft_spec32(g, 1, lmax, is_real, count, spec, out, s, fields);
 }
 
 gsht_status fft_forward32(const gsht_grid* g, int lmax, int is_real, int count, const double* in,
-                          float* spec, cudaStream_t s) {
-  return fft_spec32(g, 0, lmax, is_real, count, in, spec, s);
+                          float* spec, cudaStream_t s, double* const* fields) {
+  return fft_spec32(g, 0, lmax, is_real, count, in, spec, s, fields);
 }
 
 }  // namespace gsht

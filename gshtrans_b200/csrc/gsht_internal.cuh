@@ -209,10 +209,21 @@ gsht_status wigner_compute(int lmax, int mmax, int nmax, int mrange, int nrange,
 
 // Colatitudes [jBegin, jEnd) a ring-FFT launch transforms: the whole grid,
 // or one rank's slab of a transform sharded over colatitudes (rings outside
-// the range are not written). jEnd < 0 stands for the whole grid.
+// the range are not written). jEnd < 0 stands for the whole grid. fields:
+// when set (a device array), field f's grid is fields[f] rather than the
+// f-th of the launch's contiguous grids (batch plans: the callers' buffers).
 struct RingRange {
   int jBegin = 0, jEnd = -1;
+  double* const* fields = nullptr;
   __host__ __device__ bool has(int j) const { return j >= jBegin && j < jEnd; }
+  // Start of field f's grid, given the contiguous grids at base with
+  // fieldDoubles doubles each.
+  __host__ __device__ double* grid(double* base, int f, size_t fieldDoubles) const {
+    return fields ? fields[f] : base + (size_t)f * fieldDoubles;
+  }
+  __host__ __device__ const double* grid(const double* base, int f, size_t fieldDoubles) const {
+    return fields ? fields[f] : base + (size_t)f * fieldDoubles;
+  }
 };
 inline RingRange resolve(RingRange r, int nTheta) {
   if (r.jEnd < 0 || r.jEnd > nTheta) r.jEnd = nTheta;
@@ -229,9 +240,9 @@ gsht_status fft_forward(const gsht_grid* g, int lmax, int is_real, int count,
 // colatitudes (no mirror). Ring lengths 256..4096 (powers of two) only.
 bool fft_spec32_supported(const gsht_grid* g, int is_real);
 gsht_status fft_inverse32(const gsht_grid* g, int lmax, int is_real, int count, const float* spec,
-                          double* out, cudaStream_t s);
+                          double* out, cudaStream_t s, double* const* fields = nullptr);
 gsht_status fft_forward32(const gsht_grid* g, int lmax, int is_real, int count, const double* in,
-                          float* spec, cudaStream_t s);
+                          float* spec, cudaStream_t s, double* const* fields = nullptr);
 
 // Legendre stage, FP64 (legendre_fp64.cu).
 gsht_status fp64_operand_elems(const gsht_grid* g, const Table* t, int lmax, int is_real,
@@ -260,7 +271,8 @@ gsht_status legendre_inverse_fp64_layout(const gsht_grid* g, const Table* t, int
 // tiles of several groups (each with its grid, table, operand rows and
 // spectra; every group's tensor maps and arguments in device memory).
 gsht_status bf16_prep_inverse(const gsht_grid* g, const Table* t, int lmax, int is_real,
-                              int count, const double* coef, void* operand, cudaStream_t s);
+                              int count, const double* coef, void* operand, cudaStream_t s,
+                              const double* const* fieldPtrs = nullptr);
 gsht_status bf16_prep_forward(const gsht_grid* g, int lmax, int is_real, int count,
                               const double* spec, void* operand, cudaStream_t s, bool spec32);
 struct Bf16MultiGroup {
@@ -332,10 +344,12 @@ gsht_status legendre_forward_rec(const gsht_grid* g, const Table* t, int lmax, i
 
 // Adds order-major result rows R[m][q][l - l0] (pitch `pitch`; complex
 // FP64, or FP32 with rows32) into the packed coefficients of `count` fields
-// (forward accumulate semantics).
+// (forward accumulate semantics): coef + f * coefSize, or fieldPtrs[f] when
+// fieldPtrs (a device array) is set.
 gsht_status accumulate_forward(int L, int lmax, int n, int na, int count, int Q, int is_real,
                                long coefSize, int pitch, const double* rows, double* coef,
-                               cudaStream_t s, bool rows32 = false);
+                               cudaStream_t s, bool rows32 = false,
+                               double* const* fieldPtrs = nullptr);
 
 // Cached operand layout (legendre_fp64.cu); the caller holds g->mu.
 const OperandLayout* operand_layout(const gsht_grid* g, int lmax, int na,

@@ -708,10 +708,13 @@ __device__ __forceinline__ void split3(float x, __nv_bfloat16& h, __nv_bfloat16&
 // cover consecutive k ranges). blockIdx.x walks the triangle of (degree tile
 // a, order tile b <= a) pairs row by row (row b holds nA - b tiles), so no
 // block is launched for the empty upper half.
+// fieldPtrs: when set, field f's coefficients are read from fieldPtrs[f]
+// (batch plans: the callers' buffers) instead of coef + f * coefSize.
 template <int kQB>
 __global__ void __launch_bounds__(256) k_prep_inverse_bf16(
     int lmax, int n, int na, int count, int Q, int R, int isReal, long coefSize, int pitch,
-    size_t plane, int nA, const double2* __restrict__ coef, __nv_bfloat16* __restrict__ op) {
+    size_t plane, int nA, const double2* __restrict__ coef, __nv_bfloat16* __restrict__ op,
+    const double2* const* __restrict__ fieldPtrs) {
   constexpr int kRows = 33;  // degrees lt-1 .. lt+31
   __shared__ double2 tile[kQB][kRows][33];
   int i0 = blockIdx.x, b = 0;
@@ -734,7 +737,7 @@ __global__ void __launch_bounds__(256) k_prep_inverse_bf16(
       if (q < Q && l >= 0 && l <= lmax && m <= l && l >= na && !(sgn == 1 && m == 0)) {
         const long idx = isReal ? (long)l * (l + 1) / 2 - (long)na * (na + 1) / 2 + m
                                 : (long)l * l - (long)n * n + l + (sgn ? -m : m);
-        v = coef[(size_t)f * coefSize + idx];
+        v = fieldPtrs ? fieldPtrs[f][idx] : coef[(size_t)f * coefSize + idx];
         if (sgn == 1 && ((l + n) & 1)) v = make_double2(-v.x, -v.y);
       }
       tile[u][i][lane] = v;
@@ -783,10 +786,13 @@ __global__ void __launch_bounds__(256) k_prep_inverse_bf16(
 // transposed in shared memory, and the packed layout (order-contiguous for a
 // fixed degree) is read-modify-written coalesced. RowT: double2, or float2
 // for the rows of the BF16x3 form.
+// fieldPtrs: when set, field f's coefficients are fieldPtrs[f] (batch
+// plans: the callers' buffers) instead of coef + f * coefSize.
 template <typename RowT>
 __global__ void __launch_bounds__(256) k_accumulate_forward(
     int L, int lmax, int n, int na, int count, int Q, int isReal, long coefSize, int pitch,
-    const RowT* __restrict__ rows, double2* __restrict__ coef) {
+    const RowT* __restrict__ rows, double2* __restrict__ coef,
+    double2* const* __restrict__ fieldPtrs) {
   __shared__ double2 tile[32][33];
   const int lt = blockIdx.x * 32, mt = blockIdx.y * 32, q = blockIdx.z;
   if (mt > lt + 31 || mt > lmax) return;
@@ -810,7 +816,7 @@ __global__ void __launch_bounds__(256) k_accumulate_forward(
     if (l > lmax || l < na || m > l || m > lmax || (sgn == 1 && m == 0)) continue;
     const long idx = isReal ? (long)l * (l + 1) / 2 - (long)na * (na + 1) / 2 + m
                             : (long)l * l - (long)n * n + l + (sgn ? -m : m);
-    double2* ptr = coef + (size_t)f * coefSize + idx;
+    double2* ptr = (fieldPtrs ? fieldPtrs[f] : coef + (size_t)f * coefSize) + idx;
     double2 v = tile[lane][i];
     if (sgn == 1 && ((l + n) & 1)) v = make_double2(-v.x, -v.y);
     if (!isReal && sgn == 0 && m == L && l == L && lmax == L) {
@@ -1047,7 +1053,8 @@ size_t bf16_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, 
 }
 
 gsht_status bf16_prep_inverse(const gsht_grid* g, const Table* t, int lmax, int is_real,
-                              int count, const double* coef, void* operand, cudaStream_t s) {
+                              int count, const double* coef, void* operand, cudaStream_t s,
+                              const double* const* fieldPtrs) {
   const int na = t->n < 0 ? -t->n : t->n;
   const int Q = (is_real ? 1 : 2) * count, R = 2 * Q;
   const int pitch = (int)round_up(lmax + 1, kBKInv);
@@ -1061,7 +1068,8 @@ gsht_status bf16_prep_inverse(const gsht_grid* g, const Table* t, int lmax, int 
   k_prep_inverse_bf16<kQB><<<pg, 256, 0, s>>>(lmax, t->n, na, count, Q, R, is_real,
                                               coef_size(lmax, t->n, is_real), pitch, plane, nA,
                                               reinterpret_cast<const double2*>(coef),
-                                              static_cast<__nv_bfloat16*>(operand));
+                                              static_cast<__nv_bfloat16*>(operand),
+                                              reinterpret_cast<const double2* const*>(fieldPtrs));
   GSHT_LAUNCH_CHECK("k_prep_inverse_bf16");
   return GSHT_OK;
 }
@@ -1281,17 +1289,18 @@ void bf16_multi_free(Bf16Multi* mp) {
 
 gsht_status accumulate_forward(int L, int lmax, int n, int na, int count, int Q, int is_real,
                                long coefSize, int pitch, const double* rows, double* coef,
-                               cudaStream_t s, bool rows32) {
+                               cudaStream_t s, bool rows32, double* const* fieldPtrs) {
   StageTimer tm(GSHT_STAGE_ACCUMULATE_FORWARD, s);
   dim3 ag((lmax + 32) / 32, (lmax + 32) / 32, Q);
+  auto* fp = reinterpret_cast<double2* const*>(fieldPtrs);
   if (rows32)
     k_accumulate_forward<float2><<<ag, 256, 0, s>>>(L, lmax, n, na, count, Q, is_real, coefSize,
                                                     pitch, reinterpret_cast<const float2*>(rows),
-                                                    reinterpret_cast<double2*>(coef));
+                                                    reinterpret_cast<double2*>(coef), fp);
   else
     k_accumulate_forward<double2><<<ag, 256, 0, s>>>(L, lmax, n, na, count, Q, is_real, coefSize,
                                                      pitch, reinterpret_cast<const double2*>(rows),
-                                                     reinterpret_cast<double2*>(coef));
+                                                     reinterpret_cast<double2*>(coef), fp);
   GSHT_LAUNCH_CHECK("k_accumulate_forward");
   return GSHT_OK;
 }
