@@ -123,6 +123,7 @@ class ClockSampler:
         self._nvml = nvml
         self._stop = threading.Event()
         self._t = None
+        self._opened = None
 
     def _open_nvml(self):
         nv = self._nvml
@@ -155,29 +156,22 @@ class ClockSampler:
         nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
         return nv, h, reasons, nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
 
-    def _run_nvml(self, nv, h, reasons, mx):
-        self.source = "nvml"
-        while not self._stop.is_set():
-            try:
-                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-                r = int(reasons(h))
-                self.samples.append([str(sm), str(mx)] +
-                                    ["Active" if r & bit else "Not Active" for bit in self.REASON_BITS])
-            except Exception:
-                pass
-            self._stop.wait(self.period_s)
+    def _sample_nvml(self):
+        nv, h, reasons, mx = self._opened
         try:
-            nv.nvmlShutdown()
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            r = int(reasons(h))
+            self.samples.append([str(sm), str(mx)] +
+                                ["Active" if r & bit else "Not Active" for bit in self.REASON_BITS])
         except Exception:
             pass
 
     def _run(self):
-        try:
-            opened = self._open_nvml()
-        except Exception:
-            opened = None
-        if opened is not None:
-            self._run_nvml(*opened)
+        if self._opened is not None:
+            self.source = "nvml"
+            while not self._stop.is_set():
+                self._sample_nvml()
+                self._stop.wait(self.period_s)
             return
         self.source = "nvidia-smi"
         dev = self.bus_id or str(self.index)
@@ -196,6 +190,15 @@ class ClockSampler:
             self._stop.wait(0.2)
 
     def __enter__(self):
+        # NVML is opened here, before the timed region, and sampled once at
+        # its start and once at its end, so that a short region still has
+        # samples from its own span.
+        try:
+            self._opened = self._open_nvml()
+        except Exception:
+            self._opened = None
+        if self._opened is not None:
+            self._sample_nvml()
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
         return self
@@ -204,6 +207,12 @@ class ClockSampler:
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
+        if self._opened is not None:
+            self._sample_nvml()
+            try:
+                self._opened[0].nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
         if not self.samples:
@@ -471,8 +480,15 @@ def impl_ours(args):
     field = torch.empty((B, grid.FieldSize()), dtype=torch.complex128, device=dev)
     back = torch.zeros_like(coef)
 
-    results = {m: measure_mode(gsht, grid, torch, dev, coef, field, back, m, args, world, dist)
-               for m in modes}
+    # Each form is timed in its own loop; the GPU idles a few seconds before
+    # each, so that every form starts from a similar thermal and power state
+    # (a dense tensor-core loop leaves the part near its power cap, which
+    # would otherwise slow whichever form runs next).
+    results = {}
+    for i, m in enumerate(modes):
+        if i:
+            time.sleep(3.0)
+        results[m] = measure_mode(gsht, grid, torch, dev, coef, field, back, m, args, world, dist)
     # accuracy of each form against the FP64 path on the same inputs
     ref_f = ref_c = None
     if "fp64" in modes and len(modes) > 1:
@@ -523,6 +539,7 @@ def impl_ours(args):
                 "forward_rel_err_vs_fp64": r.get("forward_rel_err_vs_fp64"),
                 "stages": r["stages"],
                 "roofline": legendre_roofline(m, r, args, peaks),
+                "clocks": r["clocks"],
             }
             if r.get("trace"):
                 mode_lines[m]["trace"] = r["trace"]
