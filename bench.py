@@ -440,8 +440,9 @@ def legendre_roofline(precision, res, args, peaks):
     # None for any other shape.
     traffic = None
     if L == L_MAX and B == 64 and N_UPPER == 0:
-        traffic = {"fp64": (7.575e9 + 8.788e9) / 2, "bf16x3": (5.384e9 + 6.302e9) / 2,
-                   "ozaki": (7.154e9 + 6.875e9) / 2}.get(precision)
+        traffic = {"fp64": (7.581e9 + 8.784e9) / 2, "bf16x3": (5.319e9 + 5.987e9) / 2,
+                   "ozaki": (7.156e9 + 6.883e9) / 2,
+                   "ozaki4": (5.118e9 + 4.678e9) / 2}.get(precision)
     return {
         "kernel": {"fp64": "k_legendre_fp64", "bf16x3": "k_legendre_tc (kind::f16)",
                    "ozaki": "k_legendre_oz (kind::i8)",
