@@ -35,7 +35,7 @@ __global__ void k_wait_never_completes(int* err) {
 
 }  // namespace
 
-int g_tc_trace = 0;
+std::atomic<int> g_tc_trace{0};
 
 unsigned long long* trace_slots(int form, int dir, cudaStream_t s) {
   void* p = nullptr;
@@ -56,7 +56,7 @@ unsigned long long* trace_slots(int form, int dir, cudaStream_t s) {
 using namespace gsht;
 
 extern "C" gsht_status gsht_tc_trace_enable(int on) {
-  g_tc_trace = on != 0;
+  g_tc_trace.store(on != 0);
   return GSHT_OK;
 }
 

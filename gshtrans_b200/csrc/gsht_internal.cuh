@@ -29,7 +29,7 @@ extern thread_local unsigned long long t_launches;
 // set, launches take the traced kernel copies, whose counters trace_slots
 // (form 0 BF16x3, 1 Ozaki; dir 0 inverse, 1 forward) clears on stream s and
 // returns (NULL on failure).
-extern int g_tc_trace;
+extern std::atomic<int> g_tc_trace;
 unsigned long long* trace_slots(int form, int dir, cudaStream_t s);
 
 #define GSHT_CUDA(call)                                   \
