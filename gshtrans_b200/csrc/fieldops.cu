@@ -10,8 +10,15 @@
 // per grid point over a small stack: every input is read once (a complex
 // value with one 128-bit load, a real value with one 64-bit load) and the
 // result is written once, so the whole expression costs one pass over HBM.
+#include <dlfcn.h>
+#include <nvrtc.h>
+
+#include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <string>
+#include <vector>
 
 #include "gsht_internal.cuh"
 #include "tc_common.cuh"
@@ -313,6 +320,211 @@ __global__ void __launch_bounds__(32 * (kEvalWarps + 1), 2)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Compiled form: the program is turned into CUDA C++ source (one statement per
+// operation, every input loaded once per point however often the program
+// reads it) and compiled for the device with NVRTC the first time it is seen;
+// the kernel is cached per (device, source). Each thread evaluates four
+// points 256 apart per pass, with all their loads issued before the
+// arithmetic; complex values move as 128-bit loads and stores. The arithmetic
+// is written as the interpreter's (the same complex product, Smith's division),
+// compiled with the same contraction settings. Where NVRTC cannot be loaded
+// or a program fails to compile, the interpreting kernels above run instead;
+// GSHT_FIELD_JIT=0 selects them for comparisons.
+// ---------------------------------------------------------------------------
+struct JitArgs {
+  const void* in[kMaxInputs];
+  void* out;
+  long long npoints, stride;
+};
+
+constexpr int kJitThreads = 256, kJitPoints = 4;
+
+struct Nvrtc {
+  bool ok = false;
+  nvrtcResult (*create)(nvrtcProgram*, const char*, const char*, int, const char* const*,
+                        const char* const*) = nullptr;
+  nvrtcResult (*compile)(nvrtcProgram, int, const char* const*) = nullptr;
+  nvrtcResult (*cubinSize)(nvrtcProgram, size_t*) = nullptr;
+  nvrtcResult (*cubin)(nvrtcProgram, char*) = nullptr;
+  nvrtcResult (*destroy)(nvrtcProgram*) = nullptr;
+};
+
+const Nvrtc& nvrtc() {
+  static Nvrtc n;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* h = dlopen("libnvrtc.so.12", RTLD_NOW | RTLD_LOCAL);
+    if (!h) h = dlopen("libnvrtc.so", RTLD_NOW | RTLD_LOCAL);
+    if (!h) return;
+    n.create = reinterpret_cast<decltype(n.create)>(dlsym(h, "nvrtcCreateProgram"));
+    n.compile = reinterpret_cast<decltype(n.compile)>(dlsym(h, "nvrtcCompileProgram"));
+    n.cubinSize = reinterpret_cast<decltype(n.cubinSize)>(dlsym(h, "nvrtcGetCUBINSize"));
+    n.cubin = reinterpret_cast<decltype(n.cubin)>(dlsym(h, "nvrtcGetCUBIN"));
+    n.destroy = reinterpret_cast<decltype(n.destroy)>(dlsym(h, "nvrtcDestroyProgram"));
+    n.ok = n.create && n.compile && n.cubinSize && n.cubin && n.destroy;
+  });
+  return n;
+}
+
+// A double as an exact source literal.
+std::string dlit(double v) {
+  unsigned long long b;
+  std::memcpy(&b, &v, sizeof b);
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "__longlong_as_double(0x%016llxLL)", b);
+  return buf;
+}
+
+std::string jit_source(const Program& p) {
+  std::string s =
+      "struct JitArgs { const void* in[" + std::to_string(kMaxInputs) + "]; void* out;"
+      " long long npoints, stride; };\n"
+      "__device__ __forceinline__ double2 cmul(double2 a, double2 b) {\n"
+      "  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);\n}\n"
+      "__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {\n"
+      "  if (fabs(b.x) >= fabs(b.y)) {\n"
+      "    const double r = b.y / b.x, d = b.x + r * b.y;\n"
+      "    return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);\n  }\n"
+      "  const double r = b.x / b.y, d = b.y + r * b.x;\n"
+      "  return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);\n}\n"
+      "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(kJitThreads) +
+      ") gsht_field_jit(JitArgs p) {\n"
+      "  const long long base = (long long)blockIdx.y * p.stride;\n"
+      "  for (long long i0 = (long long)blockIdx.x * " + std::to_string(kJitThreads * kJitPoints) +
+      " + threadIdx.x; i0 < p.npoints; i0 += (long long)gridDim.x * " +
+      std::to_string(kJitThreads * kJitPoints) + ") {\n";
+  const std::string P = std::to_string(kJitPoints), T = std::to_string(kJitThreads);
+  // Every input the program reads, loaded once per point.
+  std::vector<int> used(p.ninputs, 0);
+  for (int k = 0; k < p.nops; k++)
+    if (p.op[k] == GSHT_OP_LOAD) used[p.arg[k]] = 1;
+  for (int a = 0; a < p.ninputs; a++) {
+    if (!used[a]) continue;
+    const std::string A = std::to_string(a);
+    s += "    double2 in" + A + "[" + P + "];\n";
+    s += "    #pragma unroll\n    for (int j = 0; j < " + P + "; j++) {\n";
+    s += "      const long long i = i0 + " + T + " * j;\n";
+    if (p.inReal[a])
+      s += "      in" + A + "[j] = i < p.npoints ? make_double2(static_cast<const double*>(p.in[" + A +
+           "])[base + i], 0.0) : make_double2(0.0, 0.0);\n";
+    else
+      s += "      in" + A + "[j] = i < p.npoints ? static_cast<const double2*>(p.in[" + A +
+           "])[base + i] : make_double2(0.0, 0.0);\n";
+    s += "    }\n";
+  }
+  s += "    #pragma unroll\n    for (int j = 0; j < " + P + "; j++) {\n";
+  s += "      const long long i = i0 + " + T + " * j;\n      if (i >= p.npoints) break;\n";
+  std::vector<std::string> stk;
+  int tmp = 0;
+  auto fresh = [&](const std::string& expr) {
+    const std::string name = "t" + std::to_string(tmp++);
+    s += "      const double2 " + name + " = " + expr + ";\n";
+    stk.push_back(name);
+  };
+  for (int k = 0; k < p.nops; k++) {
+    const int op = p.op[k];
+    if (op == GSHT_OP_LOAD) {
+      stk.push_back("in" + std::to_string(p.arg[k]) + "[j]");
+    } else if (op == GSHT_OP_CONST) {
+      fresh("make_double2(" + dlit(p.re[k]) + ", " + dlit(p.im[k]) + ")");
+    } else if (op >= GSHT_OP_NEG) {
+      const std::string a = stk.back();
+      stk.pop_back();
+      if (op == GSHT_OP_NEG) fresh("make_double2(-" + a + ".x, -" + a + ".y)");
+      else if (op == GSHT_OP_CONJ) fresh("make_double2(" + a + ".x, -" + a + ".y)");
+      else if (op == GSHT_OP_REAL) fresh("make_double2(" + a + ".x, 0.0)");
+      else fresh("make_double2(" + a + ".y, 0.0)");
+    } else {
+      const std::string b = stk.back();
+      stk.pop_back();
+      const std::string a = stk.back();
+      stk.pop_back();
+      if (op == GSHT_OP_ADD) fresh("make_double2(" + a + ".x + " + b + ".x, " + a + ".y + " + b + ".y)");
+      else if (op == GSHT_OP_SUB) fresh("make_double2(" + a + ".x - " + b + ".x, " + a + ".y - " + b + ".y)");
+      else if (op == GSHT_OP_MUL) fresh("cmul(" + a + ", " + b + ")");
+      else fresh("cdiv(" + a + ", " + b + ")");
+    }
+  }
+  if (p.outReal)
+    s += "      static_cast<double*>(p.out)[base + i] = " + stk.back() + ".x;\n";
+  else
+    s += "      static_cast<double2*>(p.out)[base + i] = " + stk.back() + ";\n";
+  s += "    }\n  }\n}\n";
+  return s;
+}
+
+std::mutex g_jit_mu;
+std::map<std::pair<int, std::string>, cudaKernel_t> g_jit_kernels;  // null: failed to build
+
+// The cached compiled kernel of p on device dev (compiled on first use), or
+// null when NVRTC is unavailable or the program does not compile.
+cudaKernel_t jit_kernel(const Program& p, int dev) {
+  const char* e = getenv("GSHT_FIELD_JIT");
+  if (e && e[0] == '0') return nullptr;
+  const Nvrtc& nv = nvrtc();
+  if (!nv.ok) return nullptr;
+  const std::string src = jit_source(p);
+  std::lock_guard<std::mutex> lk(g_jit_mu);
+  const auto key = std::make_pair(dev, src);
+  auto it = g_jit_kernels.find(key);
+  if (it != g_jit_kernels.end()) return it->second;
+  cudaKernel_t kern = nullptr;
+  nvrtcProgram prog = nullptr;
+  if (nv.create(&prog, src.c_str(), "gsht_field_jit.cu", 0, nullptr, nullptr) == NVRTC_SUCCESS) {
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, dev);
+    const std::string arch = "--gpu-architecture=sm_" + std::to_string(prop.major * 10 + prop.minor) +
+                             (prop.major >= 9 ? "a" : "");
+    const char* opts[] = {arch.c_str(), "--std=c++17"};
+    size_t n = 0;
+    if (nv.compile(prog, 2, opts) == NVRTC_SUCCESS && nv.cubinSize(prog, &n) == NVRTC_SUCCESS &&
+        n > 0) {
+      std::vector<char> cubin(n);
+      cudaLibrary_t lib = nullptr;
+      if (nv.cubin(prog, cubin.data()) == NVRTC_SUCCESS &&
+          cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0) ==
+              cudaSuccess &&
+          cudaLibraryGetKernel(&kern, lib, "gsht_field_jit") != cudaSuccess) {
+        kern = nullptr;
+      }
+      cudaGetLastError();
+    }
+    nv.destroy(&prog);
+  }
+  g_jit_kernels[key] = kern;
+  return kern;
+}
+
+// Runs p through its compiled kernel; false when there is none (the caller
+// then interprets it).
+bool jit_launch(const Program& p, int dev, int sms, cudaStream_t s, gsht_status* st) {
+  if (p.count > 65535) return false;
+  cudaKernel_t kern = jit_kernel(p, dev);
+  if (!kern) return false;
+  JitArgs a{};
+  for (int i = 0; i < p.ninputs; i++) a.in[i] = p.in[i];
+  a.out = p.out;
+  a.npoints = p.npoints;
+  a.stride = p.stride;
+  const long long per = (long long)kJitThreads * kJitPoints;
+  long long bx = (p.npoints + per - 1) / per;
+  const long long cap = ((long long)sms * 8 + p.count - 1) / p.count;
+  if (bx > cap) bx = cap < 1 ? 1 : cap;
+  void* args[] = {&a};
+  const cudaError_t e = cudaLaunchKernel(reinterpret_cast<const void*>(kern),
+                                         dim3((unsigned)bx, (unsigned)p.count), dim3(kJitThreads),
+                                         args, 0, s);
+  if (e != cudaSuccess) {
+    *st = cuda_fail(e, "compiled field kernel launch");
+    return true;
+  }
+  t_launches++;
+  g_launches++;
+  *st = GSHT_OK;
+  return true;
+}
+
 std::mutex g_stage_mu;
 void* g_stage = nullptr;
 size_t g_stage_bytes = 0;
@@ -321,6 +533,15 @@ size_t g_stage_bytes = 0;
 }  // namespace gsht
 
 using namespace gsht;
+
+extern "C" gsht_status gsht_field_jit_stats(int* compiled, int* failed) {
+  std::lock_guard<std::mutex> lk(g_jit_mu);
+  int c = 0, f = 0;
+  for (const auto& kv : g_jit_kernels) (kv.second ? c : f)++;
+  if (compiled) *compiled = c;
+  if (failed) *failed = f;
+  return GSHT_OK;
+}
 
 extern "C" gsht_status gsht_field_eval(const gsht_expr_op* program, int nops,
                                        const void* const* inputs, const int* input_is_real,
@@ -422,6 +643,17 @@ extern "C" gsht_status gsht_field_eval(const gsht_expr_op* program, int nops,
     bpp += esz;
     streamed = streamed && (reinterpret_cast<uintptr_t>(p.in[a]) % 16 == 0);
     if (p.inReal[a]) streamed = streamed && npoints % 2 == 0 && field_stride % 2 == 0;
+  }
+  gsht_status jst = GSHT_OK;
+  if (jit_launch(p, dev, sms, s, &jst)) {
+    if (jst != GSHT_OK) return jst;
+    if (anyHost) {
+      if (p.out != out)
+        GSHT_CUDA(cudaMemcpyAsync(out, p.out, sizeof(double) * (p.outReal ? 1 : 2) * span,
+                                  cudaMemcpyDeviceToHost, s));
+      GSHT_CUDA(cudaStreamSynchronize(s));
+    }
+    return GSHT_OK;
   }
   if (streamed) {
     const int threads = 32 * (kEvalWarps + 1);

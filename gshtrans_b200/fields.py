@@ -39,6 +39,15 @@ library.gsht_field_eval.argtypes = [
     ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
     ctypes.c_long, ctypes.c_int, ctypes.c_long, ctypes.c_void_p,
 ]
+library.gsht_field_jit_stats.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+
+
+def jit_stats():
+    """(programs compiled into kernels of their own, programs that could not
+    be and run interpreted) so far in this process (gsht_field_jit_stats)."""
+    c, f = ctypes.c_int(), ctypes.c_int()
+    _check(library.gsht_field_jit_stats(ctypes.byref(c), ctypes.byref(f)))
+    return int(c.value), int(f.value)
 
 
 class Expr:

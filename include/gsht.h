@@ -218,7 +218,13 @@ gsht_status gsht_inverse_noalloc(const gsht_grid* grid, int lmax, int n, int is_
  * `stream`: each point reads its inputs once and writes its value once. With
  * device buffers the call only enqueues; host buffers are staged through a
  * library workspace and the call returns with the result in host memory.
- * Limits: 64 operations, 16 inputs, a stack 8 values deep. */
+ * Limits: 64 operations, 16 inputs, a stack 8 values deep.
+ * The first call with a given program (on a device) compiles it into a
+ * kernel of its own with NVRTC (loaded at run time, libnvrtc.so.12), cached
+ * for later calls; where NVRTC is unavailable or compilation fails, an
+ * interpreting kernel evaluates the program instead (GSHT_FIELD_JIT=0 forces
+ * it). gsht_field_jit_stats reports how many programs were compiled and how
+ * many could not be (NULL arguments are skipped). */
 enum {
   GSHT_OP_LOAD = 0, GSHT_OP_CONST = 1, GSHT_OP_ADD = 2, GSHT_OP_SUB = 3,
   GSHT_OP_MUL = 4, GSHT_OP_DIV = 5, GSHT_OP_NEG = 6, GSHT_OP_CONJ = 7,
@@ -234,6 +240,7 @@ gsht_status gsht_field_eval(const gsht_expr_op* program, int nops,
                             const void* const* inputs, const int* input_is_real,
                             int ninputs, void* out, int out_is_real, long npoints,
                             int count, long field_stride, void* stream);
+gsht_status gsht_field_jit_stats(int* compiled, int* failed);
 
 /* Batched transforms of many fields of uneven size in one CUDA graph. No
  * counterpart in the reference (its transforms take one field per call,

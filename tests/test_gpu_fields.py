@@ -77,6 +77,32 @@ def test_expressions_match_elementwise_reference(gsht):
             _ = F.Field(grid, 1, False) + 1.0
 
 
+def test_compiled_programs_match_the_interpreter(gsht, monkeypatch):
+    """Each program is compiled (NVRTC) into a kernel of its own on first use;
+    GSHT_FIELD_JIT=0 runs the interpreting kernel instead. Same arithmetic:
+    the two agree to within an ulp or two, and nothing failed to compile."""
+    from gshtrans_b200 import fields as F
+
+    with gsht.GaussLegendreGrid(40, 2) as grid:
+        a, b, c = (_rand(grid, 3, False, s) for s in (11, 12, 13))
+        r = _rand(grid, 3, True, 14)
+        u = F.Field(grid, 1, False, 3, a)
+        v = F.Field(grid, -1, False, 3, b)
+        w = F.Field(grid, 0, False, 3, c)
+        x = F.Field(grid, 0, True, 3, r)
+        exprs = [u * v + F.conj(w) * w, (u * v) / (w + 1.0) - 0.25, F.real(w) * x + x,
+                 -F.imag(w) * 3.0 + x * x, (w * w * w - 1.0) / (w + 2.0)]
+        compiled, failed0 = F.jit_stats()
+        got = [e.evaluate(upper_index=e.N).Data().clone() for e in exprs]
+        compiled1, failed1 = F.jit_stats()
+        assert failed1 == failed0 and compiled1 > compiled
+        monkeypatch.setenv("GSHT_FIELD_JIT", "0")
+        ref = [e.evaluate(upper_index=e.N).Data().clone() for e in exprs]
+        for g_, r_ in zip(got, ref):
+            err = (g_ - r_).abs().max().item() / max(r_.abs().max().item(), 1e-300)
+            assert err < 2 * np.finfo(float).eps, err
+
+
 def test_compound_assignment_in_place(gsht):
     from gshtrans_b200 import fields as F
 
