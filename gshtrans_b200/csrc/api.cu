@@ -279,6 +279,8 @@ gsht_status run_transform(gsht_grid* g, int dir, int lmax, int n, int is_real,
   if (inKind == kOtherDevicePtr || outKind == kOtherDevicePtr)
     return fail(GSHT_ERR_BAD_ARG, "a buffer lives on another GPU than the grid (device %d)", g->device);
   const bool inDev = inKind == kDevicePtr, outDev = outKind == kDevicePtr;
+  if ((inDev && !aligned16(in)) || (outDev && !aligned16(out)))
+    return fail(GSHT_ERR_BAD_ARG, "device buffers must be 16-byte aligned");
 
   // Inside a stream capture (batch graphs) nothing may be allocated, the
   // calls are serial on one stream, and events recorded outside the capture
@@ -691,6 +693,8 @@ gsht_status stage_check(const gsht_grid* g, int lmax, int n, int is_real, int co
   if (pointer_kind(a, g->device) != kDevicePtr || pointer_kind(b, g->device) != kDevicePtr)
     return fail(GSHT_ERR_BAD_ARG, "the stages take device buffers of the grid's device (%d)",
                 g->device);
+  if (!aligned16(a) || !aligned16(b))
+    return fail(GSHT_ERR_BAD_ARG, "device buffers must be 16-byte aligned");
   return GSHT_OK;
 }
 

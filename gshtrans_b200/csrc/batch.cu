@@ -637,6 +637,9 @@ gsht_status gsht_plan_batch(const gsht_field_desc* fields, int count, int precis
         pointer_kind(fields[i].grid, dev) != kDevicePtr ||
         pointer_kind(fields[i].coef_out, dev) != kDevicePtr)
       return fail(GSHT_ERR_BAD_ARG, "field %d: batch buffers must be memory of the current device", i);
+    else if (!aligned16(fields[i].coef_in) || !aligned16(fields[i].grid) ||
+             !aligned16(fields[i].coef_out))
+      return fail(GSHT_ERR_BAD_ARG, "field %d: batch buffers must be 16-byte aligned", i);
   auto* b = new gsht_batch();
   const gsht_status st = plan(fields, count, precision, autotune, b);
   if (st != GSHT_OK) {

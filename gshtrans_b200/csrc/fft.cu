@@ -55,8 +55,6 @@ FftPlan make_plan(int n, int tableLen) {
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 // Spectral buffer elements: FP64 (double2) or FP32 (float2) complex.
-__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
-__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.y); }
 template <typename T>
 __device__ __forceinline__ T from_d2(double2 v);
 template <>

@@ -185,14 +185,6 @@ constexpr int kStageBudget = 32 * 1024;  // shared bytes per stage (two blocks p
 // Set when a wait of the streaming kernel ran out (reported by host-buffer calls).
 __device__ int g_field_wait_err = 0;
 
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
-          "r"(tc::smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
-      : "memory");
-}
-
 template <int kD, int kP>
 __global__ void __launch_bounds__(32 * (kEvalWarps + 1), 2)
     k_field_eval_stream(const __grid_constant__ Program p, int chunk, int stageBytes) {
@@ -238,7 +230,7 @@ __global__ void __launch_bounds__(32 * (kEvalWarps + 1), 2)
           const int esz = p.inReal[a] ? 8 : 16;
           const unsigned char* src =
               static_cast<const unsigned char*>(p.in[a]) + (f * p.stride + p0) * esz;
-          bulk_g2s(st + off[a], src, (uint32_t)(n * esz), &full[s]);
+          tc::bulk_load(st + off[a], src, (uint32_t)(n * esz), &full[s]);
         }
       }
     }

@@ -55,6 +55,9 @@ inline long long round_up(long long x, long long m) { return (x + m - 1) / m * m
 // mapping that need not exist).
 enum PtrKind { kHostPtr = 0, kDevicePtr = 1, kOtherDevicePtr = 2 };
 PtrKind pointer_kind(const void* p, int device);
+// Device buffers are read and written as 16-byte complex elements (and by
+// bulk copies, which need 16-byte addresses): misaligned ones are refused.
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 // Every device allocation of the library goes through these: the hook of
 // gsht_set_allocator when one is set, else cudaMalloc / cudaFree. A pointer

@@ -84,6 +84,8 @@ extern "C" gsht_status gsht_inverse_noalloc(const gsht_grid* g, int lmax, int n,
     return fail(GSHT_ERR_BAD_ARG,
                 "gsht_inverse_noalloc needs in and out in the memory of the grid's device (%d)",
                 g->device);
+  if (!aligned16(in) || !aligned16(out))
+    return fail(GSHT_ERR_BAD_ARG, "device buffers must be 16-byte aligned");
 
   const Table* t = g->table(n);
   if (!t->t64) return fail(GSHT_ERR_UNSUPPORTED, "gsht_inverse_noalloc needs the stored FP64 table");

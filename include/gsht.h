@@ -23,7 +23,8 @@
  * Pointers may be host or device memory (detected per call). With device
  * pointers a call only enqueues work on `stream` (NULL = legacy default
  * stream); with any host pointer the call copies through the grid's
- * workspace and returns after the results are in host memory.
+ * workspace and returns after the results are in host memory. Device
+ * pointers must be 16-byte aligned (GSHT_ERR_BAD_ARG otherwise).
  * Calls that share one grid handle share its workspace: they are ordered on
  * the GPU (each call waits for the previous one), whichever streams they use.
  */

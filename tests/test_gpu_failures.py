@@ -156,3 +156,32 @@ def test_torch_allocator_serves_the_library(gsht, restated):
         gsht.set_allocator()
     a1, r1, _ = gsht.alloc_stats()
     assert a1 > a0 and a1 - a0 == r1 - r0
+
+
+def test_misaligned_device_buffers_are_refused(gsht):
+    """Device buffers are read as 16-byte complex elements: a buffer 8 bytes
+    off that boundary is refused with GSHT_ERR_BAD_ARG before any launch."""
+    import ctypes
+
+    import torch
+
+    from gshtrans_b200 import library
+    from gshtrans_b200 import sharded  # noqa: F401  (declares the stage entry points)
+
+    L, BAD = 32, 1
+    with gsht.GaussLegendreGrid(L, 0) as g:
+        cs = gsht.coefficient_size(L, 0, False)
+        c = torch.zeros(2 * cs + 2, dtype=torch.float64, device="cuda")
+        f = torch.zeros(2 * g.FieldSize() + 2, dtype=torch.float64, device="cuda")
+        bad_c, bad_f = c.data_ptr() + 8, f.data_ptr() + 8
+        s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        assert library.gsht_inverse(g._h, L, 0, 0, 0, bad_c, f.data_ptr(), s) == BAD
+        assert library.gsht_inverse(g._h, L, 0, 0, 0, c.data_ptr(), bad_f, s) == BAD
+        assert library.gsht_forward(g._h, L, 0, 0, 0, bad_f, c.data_ptr(), s) == BAD
+        spec = torch.zeros(1 << 20, dtype=torch.float64, device="cuda")
+        assert library.gsht_inverse_orders(g._h, L, 0, 0, 1, 0, L + 1, bad_c, spec.data_ptr(),
+                                           s) == BAD
+        # aligned buffers still run
+        assert library.gsht_inverse(g._h, L, 0, 0, 0, c.data_ptr(), f.data_ptr(), s) == 0
+        torch.cuda.synchronize()
+        g.device_status()
