@@ -725,22 +725,39 @@ __global__ void __launch_bounds__(256) k_prep_inverse_bf16(
   const int lt = (b + i0) * 32, mt = b * 32, qBase = blockIdx.z * kQB;
   if (lt + 31 < (mt > na ? mt : na) || mt > lmax) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // All kQB tiles' loads are issued before the one barrier.
+  // Every load of the block's kQB tiles is issued into registers before any
+  // of them is used, then the tiles are filled and the block synchronises
+  // once: a warp keeps all its rows in flight at the same time.
+  constexpr int kPer = (kRows + 7) / 8;  // rows per warp (warp 0 takes the 33rd)
+  double2 v[kQB][kPer];
 #pragma unroll
   for (int u = 0; u < kQB; u++) {
     const int q = qBase + u;
     const int sgn = q / count, f = q - sgn * count;
+    const double2* src = q < Q ? (fieldPtrs ? fieldPtrs[f] : coef + (size_t)f * coefSize) : coef;
 #pragma unroll
-    for (int i = warp; i < kRows; i += 8) {
+    for (int r = 0; r < kPer; r++) {
+      const int i = warp + 8 * r;
       const int l = lt - 1 + i, m = mt + lane;
-      double2 v = make_double2(0.0, 0.0);
-      if (q < Q && l >= 0 && l <= lmax && m <= l && l >= na && !(sgn == 1 && m == 0)) {
+      v[u][r] = make_double2(0.0, 0.0);
+      if (i < kRows && q < Q && l >= 0 && l <= lmax && m <= l && l >= na &&
+          !(sgn == 1 && m == 0)) {
         const long idx = isReal ? (long)l * (l + 1) / 2 - (long)na * (na + 1) / 2 + m
                                 : (long)l * l - (long)n * n + l + (sgn ? -m : m);
-        v = fieldPtrs ? fieldPtrs[f][idx] : coef[(size_t)f * coefSize + idx];
-        if (sgn == 1 && ((l + n) & 1)) v = make_double2(-v.x, -v.y);
+        v[u][r] = src[idx];
       }
-      tile[u][i][lane] = v;
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kQB; u++) {
+    const int sgn = (qBase + u) / count;
+#pragma unroll
+    for (int r = 0; r < kPer; r++) {
+      const int i = warp + 8 * r;
+      if (i >= kRows) continue;
+      double2 x = v[u][r];
+      if (sgn == 1 && ((lt - 1 + i + n) & 1)) x = make_double2(-x.x, -x.y);
+      tile[u][i][lane] = x;
     }
   }
   __syncthreads();
@@ -1063,7 +1080,10 @@ gsht_status bf16_prep_inverse(const gsht_grid* g, const Table* t, int lmax, int 
   // Degrees up to l0 + kp - 1 <= lmax + kBKInv - 1: the zero padding of
   // every order's row up to its K-step multiple is written too.
   const int nA = (lmax + kBKInv + 31) / 32, nB = (lmax + 32) / 32;
-  constexpr int kQB = 2;  // field rows per block
+  // One field row per block: 18 KB of shared memory and 40 registers, eight
+  // blocks per SM (0.48 ms at lmax 1024, 64 fields; two rows per block: 0.49
+  // ms at four blocks per SM, 0.51 ms before the loads went to registers).
+  constexpr int kQB = 1;
   dim3 pg(nB * nA - nB * (nB - 1) / 2, 1, (Q + kQB - 1) / kQB);
   k_prep_inverse_bf16<kQB><<<pg, 256, 0, s>>>(lmax, t->n, na, count, Q, R, is_real,
                                               coef_size(lmax, t->n, is_real), pitch, plane, nA,
