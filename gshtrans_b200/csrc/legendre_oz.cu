@@ -454,6 +454,167 @@ __global__ void k_prep_forward_oz(int lmax, int Q, int R, int thetaPad, size_t p
 }
 
 
+// Row-per-block forms of the two preparations: 128 threads read a row once
+// and hold it while they reduce its exponent, then slice it, so the row is
+// read from memory once for both (the warp-per-row kernels above read it
+// twice, and with many rows in flight the second read misses L2). The
+// inverse holds its row in shared memory (16 B per value; few registers, so
+// up to ten blocks per SM keep the strided gathers in flight), the forward in
+// registers. Same arithmetic, bit-identical slices.
+constexpr int kRowThreads = 128;
+
+__device__ __forceinline__ void block_max2(int& a, int& b) {
+  __shared__ int red[2][kRowThreads / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  a = warp_max_int(a);
+  b = warp_max_int(b);
+  if (lane == 0) {
+    red[0][warp] = a;
+    red[1][warp] = b;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int w = 0; w < kRowThreads / 32; w++) {
+    a = max(a, red[0][w]);
+    b = max(b, red[1][w]);
+  }
+}
+
+// Dynamic shared memory: pitch double2 (the row).
+template <int kS>
+__global__ void __launch_bounds__(kRowThreads) k_prep_inverse_oz_row(
+    int lmax, int n, int na, int count, int Q, int R, int isReal, long coefSize, int pitch,
+    size_t plane, const double2* __restrict__ coef, int8_t* __restrict__ op,
+    int* __restrict__ rowExp) {
+  extern __shared__ double2 rowBuf[];
+  const int row = blockIdx.x;  // m * Q + q
+  const int m = row / Q, q = row - m * Q;
+  const int sgn = q / count, f = q - sgn * count;
+  const int l0 = m > na ? m : na;
+  const int keff = lmax - l0 + 1;
+  const int kp = (keff + kBK - 1) / kBK * kBK;
+  const double2* src = coef + (size_t)f * coefSize;
+  int ere = kNoExp, eim = kNoExp;
+  for (int k4 = 4 * (int)threadIdx.x; k4 < kp; k4 += 4 * kRowThreads) {
+    double2 v[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const int k = k4 + t, l = l0 + k;
+      v[t] = make_double2(0.0, 0.0);
+      if (k < keff && !(sgn == 1 && m == 0)) {
+        const long idx = isReal ? (long)l * (l + 1) / 2 - (long)na * (na + 1) / 2 + m
+                                : (long)l * l - (long)n * n + l + (sgn ? -m : m);
+        v[t] = src[idx];
+        if (sgn == 1 && ((l + n) & 1)) v[t] = make_double2(-v[t].x, -v[t].y);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      ere = max(ere, exp_of(v[t].x));
+      eim = max(eim, exp_of(v[t].y));
+      rowBuf[k4 + t] = v[t];
+    }
+  }
+  block_max2(ere, eim);  // its barrier also orders the row buffer
+  if (ere == kNoExp) ere = 0;
+  if (eim == kNoExp) eim = 0;
+  if (threadIdx.x == 0) {
+    rowExp[(size_t)m * R + 2 * q] = ere;
+    rowExp[(size_t)m * R + 2 * q + 1] = eim;
+  }
+  const size_t r0 = ((size_t)m * R + 2 * q) * pitch;
+  const int sre[4] = {-ere, -ere, -ere, -ere}, sim[4] = {-eim, -eim, -eim, -eim};
+  for (int k4 = 4 * (int)threadIdx.x; k4 < kp; k4 += 4 * kRowThreads) {
+    double re[4], im[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const double2 v = rowBuf[k4 + t];
+      re[t] = v.x;
+      im[t] = v.y;
+    }
+    write_slices4<kS>(re, sre, op + r0 + k4, plane);
+    write_slices4<kS>(im, sim, op + r0 + pitch + k4, plane);
+  }
+}
+
+// The forward keeps its row in registers instead (up to 512 kQ values, four
+// consecutive per thread and pass): measured faster than the shared-memory
+// buffer here (0.97 against 1.13 ms at lmax 1024, 64 fields, 7 slices),
+// while the inverse's strided gathers want the occupancy that the small
+// register footprint of the buffered form gives (0.82 against 0.93 ms).
+template <int kS, int kQ>
+__global__ void __launch_bounds__(kRowThreads) k_prep_forward_oz_row(
+    int lmax, int Q, int R, int thetaPad, size_t plane, const double2* __restrict__ spec,
+    const int* __restrict__ tabExp, int8_t* __restrict__ op, int* __restrict__ rowExp) {
+  const int row = blockIdx.x;  // m * Q + q
+  const int m = row / Q, q = row - m * Q;
+  const double2* src = spec + (size_t)row * thetaPad;
+  const int4* te4 = reinterpret_cast<const int4*>(tabExp + (size_t)m * thetaPad);
+  const int nq = thetaPad / 4;
+  double2 v[kQ][4];
+  int4 e[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; i++) {
+    const int j4 = (int)threadIdx.x + kRowThreads * i;
+    e[i] = make_int4(0, 0, 0, 0);
+#pragma unroll
+    for (int t = 0; t < 4; t++) v[i][t] = make_double2(0.0, 0.0);
+    if (j4 < nq) {
+      e[i] = te4[j4];
+#pragma unroll
+      for (int t = 0; t < 4; t++) v[i][t] = src[4 * j4 + t];
+    }
+  }
+  // Row exponents of the column-scaled values x 2^{e_j}: the largest
+  // exp(x) + e_j (0 for an all-zero row).
+  int ere = kNoExp, eim = kNoExp;
+#pragma unroll
+  for (int i = 0; i < kQ; i++) {
+    const int ev[4] = {e[i].x, e[i].y, e[i].z, e[i].w};
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const int xr = exp_of(v[i][t].x), xi = exp_of(v[i][t].y);
+      if (xr != kNoExp) ere = max(ere, xr + ev[t]);
+      if (xi != kNoExp) eim = max(eim, xi + ev[t]);
+    }
+  }
+  block_max2(ere, eim);
+  if (ere == kNoExp) ere = 0;
+  if (eim == kNoExp) eim = 0;
+  if (threadIdx.x == 0) {
+    rowExp[(size_t)m * R + 2 * q] = ere;
+    rowExp[(size_t)m * R + 2 * q + 1] = eim;
+  }
+  const size_t r0 = ((size_t)m * R + 2 * q) * thetaPad;
+#pragma unroll
+  for (int i = 0; i < kQ; i++) {
+    const int j4 = (int)threadIdx.x + kRowThreads * i;
+    if (j4 >= nq) break;
+    const int ev[4] = {e[i].x, e[i].y, e[i].z, e[i].w};
+    double re[4], im[4];
+    int sre[4], sim[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      re[t] = v[i][t].x;
+      im[t] = v[i][t].y;
+      sre[t] = ev[t] - ere;
+      sim[t] = ev[t] - eim;
+    }
+    write_slices4<kS>(re, sre, op + r0 + 4 * j4, plane);
+    write_slices4<kS>(im, sim, op + r0 + thetaPad + 4 * j4, plane);
+  }
+}
+
+// Rows up to this many values run row-per-block (inverse: 48 KB of shared
+// memory without opting in; forward: kQ = 2, 3 or 6 passes); longer ones
+// take the warp-per-row kernels.
+constexpr int kRowMax = 3072;
+
+inline int row_passes(int len) {
+  const int p = (len + 4 * kRowThreads - 1) / (4 * kRowThreads);
+  return p <= 2 ? 2 : (p <= 3 ? 3 : 6);
+}
+
 // 3-D byte tensor [planes][rows][inner] with a [1][boxRows][boxInner] box.
 gsht_status make_map_i8(CUtensorMap* map, const void* base, uint64_t inner, uint64_t rows,
                         uint64_t planes, uint64_t rowPitch, uint64_t planeBytes,
@@ -522,9 +683,15 @@ gsht_status inverse_oz(const gsht_grid* g, const Table* t, int lmax, int is_real
   {
     StageTimer tm(GSHT_STAGE_PREP_INVERSE, s);
     const long long warps = (long long)(lmax + 1) * Q;
-    k_prep_inverse_oz<kS><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
-        lmax, t->n, na, count, Q, R, is_real, coef_size(lmax, t->n, is_real), pitch, plane,
-        reinterpret_cast<const double2*>(coef), op, rowExp);
+    const auto* c2 = reinterpret_cast<const double2*>(coef);
+    const long cs = coef_size(lmax, t->n, is_real);
+    if (pitch > kRowMax) {
+      k_prep_inverse_oz<kS><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
+          lmax, t->n, na, count, Q, R, is_real, cs, pitch, plane, c2, op, rowExp);
+    } else {
+      k_prep_inverse_oz_row<kS><<<(unsigned)warps, kRowThreads, sizeof(double2) * pitch, s>>>(
+          lmax, t->n, na, count, Q, R, is_real, cs, pitch, plane, c2, op, rowExp);
+    }
     GSHT_LAUNCH_CHECK("k_prep_inverse_oz");
   }
   CUtensorMap mapA, mapB;
@@ -557,8 +724,16 @@ gsht_status forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real
   {
     StageTimer tm(GSHT_STAGE_PREP_FORWARD, s);
     const long long warps = (long long)(lmax + 1) * Q;
-    k_prep_forward_oz<kS><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
-        lmax, Q, R, tp, plane, reinterpret_cast<const double2*>(spec), t->i8_exp, op, rowExp);
+    const auto* s2 = reinterpret_cast<const double2*>(spec);
+    if (tp > kRowMax) {
+      k_prep_forward_oz<kS><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(
+          lmax, Q, R, tp, plane, s2, t->i8_exp, op, rowExp);
+    } else {
+      const int passes = row_passes(tp);
+      auto kern = passes == 2 ? k_prep_forward_oz_row<kS, 2>
+                              : (passes == 3 ? k_prep_forward_oz_row<kS, 3> : k_prep_forward_oz_row<kS, 6>);
+      kern<<<(unsigned)warps, kRowThreads, 0, s>>>(lmax, Q, R, tp, plane, s2, t->i8_exp, op, rowExp);
+    }
     GSHT_LAUNCH_CHECK("k_prep_forward_oz");
   }
   CUtensorMap mapA, mapB;
