@@ -333,6 +333,14 @@ __global__ void k_slice_i8(int L, int n, int thetaPad,
   }
 }
 
+// Column j of the FP64 table, one value per row (the rows of order m at
+// row_off[m]..).
+__global__ void k_table_column(long long rows, int thetaPad, int j, const double* __restrict__ t64,
+                               double* __restrict__ col) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < rows) col[r] = t64[(size_t)r * thetaPad + j];
+}
+
 }  // namespace
 
 gsht_status build_nodes(gsht_grid* g) {
@@ -491,6 +499,16 @@ gsht_status build_forms(gsht_grid* g, Table* t, cudaStream_t s) {
     k_slice_i8<<<grid, 128, 0, s>>>(L, t->n, tp, t->d_row_off, t->t64, t->ti8,
                                     plane, t->i8_exp);
     GSHT_LAUNCH_CHECK("k_slice_i8");
+    if (g->n_theta % 128 == 1) {
+      if (dev_malloc(&t->tail64, sizeof(double) * (size_t)t->rows) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(GSHT_ERR_OOM, "table column allocation failed");
+      }
+      k_table_column<<<(unsigned)((t->rows + 255) / 256), 256, 0, s>>>(t->rows, tp,
+                                                                       g->n_theta - 1, t->t64,
+                                                                       t->tail64);
+      GSHT_LAUNCH_CHECK("k_table_column");
+    }
   }
   GSHT_CUDA(cudaStreamSynchronize(s));
   return GSHT_OK;
@@ -571,6 +589,7 @@ void free_table(Table* t) {
   dev_free(t->tbf);
   dev_free(t->ti8);
   dev_free(t->i8_exp);
+  dev_free(t->tail64);
   dev_free(t->rec_f);
   dev_free(t->rec_e);
   dev_free(t->rec_ab);

@@ -127,6 +127,11 @@ struct Table {
   __nv_bfloat16* tbf = nullptr;       // 3 planes (hi, mid, lo), same layout
   int8_t* ti8 = nullptr;              // kTableSlices planes, same layout
   int* i8_exp = nullptr;              // (L+1) x thetaPad column exponents
+  // FP64 values of the last colatitude column (theta_{nTheta-1}), one per
+  // row, when the Ozaki form is stored and nTheta = 128 k + 1: that
+  // colatitude would fill a 128-row inverse tile of its own, so the operand
+  // preparation contracts it instead (legendre_oz.cu).
+  double* tail64 = nullptr;
   // Recurrence form (no stored values): start values d^{l0(m)}_{mn}(theta_j)
   // = rec_f * 2^rec_e, [m][thetaPad], and per row the coefficients (a', b')
   // of the rescaled recurrence e_k = (a' cos(theta) - b') e_{k-1} - e_{k-2}
@@ -153,7 +158,7 @@ struct OperandLayout {
 // Work list of a persistent tensor-core launch: tiles (m, mtile, ntile, nk)
 // in order of decreasing m-block work, cached on the grid per key.
 struct TileList {
-  int dir = 0, lmax = 0, na = 0, rows = 0, ntile = 0, kstep = 0;
+  int dir = 0, lmax = 0, na = 0, rows = 0, ntile = 0, kstep = 0, tail = 0;
   int4* d_tiles = nullptr;
   int count = 0;
 };
@@ -361,8 +366,10 @@ void free_layouts(gsht_grid* g);
 // Cached tile list for a persistent tensor-core launch (legendre_tc.cu).
 // dir 0 = inverse (M = colatitudes), 1 = forward (M = degrees); rows = field
 // rows R; ntile = field rows per tile; the caller holds g->mu.
+// tail: inverse only, colatitudes at the end left out of the M tiles (their
+// spectra are written by another kernel).
 const TileList* tile_list(const gsht_grid* g, int dir, int lmax, int na, int rows,
-                          int ntile, int kstep, gsht_status* st);
+                          int ntile, int kstep, gsht_status* st, int tail = 0);
 
 // Spectral buffer element count: (lmax+1) x sgn x count x thetaPad complex.
 inline size_t spec_elems(const gsht_grid* g, int lmax, int is_real, int count) {

@@ -481,11 +481,18 @@ __device__ __forceinline__ void block_max2(int& a, int& b) {
 }
 
 // Dynamic shared memory: pitch double2 (the row).
+// tail: when set, the FP64 table column of the last colatitude (one value
+// per table row, rows of order m from rowOff[m]); the block then also
+// contracts its row with it in FP64 and writes that colatitude's spectrum,
+// spec[(m Q + q) thetaPad + nTheta - 1] (the -m rows' spectra at the
+// mirrored index, as the tensor-core epilogue writes them), which the
+// inverse's M tiles then leave out.
 template <int kS>
-__global__ void __launch_bounds__(kRowThreads) k_prep_inverse_oz_row(
+__global__ void __launch_bounds__(kRowThreads, 10) k_prep_inverse_oz_row(
     int lmax, int n, int na, int count, int Q, int R, int isReal, long coefSize, int pitch,
     size_t plane, const double2* __restrict__ coef, int8_t* __restrict__ op,
-    int* __restrict__ rowExp) {
+    int* __restrict__ rowExp, const double* __restrict__ tail,
+    const long long* __restrict__ rowOff, double2* __restrict__ spec, int nTheta, int thetaPad) {
   extern __shared__ double2 rowBuf[];
   const int row = blockIdx.x;  // m * Q + q
   const int m = row / Q, q = row - m * Q;
@@ -495,6 +502,8 @@ __global__ void __launch_bounds__(kRowThreads) k_prep_inverse_oz_row(
   const int kp = (keff + kBK - 1) / kBK * kBK;
   const double2* src = coef + (size_t)f * coefSize;
   int ere = kNoExp, eim = kNoExp;
+  double tre = 0.0, tim = 0.0;  // this thread's part of the tail contraction
+  const double* tcol = tail ? tail + rowOff[m] : nullptr;
   for (int k4 = 4 * (int)threadIdx.x; k4 < kp; k4 += 4 * kRowThreads) {
     double2 v[4];
 #pragma unroll
@@ -534,6 +543,35 @@ __global__ void __launch_bounds__(kRowThreads) k_prep_inverse_oz_row(
     }
     write_slices4<kS>(re, sre, op + r0 + k4, plane);
     write_slices4<kS>(im, sim, op + r0 + pitch + k4, plane);
+  }
+  if (tcol) {
+    // The tail contraction, from the buffered row (a second pass over
+    // shared memory keeps the gather loop's registers as they were).
+    for (int k = (int)threadIdx.x; k < keff; k += kRowThreads) {
+      const double d = tcol[k];
+      const double2 v = rowBuf[k];
+      tre = fma(d, v.x, tre);
+      tim = fma(d, v.y, tim);
+    }
+    __shared__ double tred[2][kRowThreads / 32];
+    for (int o = 16; o; o >>= 1) {
+      tre += __shfl_xor_sync(0xffffffffu, tre, o);
+      tim += __shfl_xor_sync(0xffffffffu, tim, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      tred[0][threadIdx.x >> 5] = tre;
+      tred[1][threadIdx.x >> 5] = tim;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0, b = 0.0;
+#pragma unroll
+      for (int w = 0; w < kRowThreads / 32; w++) {
+        a += tred[0][w];
+        b += tred[1][w];
+      }
+      spec[((size_t)m * Q + q) * thetaPad + (nTheta - 1)] = make_double2(a, b);
+    }
   }
 }
 
@@ -634,11 +672,11 @@ gsht_status make_map_i8(CUtensorMap* map, const void* base, uint64_t inner, uint
 
 template <int kDir, int kS, int kN>
 gsht_status launch_oz(const gsht_grid* g, const OzArgs& a, const CUtensorMap& mapA,
-                      const CUtensorMap& mapB, cudaStream_t s) {
+                      const CUtensorMap& mapB, cudaStream_t s, int tail = 0) {
   gsht_status st;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
-  const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kN, kBK, &st);
+  const TileList* tl = tile_list(g, kDir == 0 ? 0 : 1, a.lmax, a.na, a.R, kN, kBK, &st, tail);
   if (!tl) return st;
   constexpr size_t kSmem = OzCfg<kS, kN>::kSmemBytes;
   const int blocks = tl->count < sms ? tl->count : sms;
@@ -680,6 +718,10 @@ gsht_status inverse_oz(const gsht_grid* g, const Table* t, int lmax, int is_real
   const size_t plane = (size_t)(lmax + 1) * R * pitch;
   auto* op = static_cast<int8_t*>(operand);
   int* rowExp = reinterpret_cast<int*>(static_cast<char*>(operand) + round_up(kS * plane, 256));
+  // With nTheta = 128 k + 1 the last colatitude would take a 128-row tile of
+  // its own in every order (1/9 of the MMAs at lmax 1024): the row-per-block
+  // preparation contracts it in FP64 instead.
+  const bool tail = t->tail64 && pitch <= kRowMax && g->n_theta % kBM == 1;
   {
     StageTimer tm(GSHT_STAGE_PREP_INVERSE, s);
     const long long warps = (long long)(lmax + 1) * Q;
@@ -690,7 +732,9 @@ gsht_status inverse_oz(const gsht_grid* g, const Table* t, int lmax, int is_real
           lmax, t->n, na, count, Q, R, is_real, cs, pitch, plane, c2, op, rowExp);
     } else {
       k_prep_inverse_oz_row<kS><<<(unsigned)warps, kRowThreads, sizeof(double2) * pitch, s>>>(
-          lmax, t->n, na, count, Q, R, is_real, cs, pitch, plane, c2, op, rowExp);
+          lmax, t->n, na, count, Q, R, is_real, cs, pitch, plane, c2, op, rowExp,
+          tail ? t->tail64 : nullptr, t->d_row_off, reinterpret_cast<double2*>(spec), g->n_theta,
+          g->theta_pad);
     }
     GSHT_LAUNCH_CHECK("k_prep_inverse_oz");
   }
@@ -709,7 +753,7 @@ gsht_status inverse_oz(const gsht_grid* g, const Table* t, int lmax, int is_real
   a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
   StageTimer tm(GSHT_STAGE_LEGENDRE_INVERSE, s);
-  return launch_oz<0, kS, kN>(g, a, mapA, mapB, s);
+  return launch_oz<0, kS, kN>(g, a, mapA, mapB, s, tail ? 1 : 0);
 }
 
 template <int kS, int kN>

@@ -1031,24 +1031,25 @@ gsht_status launch_bf16_pair(const gsht_grid* g, const TcArgs& a, const CUtensor
 // blocks of the persistent grid work on the same table tile at the same
 // time, so it comes from DRAM once and from L2 for the others.
 const TileList* tile_list(const gsht_grid* g, int dir, int lmax, int na, int rows, int ntile,
-                          int kstep, gsht_status* st) {
+                          int kstep, gsht_status* st, int tail) {
   *st = GSHT_OK;
   for (auto* t : g->tile_lists)
     if (t->dir == dir && t->lmax == lmax && t->na == na && t->rows == rows && t->ntile == ntile &&
-        t->kstep == kstep)
+        t->kstep == kstep && t->tail == tail)
       return t;
   std::vector<int4> v;
   const int ntiles = (rows + ntile - 1) / ntile;
   for (int m = 0; m <= lmax; m++) {
     const int l0 = m > na ? m : na;
     const int keff = lmax - l0 + 1;
-    const int mtiles = dir == 0 ? (g->n_theta + kBM - 1) / kBM : (keff + kBM - 1) / kBM;
+    const int mtiles = dir == 0 ? (g->n_theta - tail + kBM - 1) / kBM : (keff + kBM - 1) / kBM;
     const int nk = dir == 0 ? (keff + kstep - 1) / kstep : (g->theta_pad + kstep - 1) / kstep;
     for (int mt = 0; mt < mtiles; mt++)
       for (int nt = 0; nt < ntiles; nt++) v.push_back(make_int4(m, mt, nt, nk));
   }
   auto* t = new TileList();
   t->dir = dir; t->lmax = lmax; t->na = na; t->rows = rows; t->ntile = ntile; t->kstep = kstep;
+  t->tail = tail;
   t->count = (int)v.size();
   if (dev_malloc(&t->d_tiles, sizeof(int4) * v.size()) != cudaSuccess ||
       cudaMemcpy(t->d_tiles, v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice) !=
