@@ -366,8 +366,9 @@ void free_layouts(gsht_grid* g);
 // Cached tile list for a persistent tensor-core launch (legendre_tc.cu).
 // dir 0 = inverse (M = colatitudes), 1 = forward (M = degrees); rows = field
 // rows R; ntile = field rows per tile; the caller holds g->mu.
-// tail: inverse only, colatitudes at the end left out of the M tiles (their
-// spectra are written by another kernel).
+// tail: colatitudes at the end left out of the tiles: of the inverse's M
+// tiles (their spectra are written by another kernel) or the forward's K
+// steps (their products are added in the epilogue).
 const TileList* tile_list(const gsht_grid* g, int dir, int lmax, int na, int rows,
                           int ntile, int kstep, gsht_status* st, int tail = 0);
 

@@ -62,6 +62,11 @@ struct OzArgs {
   long coefSize;
   int* err;
   unsigned long long* trace;  // kTrSlots counters of a traced launch
+  // Forward with a tail colatitude left out of the K steps: the FP64 table
+  // column (rows from rowOff[m]) and the saved spectra [m Q + q], whose
+  // product the epilogue adds to each result.
+  const double* tail64;
+  const double2* tailVals;
 };
 
 // Four warps per TMEM lane quarter, 16 columns each: the MMA warp waits for
@@ -257,8 +262,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (q >= p.Q) break;
         const int ere = p.rowExp[(size_t)m * p.R + 2 * q];
         const int eim = p.rowExp[(size_t)m * p.R + 2 * q + 1];
-        p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] =
-            make_double2(ldexp(acc[2 * i], eA + ere), ldexp(acc[2 * i + 1], eA + eim));
+        double2 o = make_double2(ldexp(acc[2 * i], eA + ere), ldexp(acc[2 * i + 1], eA + eim));
+        if (kDir == 1 && p.tailVals) {
+          const double d = p.tail64[p.rowOff[m] + tileRow];
+          const double2 sv = p.tailVals[(size_t)m * p.Q + q];
+          o = make_double2(fma(d, sv.x, o.x), fma(d, sv.y, o.y));
+        }
+        p.out[((size_t)m * p.Q + q) * p.thetaPad + tileRow] = o;
       }
     }
   }
@@ -580,10 +590,14 @@ __global__ void __launch_bounds__(kRowThreads, 10) k_prep_inverse_oz_row(
 // buffer here (0.97 against 1.13 ms at lmax 1024, 64 fields, 7 slices),
 // while the inverse's strided gathers want the occupancy that the small
 // register footprint of the buffered form gives (0.82 against 0.93 ms).
+// tailOut: when set, the row's spectrum at colatitude column nTheta - 1 is
+// saved to tailOut[m Q + q] (the forward's tiles then stop before that
+// column and their epilogue adds its FP64 product with the table).
 template <int kS, int kQ>
 __global__ void __launch_bounds__(kRowThreads) k_prep_forward_oz_row(
     int lmax, int Q, int R, int thetaPad, size_t plane, const double2* __restrict__ spec,
-    const int* __restrict__ tabExp, int8_t* __restrict__ op, int* __restrict__ rowExp) {
+    const int* __restrict__ tabExp, int8_t* __restrict__ op, int* __restrict__ rowExp,
+    double2* __restrict__ tailOut, int nTheta) {
   const int row = blockIdx.x;  // m * Q + q
   const int m = row / Q, q = row - m * Q;
   const double2* src = spec + (size_t)row * thetaPad;
@@ -603,6 +617,7 @@ __global__ void __launch_bounds__(kRowThreads) k_prep_forward_oz_row(
       for (int t = 0; t < 4; t++) v[i][t] = src[4 * j4 + t];
     }
   }
+  if (tailOut && threadIdx.x == 0) tailOut[row] = src[nTheta - 1];
   // Row exponents of the column-scaled values x 2^{e_j}: the largest
   // exp(x) + e_j (0 for an all-zero row).
   int ere = kNoExp, eim = kNoExp;
@@ -704,7 +719,11 @@ size_t oz_operand_bytes(const gsht_grid* g, int lmax, int is_real, int count, in
   const int kS = slices;
   const int R = 2 * (is_real ? 1 : 2) * count;
   const long long pitch = dir == 0 ? g->theta_pad : round_up(lmax + 1, kBK);
-  return (size_t)kS * (lmax + 1) * R * pitch + sizeof(int) * (size_t)(lmax + 1) * R + 256;
+  // Slice planes, row exponents, and (forward) one saved spectrum value per
+  // field row for the tail colatitude.
+  return round_up((size_t)kS * (lmax + 1) * R * pitch, 256) +
+         round_up(sizeof(int) * (size_t)(lmax + 1) * R, 256) +
+         sizeof(double2) * (size_t)(lmax + 1) * (R / 2) + 256;
 }
 
 namespace {
@@ -765,6 +784,12 @@ gsht_status forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real
   const size_t plane = (size_t)(lmax + 1) * R * tp;
   auto* op = static_cast<int8_t*>(operand);
   int* rowExp = reinterpret_cast<int*>(static_cast<char*>(operand) + round_up(kS * plane, 256));
+  // With nTheta = 128 k + 1 the last colatitude would cost a 64-colatitude
+  // K step of its own in every tile: the preparation saves its spectra, the
+  // tiles stop before it, and the accumulation adds its FP64 product.
+  const bool tail = t->tail64 && tp <= kRowMax && g->n_theta % kBM == 1;
+  auto* tailVals = reinterpret_cast<double2*>(
+      reinterpret_cast<char*>(rowExp) + round_up(sizeof(int) * (size_t)(lmax + 1) * R, 256));
   {
     StageTimer tm(GSHT_STAGE_PREP_FORWARD, s);
     const long long warps = (long long)(lmax + 1) * Q;
@@ -776,7 +801,8 @@ gsht_status forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real
       const int passes = row_passes(tp);
       auto kern = passes == 2 ? k_prep_forward_oz_row<kS, 2>
                               : (passes == 3 ? k_prep_forward_oz_row<kS, 3> : k_prep_forward_oz_row<kS, 6>);
-      kern<<<(unsigned)warps, kRowThreads, 0, s>>>(lmax, Q, R, tp, plane, s2, t->i8_exp, op, rowExp);
+      kern<<<(unsigned)warps, kRowThreads, 0, s>>>(lmax, Q, R, tp, plane, s2, t->i8_exp, op, rowExp,
+                                                   tail ? tailVals : nullptr, g->n_theta);
     }
     GSHT_LAUNCH_CHECK("k_prep_forward_oz");
   }
@@ -796,9 +822,13 @@ gsht_status forward_oz(const gsht_grid* g, const Table* t, int lmax, int is_real
   // go into their buffer and are then added into the coefficients.
   a.out = reinterpret_cast<double2*>(spec);
   a.coefSize = coef_size(lmax, t->n, is_real); a.err = g->d_err;
+  if (tail) {
+    a.tail64 = t->tail64;
+    a.tailVals = tailVals;
+  }
   {
     StageTimer tm(GSHT_STAGE_LEGENDRE_FORWARD, s);
-    st = launch_oz<1, kS, kN>(g, a, mapA, mapB, s);
+    st = launch_oz<1, kS, kN>(g, a, mapA, mapB, s, tail ? 1 : 0);
   }
   if (st != GSHT_OK) return st;
   return accumulate_forward(g->L, lmax, t->n, na, count, Q, is_real, a.coefSize, tp, spec, coef, s);

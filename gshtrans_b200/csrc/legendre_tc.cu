@@ -1043,7 +1043,9 @@ const TileList* tile_list(const gsht_grid* g, int dir, int lmax, int na, int row
     const int l0 = m > na ? m : na;
     const int keff = lmax - l0 + 1;
     const int mtiles = dir == 0 ? (g->n_theta - tail + kBM - 1) / kBM : (keff + kBM - 1) / kBM;
-    const int nk = dir == 0 ? (keff + kstep - 1) / kstep : (g->theta_pad + kstep - 1) / kstep;
+    const int nk = dir == 0 ? (keff + kstep - 1) / kstep
+                            : (tail ? (g->n_theta - tail + kstep - 1) / kstep
+                                    : (g->theta_pad + kstep - 1) / kstep);
     for (int mt = 0; mt < mtiles; mt++)
       for (int nt = 0; nt < ntiles; nt++) v.push_back(make_int4(m, mt, nt, nk));
   }
