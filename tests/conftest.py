@@ -24,6 +24,25 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and libgsht_cuda.so")
 
 
+@pytest.fixture(autouse=True, scope="module")
+def _release_device_memory():
+    """After each test module, return the device memory its objects held
+    (collected grids, torch's cached blocks), so that the large-table tests
+    (lmax 2048 grids take up to ~180 GB) see the whole GPU whatever ran
+    before them. No-op where CUDA was never initialised."""
+    yield
+    if "torch" not in sys.modules:
+        return
+    import gc
+
+    import torch
+
+    gc.collect()
+    if torch.cuda.is_available() and torch.cuda.is_initialized():
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
+
 def relerr(a, b) -> float:
     """Norm-wise relative error ||a - b||_2 / ||b||_2."""
     a = np.asarray(a)

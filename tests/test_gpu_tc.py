@@ -107,8 +107,13 @@ def test_bf16x3_fp32_spectra_every_ring_length(gsht, L):
     # = 2L for complex fields, L for real ones), the BF16x3 form keeps its
     # spectra in FP32 with unmirrored -m rows; 4096-point rings load them
     # without TMA. Both field kinds, a negative upper index (mirror signs).
+    import gc
+
     import torch
 
+    if L >= 2048:  # three n tables of FP64 + BF16 planes: ~182 GB of the GPU
+        gc.collect()
+        torch.cuda.empty_cache()
     rng = np.random.default_rng(500 + L)
     with gsht.GaussLegendreGrid(L, 1, forms=("bf16x3",)) as g:
         for is_real, n, lmax in ((False, -1, L), (True, 1, L), (False, 1, L - 37)):
