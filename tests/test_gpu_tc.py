@@ -241,6 +241,37 @@ def test_ozaki_L1024_batched(gsht, n, is_real):
     assert relerr(res["ozaki"][1], res["fp64"][1]) < TOL_OZ
 
 
+@pytest.mark.parametrize("L,lmax,n,is_real,prec", [
+    (128, 128, 0, False, "ozaki"),
+    (128, 97, -3, True, "ozaki"),
+    (256, 256, 2, False, "ozaki4"),
+    (256, 201, 1, True, "ozaki"),
+    (256, 256, -1, False, "ozaki"),
+])
+def test_ozaki_tail_colatitude(gsht, L, lmax, n, is_real, prec):
+    # nTheta = L + 1 = 128 k + 1: the last colatitude is contracted outside
+    # the tensor-core tiles, in FP64 (inverse: by the operand preparation;
+    # forward: saved by the preparation, added by the epilogue). The two
+    # pole rings (the last one, and the first, where complex fields' -m
+    # rows of that column land) are checked on their own as well as the
+    # whole field and the forward.
+    rng = np.random.default_rng(4000 + L + lmax + 7 * n)
+    tol = TOL_OZ if prec == "ozaki" else TOL_BF16
+    with gsht.GaussLegendreGrid(L, max(abs(n), 1), forms=("ozaki",)) as g:
+        nt, nphi = g.NumberOfCoLatitudes(), g.NumberOfLongitudes()
+        assert nt % 128 == 1
+        c = oracle.random_coefficients(rng, L, lmax, n, is_real, 1.0)
+        f64, b64 = _both(g, lmax, n, is_real, c, "fp64")
+        fo, bo = _both(g, lmax, n, is_real, c, prec)
+        ring64, ringo = f64.reshape(nt, -1), fo.reshape(nt, -1)
+        for ring in (0, nt - 1):
+            assert relerr(ringo[ring], ring64[ring]) < 10 * tol, (ring, L, lmax, n, is_real)
+        assert relerr(fo, f64) < tol, (L, lmax, n, is_real)
+        out = np.zeros_like(c)
+        g.ForwardTransformation(lmax, n, f64, out, prec)
+        assert relerr(out, b64) < 2 * tol, (L, lmax, n, is_real)
+
+
 @pytest.mark.parametrize("is_real", [False, True])
 def test_ozaki_L2048_single_field_vs_fp64(gsht, is_real):
     # The large single-transform case: lmax 2048, n = 1, envelope (l+1)^-2;
